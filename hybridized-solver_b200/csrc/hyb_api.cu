@@ -1,0 +1,1022 @@
+// hyb_api.cu - the C ABI (include/hybsol_b200.h): handle lifecycle, device memory,
+// the level schedule (captured into CUDA graphs), plain FP64 and mixed FP32+refinement
+// solves.
+#include "hyb_internal.h"
+#include "hyb_kernels.cuh"
+
+#include "hybsol_b200.h"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+using hyb::DevSym;
+using hyb::Symbolic;
+
+namespace
+{
+thread_local std::string g_cuda_error;
+
+int cuda_fail(cudaError_t e, const char *what)
+{
+    g_cuda_error = std::string(what) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation)
+        return HYB_FAILED_ALLOC;
+    return HYB_CUDA_ERROR;
+}
+
+#define HYB_CUDA(call)                                                                                                 \
+    do                                                                                                                 \
+    {                                                                                                                  \
+        cudaError_t e_ = (call);                                                                                       \
+        if (e_ != cudaSuccess)                                                                                         \
+            return cuda_fail(e_, #call);                                                                               \
+    } while (0)
+
+// Largest dynamic shared memory a CTA may request on this device (set once per kernel).
+int g_smem_optin = 0;
+
+int smem_optin()
+{
+    if (g_smem_optin == 0)
+    {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        g_smem_optin = v > 0 ? v : 48 * 1024;
+    }
+    return g_smem_optin;
+}
+
+template <typename K> void allow_smem(K kernel)
+{
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin());
+}
+
+__global__ void k_status_init(int *st)
+{
+    if (threadIdx.x == 0)
+    {
+        st[hyb::ST_ZERO_PIVOTS] = 0;
+        st[hyb::ST_NON_FINITE] = 0;
+        st[hyb::ST_FIRST_BAD] = INT_MAX;
+        st[3] = 0;
+    }
+}
+
+struct GraphExec
+{
+    cudaGraphExec_t exec = nullptr;
+    uint64_t launches = 0;
+    ~GraphExec()
+    {
+        if (exec)
+            cudaGraphExecDestroy(exec);
+    }
+};
+
+} // namespace
+
+struct hyb_system
+{
+    Symbolic S;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    void *arena = nullptr;
+    DevSym ds{};
+    double *d_a = nullptr; // original values (FP64, CSR order)
+    int *d_status = nullptr;
+    int factored = -1; // -1, HYB_PRECISION_FP64 or HYB_PRECISION_MIXED
+    double *d_f64 = nullptr;
+    float *d_f32 = nullptr;
+    // solve buffers, sized for buf_nrhs right-hand sides
+    int64_t buf_nrhs = 0;
+    double *d_b = nullptr, *d_x = nullptr, *d_r = nullptr, *d_scr64 = nullptr, *d_part = nullptr, *d_norm = nullptr;
+    float *d_yf = nullptr, *d_scr32 = nullptr;
+    int n_norm_parts = 0;
+    std::unique_ptr<GraphExec> g_factor[2];
+    std::map<std::pair<int, int>, std::unique_ptr<GraphExec>> g_solve; // (precision, nrhs)
+    uint64_t launches = 0;
+    uint64_t last_launches = 0;
+
+    ~hyb_system()
+    {
+        g_factor[0].reset();
+        g_factor[1].reset();
+        g_solve.clear();
+        cudaFree(arena);
+        cudaFree(d_a);
+        cudaFree(d_status);
+        cudaFree(d_f64);
+        cudaFree(d_f32);
+        free_solve_buffers();
+        if (stream)
+            cudaStreamDestroy(stream);
+    }
+
+    void free_solve_buffers()
+    {
+        for (void *p : {(void *)d_b, (void *)d_x, (void *)d_r, (void *)d_scr64, (void *)d_part, (void *)d_norm,
+                        (void *)d_yf, (void *)d_scr32})
+            cudaFree(p);
+        d_b = d_x = d_r = d_scr64 = d_part = d_norm = nullptr;
+        d_yf = d_scr32 = nullptr;
+        buf_nrhs = 0;
+        g_solve.clear();
+    }
+};
+
+namespace
+{
+
+// Copies the symbolic arrays into one device allocation and fills the DevSym view.
+int upload_symbolic(hyb_system *h)
+{
+    const Symbolic &S = h->S;
+    struct Item
+    {
+        const void *src;
+        size_t bytes;
+        const void **dst;
+    };
+    DevSym &d = h->ds;
+    d.n = S.n;
+    std::vector<Item> items = {
+        {S.size.data(), S.size.size() * 4, (const void **)&d.size},
+        {S.dof_off.data(), S.dof_off.size() * 8, (const void **)&d.dof_off},
+        {S.row_ptr.data(), S.row_ptr.size() * 8, (const void **)&d.row_ptr},
+        {S.cols.data(), S.cols.size() * 4, (const void **)&d.cols},
+        {S.diag_pos.data(), S.diag_pos.size() * 8, (const void **)&d.diag_pos},
+        {S.blk_off.data(), S.blk_off.size() * 8, (const void **)&d.blk_off},
+        {S.lcol_ptr.data(), S.lcol_ptr.size() * 8, (const void **)&d.lcol_ptr},
+        {S.lcol_row.data(), S.lcol_row.size() * 4, (const void **)&d.lcol_row},
+        {S.lcol_blk.data(), S.lcol_blk.size() * 4, (const void **)&d.lcol_blk},
+        {S.piv.data(), S.piv.size() * 4, (const void **)&d.piv},
+        {S.trsm_pref.data(), S.trsm_pref.size() * 8, (const void **)&d.trsm_pref},
+        {S.upd_pref.data(), S.upd_pref.size() * 8, (const void **)&d.upd_pref},
+        {S.fwd_pref.data(), S.fwd_pref.size() * 8, (const void **)&d.fwd_pref},
+        {S.fwd_rows.data(), S.fwd_rows.size() * 8, (const void **)&d.fwd_rows},
+        {S.bwd_rows.data(), S.bwd_rows.size() * 8, (const void **)&d.bwd_rows},
+        {S.mt_tgt.data(), S.mt_tgt.size() * 4, (const void **)&d.mt_tgt},
+        {S.mt_row.data(), S.mt_row.size() * 4, (const void **)&d.mt_row},
+        {S.mt_col.data(), S.mt_col.size() * 4, (const void **)&d.mt_col},
+        {S.mt_src_ptr.data(), S.mt_src_ptr.size() * 8, (const void **)&d.mt_src_ptr},
+        {S.mt_src_k.data(), S.mt_src_k.size() * 4, (const void **)&d.mt_src_k},
+        {S.mt_src_l.data(), S.mt_src_l.size() * 4, (const void **)&d.mt_src_l},
+        {S.mt_src_u.data(), S.mt_src_u.size() * 4, (const void **)&d.mt_src_u},
+        {S.a_row_ptr.data(), S.a_row_ptr.size() * 8, (const void **)&d.a_row_ptr},
+        {S.a_cols.data(), S.a_cols.size() * 4, (const void **)&d.a_cols},
+        {S.a_val_off.data(), S.a_val_off.size() * 8, (const void **)&d.a_val_off},
+        {S.a_to_f.data(), S.a_to_f.size() * 4, (const void **)&d.a_to_f},
+    };
+    size_t total = 0;
+    for (const Item &it : items)
+        total += (it.bytes + 255) / 256 * 256 + 256;
+    HYB_CUDA(cudaMalloc(&h->arena, total));
+    std::vector<char> host(total, 0);
+    size_t off = 0;
+    for (const Item &it : items)
+    {
+        if (it.bytes)
+            std::memcpy(host.data() + off, it.src, it.bytes);
+        *it.dst = (const char *)h->arena + off;
+        off += (it.bytes + 255) / 256 * 256 + 256;
+    }
+    HYB_CUDA(cudaMemcpy(h->arena, host.data(), total, cudaMemcpyHostToDevice));
+    return HYB_SUCCESS;
+}
+
+template <typename T> int lu_smem_bytes(int m)
+{
+    return m * m * (int)sizeof(T);
+}
+
+template <typename T> int trsm_smem_bytes(int m)
+{
+    return (m * m + m * hyb::kTile) * (int)sizeof(T);
+}
+
+// Issues the whole factorization on the handle's stream (also used under capture).
+template <typename T> int enqueue_factor(hyb_system *h, T *slab, uint64_t &launches)
+{
+    const Symbolic &S = h->S;
+    const DevSym &ds = h->ds;
+    cudaStream_t st = h->stream;
+    const int optin = smem_optin();
+    k_status_init<<<1, 32, 0, st>>>(h->d_status);
+    ++launches;
+    for (int64_t l = 0; l < S.n_levels; ++l)
+    {
+        const int64_t p0 = S.lvl_ptr[l], p1 = S.lvl_ptr[l + 1];
+        const Symbolic::LevelShape &sh = S.shape[l];
+        // 1. diagonal LU
+        const int lu_bytes = lu_smem_bytes<T>(sh.max_piv);
+        if (lu_bytes <= optin)
+            hyb::k_lu<T, true><<<(unsigned)(p1 - p0), hyb::kThreads, lu_bytes, st>>>(ds, slab, p0, h->d_status);
+        else
+            hyb::k_lu<T, false><<<(unsigned)(p1 - p0), hyb::kThreads, 0, st>>>(ds, slab, p0, h->d_status);
+        ++launches;
+        // 2. upper blocks of the pivot rows
+        const int64_t n_trsm = S.trsm_pref[p1] - S.trsm_pref[p0];
+        if (n_trsm > 0)
+        {
+            dim3 grid((unsigned)n_trsm, (unsigned)((sh.max_up + hyb::kTile - 1) / hyb::kTile));
+            const int bytes = trsm_smem_bytes<T>(sh.max_piv);
+            if (bytes <= optin)
+                hyb::k_trsm<T, true><<<grid, hyb::kThreads, bytes, st>>>(ds, slab, p0, p1);
+            else
+                hyb::k_trsm<T, false><<<grid, hyb::kThreads, 0, st>>>(ds, slab, p0, p1);
+            ++launches;
+        }
+        // 3. Schur-complement updates
+        const unsigned tiles = (unsigned)(((sh.max_row + hyb::kTile - 1) / hyb::kTile) *
+                                          ((sh.max_col + hyb::kTile - 1) / hyb::kTile));
+        if (S.lvl_listed[l])
+        {
+            const int64_t q0 = S.mt_lvl_ptr[l], nq = S.mt_lvl_ptr[l + 1] - q0;
+            if (nq > 0)
+            {
+                hyb::k_update_listed<T><<<dim3((unsigned)nq, tiles), hyb::kThreads, 0, st>>>(ds, slab, q0);
+                ++launches;
+            }
+        }
+        else
+        {
+            const int64_t nu = S.upd_pref[p1] - S.upd_pref[p0];
+            if (nu > 0)
+            {
+                hyb::k_update<T><<<dim3((unsigned)nu, tiles), hyb::kThreads, 0, st>>>(ds, slab, p0, p1);
+                ++launches;
+            }
+        }
+    }
+    HYB_CUDA(cudaGetLastError());
+    return HYB_SUCCESS;
+}
+
+// Forward + backward substitution of y (type V, dof x nrhs) with the factors in `slab`.
+template <typename T, typename V> int enqueue_solve(hyb_system *h, const T *slab, V *y, V *scratch, int nrhs,
+                                                    uint64_t &launches)
+{
+    const Symbolic &S = h->S;
+    const DevSym &ds = h->ds;
+    cudaStream_t st = h->stream;
+    for (int64_t l = 0; l < S.n_levels; ++l)
+    {
+        const int64_t p0 = S.lvl_ptr[l], p1 = S.lvl_ptr[l + 1];
+        const int64_t units = S.fwd_pref[p1] - S.fwd_pref[p0];
+        if (units > 0)
+        {
+            hyb::k_fwd_partial<T, V><<<(unsigned)units, hyb::kThreads, 0, st>>>(ds, slab, y, scratch, p0, p1, nrhs);
+            ++launches;
+        }
+        const int bytes = S.shape[l].max_piv * nrhs * (int)sizeof(V);
+        hyb::k_fwd_final<T, V><<<(unsigned)(p1 - p0), hyb::kThreads, bytes, st>>>(ds, slab, y, scratch, p0, nrhs);
+        ++launches;
+    }
+    for (int64_t l = S.n_levels - 1; l >= 0; --l)
+    {
+        const int64_t p0 = S.lvl_ptr[l], p1 = S.lvl_ptr[l + 1];
+        const int64_t units = S.trsm_pref[p1] - S.trsm_pref[p0];
+        if (units == 0)
+            continue;
+        hyb::k_bwd_partial<T, V><<<(unsigned)units, hyb::kThreads, 0, st>>>(ds, slab, y, scratch, p0, p1, nrhs);
+        hyb::k_bwd_final<V><<<(unsigned)(p1 - p0), hyb::kThreads, 0, st>>>(ds, y, scratch, p0, nrhs);
+        launches += 2;
+    }
+    HYB_CUDA(cudaGetLastError());
+    return HYB_SUCCESS;
+}
+
+// Runs `body` (which enqueues work and counts launches) through a cached CUDA graph.
+template <typename F> int run_graph(hyb_system *h, std::unique_ptr<GraphExec> &slot, F body)
+{
+    if (!slot)
+    {
+        auto g = std::make_unique<GraphExec>();
+        HYB_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        uint64_t count = 0;
+        const int rc = body(count);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+        if (rc != HYB_SUCCESS)
+        {
+            if (graph)
+                cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (e != cudaSuccess)
+            return cuda_fail(e, "cudaStreamEndCapture");
+        const cudaError_t ie = cudaGraphInstantiate(&g->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess)
+            return cuda_fail(ie, "cudaGraphInstantiate");
+        g->launches = count;
+        slot = std::move(g);
+    }
+    HYB_CUDA(cudaGraphLaunch(slot->exec, h->stream));
+    h->last_launches += slot->launches;
+    return HYB_SUCCESS;
+}
+
+int ensure_solve_buffers(hyb_system *h, int64_t nrhs)
+{
+    if (h->buf_nrhs >= nrhs)
+        return HYB_SUCCESS;
+    h->free_solve_buffers();
+    const Symbolic &S = h->S;
+    const int64_t dof = S.dof_off[S.n];
+    const int64_t scr = std::max(S.max_fwd_scratch_rows, S.max_bwd_scratch_rows) * nrhs + 1;
+    h->n_norm_parts = 296;
+    HYB_CUDA(cudaMalloc(&h->d_b, dof * nrhs * sizeof(double)));
+    HYB_CUDA(cudaMalloc(&h->d_x, dof * nrhs * sizeof(double)));
+    HYB_CUDA(cudaMalloc(&h->d_r, dof * nrhs * sizeof(double)));
+    HYB_CUDA(cudaMalloc(&h->d_scr64, scr * sizeof(double)));
+    HYB_CUDA(cudaMalloc(&h->d_yf, dof * nrhs * sizeof(float)));
+    HYB_CUDA(cudaMalloc(&h->d_scr32, scr * sizeof(float)));
+    HYB_CUDA(cudaMalloc(&h->d_part, (size_t)h->n_norm_parts * nrhs * sizeof(double)));
+    HYB_CUDA(cudaMalloc(&h->d_norm, 2 * nrhs * sizeof(double)));
+    h->buf_nrhs = nrhs;
+    return HYB_SUCCESS;
+}
+
+void enqueue_sumsq(hyb_system *h, const double *v, int64_t rows, int nrhs, double *out, uint64_t &launches)
+{
+    hyb::k_sumsq_partial<<<h->n_norm_parts, hyb::kThreads, 0, h->stream>>>(v, rows, nrhs, h->d_part);
+    hyb::k_sumsq_final<<<1, 32, 0, h->stream>>>(h->d_part, h->n_norm_parts, nrhs, out);
+    launches += 2;
+}
+
+void enqueue_residual(hyb_system *h, const double *b, const double *x, double *r, int nrhs, uint64_t &launches)
+{
+    const int64_t dof = h->S.dof_off[h->S.n];
+    const int64_t warps = hyb::kThreads / 32;
+    hyb::k_residual<<<(unsigned)((dof + warps - 1) / warps), hyb::kThreads, 0, h->stream>>>(h->ds, h->d_a, b, x, r,
+                                                                                            dof, nrhs);
+    ++launches;
+}
+
+unsigned elementwise_grid(int64_t n)
+{
+    return (unsigned)std::min<int64_t>((n + hyb::kThreads - 1) / hyb::kThreads, 148 * 32);
+}
+
+int check_handle(const hyb_system *h)
+{
+    return h ? HYB_SUCCESS : HYB_INVALID_ARGUMENT;
+}
+
+} // namespace
+
+// =====================================================================================
+extern "C" {
+
+HYB_API const char *hyb_status_string(int status)
+{
+    switch (status)
+    {
+    case HYB_SUCCESS:
+        return "success";
+    case HYB_BLOCK_NOT_IN_SYSTEM:
+        return "block not in system";
+    case HYB_FAILED_ALLOC:
+        return "memory allocation failed";
+    case HYB_MAX_COLORS:
+        return "maximum number of colors exceeded";
+    case HYB_INVALID_ARGUMENT:
+        return "invalid argument";
+    case HYB_MISSING_DIAGONAL:
+        return "a row has no diagonal block";
+    case HYB_NOT_DECOMPOSED:
+        return "the system has not been decomposed yet";
+    case HYB_CUDA_ERROR:
+        return "CUDA error";
+    case HYB_NO_DEVICE:
+        return "no sm_100 CUDA device";
+    case HYB_ZERO_PIVOT:
+        return "zero pivot";
+    case HYB_NON_FINITE:
+        return "non-finite pivot";
+    case HYB_NOT_CONVERGED:
+        return "iterative refinement did not converge";
+    case HYB_TOO_LARGE:
+        return "size beyond the supported limit";
+    default:
+        return "unknown status";
+    }
+}
+
+HYB_API const char *hyb_last_cuda_error(void)
+{
+    return g_cuda_error.c_str();
+}
+
+HYB_API int hyb_version(void)
+{
+    return 100;
+}
+
+HYB_API int hyb_device_available(void)
+{
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+    {
+        cudaGetLastError();
+        return 0;
+    }
+    int dev = 0, major = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    return major == 10;
+}
+
+HYB_API int hyb_compute_ordering(uint64_t n, const uint64_t *row_ptr, const uint64_t *cols, int strategy,
+                                 uint64_t max_colors, uint64_t *ordering)
+{
+    if (n && (!row_ptr || !ordering || (!cols && row_ptr[n])))
+        return HYB_INVALID_ARGUMENT;
+    try
+    {
+        return hyb::compute_ordering(n, row_ptr, cols, strategy, max_colors, ordering);
+    }
+    catch (const std::bad_alloc &)
+    {
+        return HYB_FAILED_ALLOC;
+    }
+}
+
+HYB_API int hyb_analyze(uint64_t n, const uint64_t *block_sizes, const uint64_t *row_ptr, const uint64_t *cols,
+                        hyb_analysis *out, uint64_t *filled_row_ptr, uint64_t *filled_cols, int64_t *ops)
+{
+    if (!out || !block_sizes || !row_ptr || (!cols && n && row_ptr[n]))
+        return HYB_INVALID_ARGUMENT;
+    try
+    {
+        Symbolic S;
+        std::string err;
+        const int rc = hyb::symbolic_build((int64_t)n, block_sizes, row_ptr, cols, S, err);
+        if (rc != HYB_SUCCESS)
+        {
+            g_cuda_error = err;
+            return rc;
+        }
+        out->filled_blocks = (uint64_t)S.nnz_f();
+        out->factor_values = (uint64_t)S.factor_values;
+        out->n_levels = (uint64_t)S.n_levels;
+        out->nops = (uint64_t)(S.lcol_ptr[S.n] + S.n);
+        out->slab_bytes_fp64 = (uint64_t)S.slab_elems() * sizeof(double);
+        out->factor_flops = S.factor_flops;
+        if (filled_row_ptr)
+            for (int64_t i = 0; i <= S.n; ++i)
+                filled_row_ptr[i] = (uint64_t)S.row_ptr[i];
+        if (filled_cols)
+            for (int64_t j = 0; j < S.nnz_f(); ++j)
+                filled_cols[j] = (uint64_t)S.cols[j];
+        if (ops)
+        {
+            std::vector<int64_t> v;
+            hyb::symbolic_operations(S, v);
+            std::memcpy(ops, v.data(), v.size() * sizeof(int64_t));
+        }
+    }
+    catch (const std::bad_alloc &)
+    {
+        return HYB_FAILED_ALLOC;
+    }
+    return HYB_SUCCESS;
+}
+
+HYB_API int hyb_system_create(uint64_t n, const uint64_t *block_sizes, const uint64_t *row_ptr, const uint64_t *cols,
+                              hyb_system **out)
+{
+    if (!out || !block_sizes || !row_ptr || (!cols && n && row_ptr[n]))
+        return HYB_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (!hyb_device_available())
+        return HYB_NO_DEVICE;
+    std::unique_ptr<hyb_system> h;
+    try
+    {
+        h = std::make_unique<hyb_system>();
+        std::string err;
+        const int rc = hyb::symbolic_build((int64_t)n, block_sizes, row_ptr, cols, h->S, err);
+        if (rc != HYB_SUCCESS)
+        {
+            g_cuda_error = err;
+            return rc;
+        }
+    }
+    catch (const std::bad_alloc &)
+    {
+        return HYB_FAILED_ALLOC;
+    }
+    HYB_CUDA(cudaGetDevice(&h->device));
+    HYB_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    int rc = upload_symbolic(h.get());
+    if (rc != HYB_SUCCESS)
+        return rc;
+    HYB_CUDA(cudaMalloc(&h->d_a, std::max<int64_t>(1, h->S.a_val_off.back()) * sizeof(double)));
+    HYB_CUDA(cudaMemsetAsync(h->d_a, 0, std::max<int64_t>(1, h->S.a_val_off.back()) * sizeof(double), h->stream));
+    HYB_CUDA(cudaMalloc(&h->d_status, hyb::ST_WORDS * sizeof(int)));
+    HYB_CUDA(cudaStreamSynchronize(h->stream));
+    *out = h.release();
+    return HYB_SUCCESS;
+}
+
+HYB_API int hyb_system_destroy(hyb_system *h)
+{
+    if (!h)
+        return HYB_SUCCESS;
+    cudaStreamSynchronize(h->stream);
+    delete h;
+    return HYB_SUCCESS;
+}
+
+HYB_API int hyb_system_copy(const hyb_system *src, hyb_system **out)
+{
+    if (!src || !out)
+        return HYB_INVALID_ARGUMENT;
+    *out = nullptr;
+    std::unique_ptr<hyb_system> h;
+    try
+    {
+        h = std::make_unique<hyb_system>();
+        h->S = src->S;
+    }
+    catch (const std::bad_alloc &)
+    {
+        return HYB_FAILED_ALLOC;
+    }
+    h->device = src->device;
+    HYB_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    int rc = upload_symbolic(h.get());
+    if (rc != HYB_SUCCESS)
+        return rc;
+    const size_t a_bytes = std::max<int64_t>(1, h->S.a_val_off.back()) * sizeof(double);
+    HYB_CUDA(cudaMalloc(&h->d_a, a_bytes));
+    HYB_CUDA(cudaMalloc(&h->d_status, hyb::ST_WORDS * sizeof(int)));
+    HYB_CUDA(cudaStreamSynchronize(src->stream));
+    HYB_CUDA(cudaMemcpyAsync(h->d_a, src->d_a, a_bytes, cudaMemcpyDeviceToDevice, h->stream));
+    const size_t slab = std::max<int64_t>(1, h->S.slab_elems());
+    if (src->d_f64)
+    {
+        HYB_CUDA(cudaMalloc(&h->d_f64, slab * sizeof(double)));
+        HYB_CUDA(cudaMemcpyAsync(h->d_f64, src->d_f64, slab * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    }
+    if (src->d_f32)
+    {
+        HYB_CUDA(cudaMalloc(&h->d_f32, slab * sizeof(float)));
+        HYB_CUDA(cudaMemcpyAsync(h->d_f32, src->d_f32, slab * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+    }
+    h->factored = src->factored;
+    HYB_CUDA(cudaStreamSynchronize(h->stream));
+    *out = h.release();
+    return HYB_SUCCESS;
+}
+
+HYB_API uint64_t hyb_system_value_count(const hyb_system *h)
+{
+    return h ? (uint64_t)h->S.a_val_off.back() : 0;
+}
+
+HYB_API uint64_t hyb_system_dof(const hyb_system *h)
+{
+    return h ? (uint64_t)h->S.dof_off[h->S.n] : 0;
+}
+
+HYB_API void *hyb_system_stream(const hyb_system *h)
+{
+    return h ? (void *)h->stream : nullptr;
+}
+
+HYB_API int hyb_system_set_values(hyb_system *h, const double *values, int memory)
+{
+    if (check_handle(h) || (!values && h->S.a_val_off.back() > 0))
+        return HYB_INVALID_ARGUMENT;
+    const size_t bytes = h->S.a_val_off.back() * sizeof(double);
+    if (bytes)
+        HYB_CUDA(cudaMemcpyAsync(h->d_a, values, bytes,
+                                 memory == HYB_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                 h->stream));
+    h->factored = -1;
+    if (memory != HYB_MEMORY_DEVICE)
+        HYB_CUDA(cudaStreamSynchronize(h->stream)); // the caller may reuse a pageable buffer
+    return HYB_SUCCESS;
+}
+
+HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info)
+{
+    if (check_handle(h) || (precision != HYB_PRECISION_FP64 && precision != HYB_PRECISION_MIXED))
+        return HYB_INVALID_ARGUMENT;
+    const Symbolic &S = h->S;
+    const size_t slab = std::max<int64_t>(1, S.slab_elems());
+    static bool attrs_set = false;
+    if (!attrs_set)
+    {
+        allow_smem(hyb::k_lu<double, true>);
+        allow_smem(hyb::k_lu<float, true>);
+        allow_smem(hyb::k_trsm<double, true>);
+        allow_smem(hyb::k_trsm<float, true>);
+        allow_smem(hyb::k_fwd_final<double, double>);
+        allow_smem(hyb::k_fwd_final<float, float>);
+        allow_smem(hyb::k_dense_lu);
+        attrs_set = true;
+    }
+    h->last_launches = 0;
+    h->factored = -1;
+    const unsigned sgrid = (unsigned)std::min<int64_t>(std::max<int64_t>(1, S.nnz_a()), 148 * 16);
+    if (precision == HYB_PRECISION_FP64)
+    {
+        if (h->d_f32)
+        {
+            cudaFree(h->d_f32);
+            h->d_f32 = nullptr;
+            h->g_factor[1].reset();
+            h->g_solve.clear();
+        }
+        if (!h->d_f64)
+        {
+            HYB_CUDA(cudaMalloc(&h->d_f64, slab * sizeof(double)));
+            h->g_factor[0].reset();
+            h->g_solve.clear();
+        }
+        HYB_CUDA(cudaMemsetAsync(h->d_f64, 0, slab * sizeof(double), h->stream));
+        hyb::k_scatter<double><<<sgrid, hyb::kThreads, 0, h->stream>>>(h->ds, h->d_a, h->d_f64, S.nnz_a());
+        h->last_launches += 1;
+        const int rc = run_graph(h, h->g_factor[0],
+                                 [&](uint64_t &count) { return enqueue_factor<double>(h, h->d_f64, count); });
+        if (rc != HYB_SUCCESS)
+            return rc;
+    }
+    else
+    {
+        if (h->d_f64)
+        {
+            cudaFree(h->d_f64);
+            h->d_f64 = nullptr;
+            h->g_factor[0].reset();
+            h->g_solve.clear();
+        }
+        if (!h->d_f32)
+        {
+            HYB_CUDA(cudaMalloc(&h->d_f32, slab * sizeof(float)));
+            h->g_factor[1].reset();
+            h->g_solve.clear();
+        }
+        HYB_CUDA(cudaMemsetAsync(h->d_f32, 0, slab * sizeof(float), h->stream));
+        hyb::k_scatter<float><<<sgrid, hyb::kThreads, 0, h->stream>>>(h->ds, h->d_a, h->d_f32, S.nnz_a());
+        h->last_launches += 1;
+        const int rc =
+            run_graph(h, h->g_factor[1], [&](uint64_t &count) { return enqueue_factor<float>(h, h->d_f32, count); });
+        if (rc != HYB_SUCCESS)
+            return rc;
+    }
+    int st[hyb::ST_WORDS];
+    HYB_CUDA(cudaMemcpyAsync(st, h->d_status, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+    HYB_CUDA(cudaStreamSynchronize(h->stream));
+    h->factored = precision;
+    h->launches += h->last_launches;
+    if (info)
+    {
+        info->n_levels = (uint64_t)S.n_levels;
+        info->filled_blocks = (uint64_t)S.nnz_f();
+        info->factor_values = (uint64_t)S.factor_values;
+        info->factor_flops = S.factor_flops;
+        info->zero_pivots = (uint64_t)st[hyb::ST_ZERO_PIVOTS];
+        info->non_finite = (uint64_t)st[hyb::ST_NON_FINITE];
+        info->first_bad_pivot = st[hyb::ST_FIRST_BAD] == INT_MAX ? -1 : st[hyb::ST_FIRST_BAD];
+    }
+    return HYB_SUCCESS;
+}
+
+HYB_API int hyb_residual(hyb_system *h, const double *b, const double *x, double *r, uint64_t nrhs, int memory)
+{
+    if (check_handle(h) || !b || !x || !r || nrhs == 0 || nrhs > 1024)
+        return HYB_INVALID_ARGUMENT;
+    int rc = ensure_solve_buffers(h, (int64_t)nrhs);
+    if (rc != HYB_SUCCESS)
+        return rc;
+    const int64_t dof = h->S.dof_off[h->S.n];
+    const size_t bytes = dof * nrhs * sizeof(double);
+    const cudaMemcpyKind in = memory == HYB_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const cudaMemcpyKind outk = memory == HYB_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    HYB_CUDA(cudaMemcpyAsync(h->d_b, b, bytes, in, h->stream));
+    HYB_CUDA(cudaMemcpyAsync(h->d_x, x, bytes, in, h->stream));
+    uint64_t launches = 0;
+    enqueue_residual(h, h->d_b, h->d_x, h->d_r, (int)nrhs, launches);
+    HYB_CUDA(cudaMemcpyAsync(r, h->d_r, bytes, outk, h->stream));
+    HYB_CUDA(cudaStreamSynchronize(h->stream));
+    return HYB_SUCCESS;
+}
+
+HYB_API int hyb_solve(hyb_system *h, const double *b, double *x, uint64_t nrhs, int memory, double tol,
+                      uint32_t max_iter, hyb_solve_info *info)
+{
+    if (check_handle(h) || !b || !x || nrhs == 0 || nrhs > 1024)
+        return HYB_INVALID_ARGUMENT;
+    if (h->factored < 0)
+        return HYB_NOT_DECOMPOSED;
+    const Symbolic &S = h->S;
+    for (int64_t l = 0; l < S.n_levels; ++l)
+        if ((int64_t)S.shape[l].max_piv * (int64_t)nrhs * 8 > smem_optin())
+            return HYB_TOO_LARGE;
+    int rc = ensure_solve_buffers(h, (int64_t)nrhs);
+    if (rc != HYB_SUCCESS)
+        return rc;
+    h->last_launches = 0;
+    const int nr = (int)nrhs;
+    const int64_t dof = S.dof_off[S.n];
+    const int64_t len = dof * nr;
+    const size_t bytes = len * sizeof(double);
+    const cudaMemcpyKind in = memory == HYB_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const cudaMemcpyKind outk = memory == HYB_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    const bool want_residual = info != nullptr && tol > 0;
+    if (tol <= 0)
+        tol = 1e-12;
+    HYB_CUDA(cudaMemcpyAsync(h->d_b, b, bytes, in, h->stream));
+    uint32_t iters = 0;
+    double relres = -1;
+    int status = HYB_SUCCESS;
+    if (h->factored == HYB_PRECISION_FP64)
+    {
+        HYB_CUDA(cudaMemcpyAsync(h->d_x, h->d_b, bytes, cudaMemcpyDeviceToDevice, h->stream));
+        auto &slot = h->g_solve[{HYB_PRECISION_FP64, nr}];
+        rc = run_graph(h, slot, [&](uint64_t &count) {
+            return enqueue_solve<double, double>(h, h->d_f64, h->d_x, h->d_scr64, nr, count);
+        });
+        if (rc != HYB_SUCCESS)
+            return rc;
+        if (want_residual)
+        {
+            uint64_t cnt = 0;
+            enqueue_residual(h, h->d_b, h->d_x, h->d_r, nr, cnt);
+            enqueue_sumsq(h, h->d_r, dof, nr, h->d_norm, cnt);
+            enqueue_sumsq(h, h->d_b, dof, nr, h->d_norm + nr, cnt);
+            std::vector<double> nrm(2 * nr);
+            HYB_CUDA(cudaMemcpyAsync(nrm.data(), h->d_norm, 2 * nr * sizeof(double), cudaMemcpyDeviceToHost,
+                                     h->stream));
+            HYB_CUDA(cudaStreamSynchronize(h->stream));
+            relres = 0;
+            for (int r = 0; r < nr; ++r)
+                relres = std::max(relres, nrm[r + nr] > 0 ? std::sqrt(nrm[r] / nrm[r + nr]) : std::sqrt(nrm[r]));
+            h->last_launches += cnt;
+        }
+    }
+    else
+    {
+        // Mixed: x0 = LU32^{-1} b, then x += LU32^{-1} (b - A x) with the FP64 residual.
+        uint64_t cnt = 0;
+        auto &slot = h->g_solve[{HYB_PRECISION_MIXED, nr}];
+        auto solve32 = [&](uint64_t &count) {
+            return enqueue_solve<float, float>(h, h->d_f32, h->d_yf, h->d_scr32, nr, count);
+        };
+        hyb::k_convert<double, float><<<elementwise_grid(len), hyb::kThreads, 0, h->stream>>>(h->d_b, h->d_yf, len);
+        ++cnt;
+        rc = run_graph(h, slot, solve32);
+        if (rc != HYB_SUCCESS)
+            return rc;
+        hyb::k_convert<float, double><<<elementwise_grid(len), hyb::kThreads, 0, h->stream>>>(h->d_yf, h->d_x, len);
+        ++cnt;
+        enqueue_sumsq(h, h->d_b, dof, nr, h->d_norm + nr, cnt);
+        std::vector<double> nrm(2 * nr);
+        for (;;)
+        {
+            enqueue_residual(h, h->d_b, h->d_x, h->d_r, nr, cnt);
+            enqueue_sumsq(h, h->d_r, dof, nr, h->d_norm, cnt);
+            HYB_CUDA(cudaMemcpyAsync(nrm.data(), h->d_norm, 2 * nr * sizeof(double), cudaMemcpyDeviceToHost,
+                                     h->stream));
+            HYB_CUDA(cudaStreamSynchronize(h->stream));
+            relres = 0;
+            for (int r = 0; r < nr; ++r)
+                relres = std::max(relres, nrm[r + nr] > 0 ? std::sqrt(nrm[r] / nrm[r + nr]) : std::sqrt(nrm[r]));
+            if (!(relres > tol))
+                break;
+            if (iters >= max_iter || !std::isfinite(relres))
+            {
+                status = HYB_NOT_CONVERGED;
+                break;
+            }
+            hyb::k_convert<double, float><<<elementwise_grid(len), hyb::kThreads, 0, h->stream>>>(h->d_r, h->d_yf,
+                                                                                                len);
+            ++cnt;
+            rc = run_graph(h, slot, solve32);
+            if (rc != HYB_SUCCESS)
+                return rc;
+            hyb::k_add_correction<float><<<elementwise_grid(len), hyb::kThreads, 0, h->stream>>>(h->d_x, h->d_yf,
+                                                                                               len);
+            ++cnt;
+            ++iters;
+        }
+        h->last_launches += cnt;
+    }
+    HYB_CUDA(cudaGetLastError());
+    HYB_CUDA(cudaMemcpyAsync(x, h->d_x, bytes, outk, h->stream));
+    HYB_CUDA(cudaStreamSynchronize(h->stream));
+    h->launches += h->last_launches;
+    if (info)
+    {
+        info->iterations = iters;
+        info->relative_residual = relres;
+    }
+    return status;
+}
+
+HYB_API int hyb_row_count(const hyb_system *h, uint64_t row, uint64_t *count)
+{
+    if (check_handle(h) || row >= (uint64_t)h->S.n || !count)
+        return HYB_INVALID_ARGUMENT;
+    if (h->factored >= 0)
+        *count = (uint64_t)(h->S.row_ptr[row + 1] - h->S.row_ptr[row]);
+    else
+        *count = (uint64_t)(h->S.a_row_ptr[row + 1] - h->S.a_row_ptr[row]);
+    return HYB_SUCCESS;
+}
+
+HYB_API int hyb_row_cols(const hyb_system *h, uint64_t row, uint64_t *cols)
+{
+    if (check_handle(h) || row >= (uint64_t)h->S.n || !cols)
+        return HYB_INVALID_ARGUMENT;
+    const bool f = h->factored >= 0;
+    const int64_t b = f ? h->S.row_ptr[row] : h->S.a_row_ptr[row];
+    const int64_t e = f ? h->S.row_ptr[row + 1] : h->S.a_row_ptr[row + 1];
+    const int32_t *src = f ? h->S.cols.data() : h->S.a_cols.data();
+    for (int64_t j = b; j < e; ++j)
+        cols[j - b] = (uint64_t)src[j];
+    return HYB_SUCCESS;
+}
+
+HYB_API int hyb_get_block(const hyb_system *h, uint64_t row, uint64_t col, double *out)
+{
+    if (check_handle(h) || row >= (uint64_t)h->S.n || col >= (uint64_t)h->S.n || !out)
+        return HYB_INVALID_ARGUMENT;
+    const Symbolic &S = h->S;
+    const int64_t cnt = (int64_t)S.size[row] * S.size[col];
+    if (h->factored < 0)
+    {
+        const int32_t *b = S.a_cols.data() + S.a_row_ptr[row];
+        const int32_t *e = S.a_cols.data() + S.a_row_ptr[row + 1];
+        const int32_t *p = std::lower_bound(b, e, (int32_t)col);
+        if (p == e || *p != (int32_t)col)
+            return HYB_BLOCK_NOT_IN_SYSTEM;
+        const int64_t j = p - S.a_cols.data();
+        HYB_CUDA(cudaMemcpyAsync(out, h->d_a + S.a_val_off[j], cnt * sizeof(double), cudaMemcpyDeviceToHost,
+                                 h->stream));
+        HYB_CUDA(cudaStreamSynchronize(h->stream));
+        return HYB_SUCCESS;
+    }
+    const int64_t j = hyb::find_block(S, (int64_t)row, (int64_t)col);
+    if (j < 0)
+        return HYB_BLOCK_NOT_IN_SYSTEM;
+    if (h->factored == HYB_PRECISION_FP64)
+    {
+        HYB_CUDA(cudaMemcpyAsync(out, h->d_f64 + S.blk_off[j], cnt * sizeof(double), cudaMemcpyDeviceToHost,
+                                 h->stream));
+        HYB_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    else
+    {
+        std::vector<float> tmp(cnt);
+        HYB_CUDA(cudaMemcpyAsync(tmp.data(), h->d_f32 + S.blk_off[j], cnt * sizeof(float), cudaMemcpyDeviceToHost,
+                                 h->stream));
+        HYB_CUDA(cudaStreamSynchronize(h->stream));
+        for (int64_t i = 0; i < cnt; ++i)
+            out[i] = tmp[i];
+    }
+    return HYB_SUCCESS;
+}
+
+HYB_API int hyb_operations(const hyb_system *h, uint64_t *nops, int64_t *ops)
+{
+    if (check_handle(h) || !nops)
+        return HYB_INVALID_ARGUMENT;
+    if (h->factored < 0)
+        return HYB_NOT_DECOMPOSED;
+    try
+    {
+        std::vector<int64_t> v;
+        hyb::symbolic_operations(h->S, v);
+        *nops = v.size() / 2;
+        if (ops)
+            std::memcpy(ops, v.data(), v.size() * sizeof(int64_t));
+    }
+    catch (const std::bad_alloc &)
+    {
+        return HYB_FAILED_ALLOC;
+    }
+    return HYB_SUCCESS;
+}
+
+HYB_API uint64_t hyb_last_launch_count(const hyb_system *h)
+{
+    return h ? h->last_launches : 0;
+}
+
+HYB_API int hyb_block_lu(uint64_t m, double *a, int memory)
+{
+    if (!a || m == 0 || m > 4096)
+        return HYB_INVALID_ARGUMENT;
+    if (!hyb_device_available())
+        return HYB_NO_DEVICE;
+    const size_t bytes = m * m * sizeof(double);
+    double *d = a;
+    int *st = nullptr;
+    if (memory != HYB_MEMORY_DEVICE)
+        HYB_CUDA(cudaMalloc(&d, bytes));
+    HYB_CUDA(cudaMalloc(&st, hyb::ST_WORDS * sizeof(int)));
+    if (memory != HYB_MEMORY_DEVICE)
+        HYB_CUDA(cudaMemcpy(d, a, bytes, cudaMemcpyHostToDevice));
+    k_status_init<<<1, 32>>>(st);
+    allow_smem(hyb::k_dense_lu);
+    if ((int)bytes <= smem_optin())
+        hyb::k_dense_lu<<<1, hyb::kThreads, bytes>>>(d, (int)m, st);
+    else
+        hyb::k_dense_lu_global<<<1, hyb::kThreads>>>(d, (int)m, st);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && memory != HYB_MEMORY_DEVICE)
+        e = cudaMemcpy(a, d, bytes, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaDeviceSynchronize();
+    if (memory != HYB_MEMORY_DEVICE)
+        cudaFree(d);
+    cudaFree(st);
+    return e == cudaSuccess ? HYB_SUCCESS : cuda_fail(e, "hyb_block_lu");
+}
+
+HYB_API int hyb_block_lu_solve(uint64_t m, const double *lu, uint64_t ncols, const double *b, double *out,
+                               int memory)
+{
+    if (!lu || !b || !out || m == 0 || ncols == 0 || m > 4096)
+        return HYB_INVALID_ARGUMENT;
+    if (!hyb_device_available())
+        return HYB_NO_DEVICE;
+    const size_t lu_bytes = m * m * sizeof(double), b_bytes = m * ncols * sizeof(double);
+    double *dlu = (double *)lu, *db = out;
+    if (memory != HYB_MEMORY_DEVICE)
+    {
+        HYB_CUDA(cudaMalloc(&dlu, lu_bytes));
+        HYB_CUDA(cudaMalloc(&db, b_bytes));
+        HYB_CUDA(cudaMemcpy(dlu, lu, lu_bytes, cudaMemcpyHostToDevice));
+        HYB_CUDA(cudaMemcpy(db, b, b_bytes, cudaMemcpyHostToDevice));
+    }
+    else if (b != out)
+    {
+        HYB_CUDA(cudaMemcpy(db, b, b_bytes, cudaMemcpyDeviceToDevice));
+    }
+    hyb::k_dense_lu_solve<<<(unsigned)((ncols + hyb::kTile - 1) / hyb::kTile), hyb::kThreads>>>(dlu, (int)m, db,
+                                                                                               (int)ncols);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && memory != HYB_MEMORY_DEVICE)
+        e = cudaMemcpy(out, db, b_bytes, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaDeviceSynchronize();
+    if (memory != HYB_MEMORY_DEVICE)
+    {
+        cudaFree(dlu);
+        cudaFree(db);
+    }
+    return e == cudaSuccess ? HYB_SUCCESS : cuda_fail(e, "hyb_block_lu_solve");
+}
+
+HYB_API int hyb_block_gemm(uint64_t m, uint64_t k, uint64_t n, const double *a, const double *b, double *c,
+                           int subtract, int memory)
+{
+    if (!a || !b || !c || m == 0 || n == 0 || m > (1u << 20) || n > (1u << 20) || k > (1u << 20))
+        return HYB_INVALID_ARGUMENT;
+    if (!hyb_device_available())
+        return HYB_NO_DEVICE;
+    const size_t ab = m * k * sizeof(double), bb = k * n * sizeof(double), cb = m * n * sizeof(double);
+    double *da = (double *)a, *db = (double *)b, *dc = c;
+    if (memory != HYB_MEMORY_DEVICE)
+    {
+        HYB_CUDA(cudaMalloc(&da, ab + 8));
+        HYB_CUDA(cudaMalloc(&db, bb + 8));
+        HYB_CUDA(cudaMalloc(&dc, cb));
+        HYB_CUDA(cudaMemcpy(da, a, ab, cudaMemcpyHostToDevice));
+        HYB_CUDA(cudaMemcpy(db, b, bb, cudaMemcpyHostToDevice));
+        if (subtract)
+            HYB_CUDA(cudaMemcpy(dc, c, cb, cudaMemcpyHostToDevice));
+    }
+    const dim3 grid((unsigned)((n + hyb::kTile - 1) / hyb::kTile), (unsigned)((m + hyb::kTile - 1) / hyb::kTile));
+    hyb::k_dense_gemm<<<grid, hyb::kThreads>>>(da, db, dc, (int)m, (int)k, (int)n, subtract);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && memory != HYB_MEMORY_DEVICE)
+        e = cudaMemcpy(c, dc, cb, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaDeviceSynchronize();
+    if (memory != HYB_MEMORY_DEVICE)
+    {
+        cudaFree(da);
+        cudaFree(db);
+        cudaFree(dc);
+    }
+    return e == cudaSuccess ? HYB_SUCCESS : cuda_fail(e, "hyb_block_gemm");
+}
+
+} // extern "C"

@@ -1,0 +1,101 @@
+// hyb_internal.h - data structures shared by the host symbolic phase (hyb_symbolic.cpp),
+// the orderings (hyb_ordering.cpp) and the device side (hyb_api.cu, hyb_kernels.cuh).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace hyb
+{
+
+// Scalars of each block are padded to a multiple of this many elements in the factor
+// slab, so every block starts 256-byte aligned in FP64 and 128-byte aligned in FP32.
+constexpr int64_t kBlockAlign = 32;
+
+// Result of the symbolic phase: the reference's elimination replayed on the block
+// pattern alone. Everything the device schedule needs is precomputed here.
+struct Symbolic
+{
+    int64_t n = 0;                 // block rows/columns
+    std::vector<int32_t> size;     // [n] block sizes
+    std::vector<int64_t> dof_off;  // [n+1] scalar offsets of block rows
+
+    // Original pattern (block-CSR) and where each original block lands after fill.
+    std::vector<int64_t> a_row_ptr; // [n+1]
+    std::vector<int32_t> a_cols;    // [nnzA]
+    std::vector<int64_t> a_val_off; // [nnzA+1] unpadded value offsets (CSR order)
+    std::vector<int32_t> a_to_f;    // [nnzA] filled block index of each original block
+
+    // Filled pattern: rows hold their original blocks plus the fill of the elimination.
+    std::vector<int64_t> row_ptr;  // [n+1]
+    std::vector<int32_t> cols;     // [nnzF] ascending within a row
+    std::vector<int64_t> diag_pos; // [n] index (into cols) of the diagonal block of each row
+    std::vector<int64_t> blk_off;  // [nnzF+1] padded element offset of each block in the slab
+
+    // Strictly lower part by column: lcol_row[j], lcol_blk[j] for j in
+    // [lcol_ptr[k], lcol_ptr[k+1]) are the rows t > k holding block (t, k), ascending.
+    std::vector<int64_t> lcol_ptr; // [n+1]
+    std::vector<int32_t> lcol_row;
+    std::vector<int32_t> lcol_blk;
+
+    // Dependency levels: the pivots of level l are piv[lvl_ptr[l] .. lvl_ptr[l+1]), ascending.
+    // A pivot depends on every earlier pivot whose row or column reaches it, so within a
+    // level no pivot reads or writes another's row or column.
+    int64_t n_levels = 0;
+    std::vector<int32_t> level;     // [n] level of each block row
+    std::vector<int64_t> lvl_ptr;   // [L+1]
+    std::vector<int32_t> piv;       // [n]
+    std::vector<int64_t> trsm_pref; // [n+1] prefix (in piv order) of upper-block counts
+    std::vector<int64_t> upd_pref;  // [n+1] prefix of |lower column| * |upper row|
+    std::vector<int64_t> fwd_pref;  // [n+1] prefix of lower-row block counts (forward solve units)
+    std::vector<int64_t> fwd_rows;  // [n+1] prefix of lower-row block count * pivot size (scratch rows)
+    std::vector<int64_t> bwd_rows;  // [n+1] prefix of upper-row block count * pivot size
+
+    // Levels whose pivots share target rows get explicit target lists, each target's
+    // sources in ascending pivot order (a fixed order, no atomics).
+    std::vector<uint8_t> lvl_listed; // [L] 1 if the level's update is listed
+    std::vector<int64_t> mt_lvl_ptr; // [L+1] into the target list
+    std::vector<int32_t> mt_tgt;     // filled block index of each target
+    std::vector<int32_t> mt_row;     // target block row
+    std::vector<int32_t> mt_col;     // target block column
+    std::vector<int64_t> mt_src_ptr; // [targets+1]
+    std::vector<int32_t> mt_src_k;   // pivot of each source
+    std::vector<int32_t> mt_src_l;   // filled block (t, k)
+    std::vector<int32_t> mt_src_u;   // filled block (k, c)
+
+    // Per-level shape summary used to pick kernels and launch sizes.
+    struct LevelShape
+    {
+        int32_t max_piv = 0;  // largest pivot block
+        int32_t max_row = 0;  // largest target row block
+        int32_t max_col = 0;  // largest target column block
+        int32_t max_up = 0;   // largest upper-block column size of a pivot row
+        bool uniform64 = false; // every pivot, target row and column block is 64
+    };
+    std::vector<LevelShape> shape;
+
+    int64_t max_fwd_scratch_rows = 0; // max over levels of fwd_rows span
+    int64_t max_bwd_scratch_rows = 0;
+    double factor_flops = 0;          // exact algorithmic flops of the factorization
+    int64_t factor_values = 0;        // unpadded scalars in the filled pattern
+
+    int64_t nnz_a() const { return (int64_t)a_cols.size(); }
+    int64_t nnz_f() const { return (int64_t)cols.size(); }
+    int64_t slab_elems() const { return blk_off.empty() ? 0 : blk_off.back(); }
+};
+
+// Runs the symbolic phase. Returns a hyb_status code.
+int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, const uint64_t *cols, Symbolic &out,
+                   std::string &err);
+
+// Operation list in the reference's single-thread order (pairs row, src|-1).
+void symbolic_operations(const Symbolic &s, std::vector<int64_t> &ops);
+
+// Filled block index of (r, c), or -1.
+int64_t find_block(const Symbolic &s, int64_t r, int64_t c);
+
+int compute_ordering(uint64_t n, const uint64_t *row_ptr, const uint64_t *cols, int strategy, uint64_t max_colors,
+                     uint64_t *ordering);
+
+} // namespace hyb

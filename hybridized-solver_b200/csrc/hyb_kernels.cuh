@@ -1,0 +1,643 @@
+// hyb_kernels.cuh - device kernels of the block LU (sm_100a).
+//
+// Storage: every block of the filled pattern is a row-major tile in one slab; block j
+// starts at element blk_off[j] (256-byte aligned in FP64). The factors overwrite the
+// values in place exactly as the reference's (src/blocks.c:360-514): diagonal blocks hold
+// their unpivoted Doolittle LU, blocks right of the diagonal hold D^{-1} A (so U has
+// identity diagonal blocks), blocks left of the diagonal hold the Schur-complemented A.
+//
+// The factorization runs level by level (levels from the host symbolic phase). In a
+// level every pivot k: (1) LU of its diagonal block, (2) the upper blocks of row k are
+// solved with it, (3) every target (t, c), t in the lower column of k and c in the upper
+// row of k, receives T -= A(t,k) * U(k,c). Each target block is owned by one CTA, which
+// applies its sources in ascending pivot order: no atomics, a fixed summation order.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace hyb
+{
+
+struct DevSym
+{
+    int64_t n;
+    const int32_t *size;
+    const int64_t *dof_off;
+    const int64_t *row_ptr;
+    const int32_t *cols;
+    const int64_t *diag_pos;
+    const int64_t *blk_off;
+    const int64_t *lcol_ptr;
+    const int32_t *lcol_row;
+    const int32_t *lcol_blk;
+    const int32_t *piv;
+    const int64_t *trsm_pref;
+    const int64_t *upd_pref;
+    const int64_t *fwd_pref;
+    const int64_t *fwd_rows;
+    const int64_t *bwd_rows;
+    const int32_t *mt_tgt;
+    const int32_t *mt_row;
+    const int32_t *mt_col;
+    const int64_t *mt_src_ptr;
+    const int32_t *mt_src_k;
+    const int32_t *mt_src_l;
+    const int32_t *mt_src_u;
+    const int64_t *a_row_ptr;
+    const int32_t *a_cols;
+    const int64_t *a_val_off;
+    const int32_t *a_to_f;
+};
+
+// Status words written by the factorization (host reads them after a decompose).
+enum
+{
+    ST_ZERO_PIVOTS = 0,
+    ST_NON_FINITE = 1,
+    ST_FIRST_BAD = 2, // atomicMin of the block row, INT32_MAX if none
+    ST_WORDS = 4
+};
+
+constexpr int kThreads = 256;
+constexpr int kTile = 64;  // output tile edge of the generic update kernel
+constexpr int kTileK = 16; // K chunk staged through shared memory
+
+// Largest p with pref[p] <= u in [lo, hi) (pref is non-decreasing); work units are
+// assigned to pivots through these prefix arrays.
+__device__ __forceinline__ int64_t find_owner(const int64_t *pref, int64_t lo, int64_t hi, int64_t u)
+{
+    while (hi - lo > 1)
+    {
+        const int64_t mid = (lo + hi) >> 1;
+        if (pref[mid] <= u)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Index of column c in the sorted range cols[b, e) (the caller guarantees presence).
+__device__ __forceinline__ int64_t find_col(const int32_t *cols, int64_t b, int64_t e, int32_t c)
+{
+    while (b < e)
+    {
+        const int64_t mid = (b + e) >> 1;
+        if (cols[mid] < c)
+            b = mid + 1;
+        else
+            e = mid;
+    }
+    return b;
+}
+
+template <typename T> __device__ __forceinline__ bool finite_val(T v)
+{
+    return isfinite(v);
+}
+
+// ----------------------------------------------------------------------------------
+// Values -> slab: original blocks are copied (and converted) to their filled slots.
+template <typename T>
+__global__ void k_scatter(DevSym S, const double *__restrict__ a, T *__restrict__ slab, int64_t nnz_a)
+{
+    for (int64_t b = blockIdx.x; b < nnz_a; b += gridDim.x)
+    {
+        const int64_t src = S.a_val_off[b];
+        const int64_t cnt = S.a_val_off[b + 1] - src;
+        T *dst = slab + S.blk_off[S.a_to_f[b]];
+        for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x)
+            dst[i] = (T)a[src + i];
+    }
+}
+
+// ----------------------------------------------------------------------------------
+// Unpivoted LU of one m x m block held at `a` (shared or global memory), right-looking:
+// for each pivot i the column below it is divided by the pivot, then the trailing block
+// receives the rank-1 update. Same factors as matrix_lu_decompose (src/blocks.c:254-283)
+// up to rounding; a zero pivot divides by zero as there.
+template <typename T>
+__device__ void lu_inplace(T *a, int m, int lda, int *status, int row_id)
+{
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int i = 0; i < m; ++i)
+    {
+        const T p = a[i * lda + i];
+        if (tid == 0 && status != nullptr && (p == T(0) || !finite_val(p)))
+        {
+            atomicAdd(status + (p == T(0) ? ST_ZERO_PIVOTS : ST_NON_FINITE), 1);
+            atomicMin(status + ST_FIRST_BAD, row_id);
+        }
+        for (int j = i + 1 + tid; j < m; j += nt)
+            a[j * lda + i] = a[j * lda + i] / p;
+        __syncthreads();
+        const int w = m - i - 1;
+        for (int idx = tid; idx < w * w; idx += nt)
+        {
+            const int r = i + 1 + idx / w, c = i + 1 + idx % w;
+            a[r * lda + c] -= a[r * lda + i] * a[i * lda + c];
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T, bool kShared>
+__global__ void __launch_bounds__(kThreads) k_lu(DevSym S, T *__restrict__ slab, int64_t p0, int *status)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int64_t k = S.piv[p0 + blockIdx.x];
+    const int m = S.size[k];
+    T *g = slab + S.blk_off[S.diag_pos[k]];
+    if constexpr (kShared)
+    {
+        T *a = reinterpret_cast<T *>(smem_raw);
+        for (int i = threadIdx.x; i < m * m; i += blockDim.x)
+            a[i] = g[i];
+        __syncthreads();
+        lu_inplace(a, m, m, status, (int)k);
+        for (int i = threadIdx.x; i < m * m; i += blockDim.x)
+            g[i] = a[i];
+    }
+    else
+    {
+        lu_inplace(g, m, m, status, (int)k);
+    }
+}
+
+// ----------------------------------------------------------------------------------
+// B <- D^{-1} B for a column strip of an upper block of the pivot row, with D the
+// factored diagonal block (unit L then U): block_system_apply_diagonal_inverse
+// (src/blocks.c:516-539). Right-looking over the strip's rows.
+template <typename T>
+__device__ void lu_solve_strip(const T *d, int ldd, T *b, int ldb, int m, int w)
+{
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int i = 0; i < m - 1; ++i)
+    {
+        const int rows = m - i - 1;
+        for (int idx = tid; idx < rows * w; idx += nt)
+        {
+            const int r = i + 1 + idx / w, c = idx % w;
+            b[r * ldb + c] -= d[r * ldd + i] * b[i * ldb + c];
+        }
+        __syncthreads();
+    }
+    for (int i = m - 1; i >= 0; --i)
+    {
+        for (int c = tid; c < w; c += nt)
+            b[i * ldb + c] = b[i * ldb + c] / d[i * ldd + i];
+        __syncthreads();
+        for (int idx = tid; idx < i * w; idx += nt)
+        {
+            const int r = idx / w, c = idx % w;
+            b[r * ldb + c] -= d[r * ldd + i] * b[i * ldb + c];
+        }
+        __syncthreads();
+    }
+}
+
+// grid.x: upper blocks of the level's pivots, grid.y: 64-column strips.
+template <typename T, bool kShared>
+__global__ void __launch_bounds__(kThreads) k_trsm(DevSym S, T *__restrict__ slab, int64_t p0, int64_t p1)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int64_t u = S.trsm_pref[p0] + blockIdx.x;
+    const int64_t p = find_owner(S.trsm_pref, p0, p1, u);
+    const int64_t k = S.piv[p];
+    const int64_t blk = S.diag_pos[k] + 1 + (u - S.trsm_pref[p]);
+    const int m = S.size[k];
+    const int nc = S.size[S.cols[blk]];
+    const int c0 = blockIdx.y * kTile;
+    if (c0 >= nc)
+        return;
+    const int w = min(kTile, nc - c0);
+    const T *gd = slab + S.blk_off[S.diag_pos[k]];
+    T *gb = slab + S.blk_off[blk] + c0;
+    if constexpr (kShared)
+    {
+        T *d = reinterpret_cast<T *>(smem_raw);
+        T *b = d + m * m;
+        for (int i = threadIdx.x; i < m * m; i += blockDim.x)
+            d[i] = gd[i];
+        for (int i = threadIdx.x; i < m * w; i += blockDim.x)
+            b[i] = gb[(i / w) * nc + i % w];
+        __syncthreads();
+        lu_solve_strip(d, m, b, w, m, w);
+        for (int i = threadIdx.x; i < m * w; i += blockDim.x)
+            gb[(i / w) * nc + i % w] = b[i];
+    }
+    else
+    {
+        lu_solve_strip(gd, m, gb, nc, m, w);
+    }
+}
+
+// ----------------------------------------------------------------------------------
+// Generic tiled update of one 64x64 output tile: acc -= A * B with A (M x K, lda) and
+// B (K x N, ldb), both row-major; 256 threads, 4x4 outputs each.
+template <typename T> struct TileAcc
+{
+    T v[4][4];
+};
+
+template <typename T>
+__device__ __forceinline__ void tile_load(TileAcc<T> &acc, const T *c, int ldc, int M, int N)
+{
+    const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            const int r = ty * 4 + i, cc = tx * 4 + j;
+            acc.v[i][j] = (r < M && cc < N) ? c[r * ldc + cc] : T(0);
+        }
+}
+
+template <typename T>
+__device__ __forceinline__ void tile_store(const TileAcc<T> &acc, T *c, int ldc, int M, int N)
+{
+    const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            const int r = ty * 4 + i, cc = tx * 4 + j;
+            if (r < M && cc < N)
+                c[r * ldc + cc] = acc.v[i][j];
+        }
+}
+
+template <typename T>
+__device__ __forceinline__ void tile_sub_ab(TileAcc<T> &acc, const T *__restrict__ a, int lda,
+                                            const T *__restrict__ b, int ldb, int M, int N, int K, T *sa, T *sb)
+{
+    const int tid = threadIdx.x;
+    const int ty = tid / 16, tx = tid % 16;
+    for (int k0 = 0; k0 < K; k0 += kTileK)
+    {
+        for (int idx = tid; idx < kTile * kTileK; idx += kThreads)
+        {
+            const int r = idx / kTileK, kk = idx % kTileK;
+            sa[kk * kTile + r] = (r < M && k0 + kk < K) ? a[r * lda + k0 + kk] : T(0);
+            const int kr = idx / kTile, cc = idx % kTile;
+            sb[kr * kTile + cc] = (cc < N && k0 + kr < K) ? b[(k0 + kr) * ldb + cc] : T(0);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < kTileK; ++kk)
+        {
+            T av[4], bv[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                av[i] = sa[kk * kTile + ty * 4 + i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                bv[j] = sb[kk * kTile + tx * 4 + j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    acc.v[i][j] -= av[i] * bv[j];
+        }
+        __syncthreads();
+    }
+}
+
+// Update of a level whose pivots touch disjoint target rows. grid.x enumerates
+// (pivot, lower row i, upper column j) through upd_pref; grid.y the 64x64 tiles.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_update(DevSym S, T *__restrict__ slab, int64_t p0, int64_t p1)
+{
+    __shared__ __align__(16) T sa[kTile * kTileK];
+    __shared__ __align__(16) T sb[kTile * kTileK];
+    const int64_t u = S.upd_pref[p0] + blockIdx.x;
+    const int64_t p = find_owner(S.upd_pref, p0, p1, u);
+    const int64_t k = S.piv[p];
+    const int64_t local = u - S.upd_pref[p];
+    const int64_t n_up = S.row_ptr[k + 1] - S.diag_pos[k] - 1;
+    const int64_t li = S.lcol_ptr[k] + local / n_up;
+    const int64_t bu = S.diag_pos[k] + 1 + local % n_up;
+    const int32_t t = S.lcol_row[li];
+    const int32_t c = S.cols[bu];
+    const int M = S.size[t], N = S.size[c], K = S.size[k];
+    const int tn = (N + kTile - 1) / kTile;
+    const int tm = (M + kTile - 1) / kTile;
+    if ((int)blockIdx.y >= tm * tn)
+        return;
+    const int r0 = (blockIdx.y / tn) * kTile, c0 = (blockIdx.y % tn) * kTile;
+    const int64_t tgt = find_col(S.cols, S.row_ptr[t], S.row_ptr[t + 1], c);
+    T *cb = slab + S.blk_off[tgt] + (int64_t)r0 * N + c0;
+    const T *ab = slab + S.blk_off[S.lcol_blk[li]] + (int64_t)r0 * K;
+    const T *bb = slab + S.blk_off[bu] + c0;
+    TileAcc<T> acc;
+    tile_load(acc, cb, N, M - r0, N - c0);
+    tile_sub_ab(acc, ab, K, bb, N, M - r0, N - c0, K, sa, sb);
+    tile_store(acc, cb, N, M - r0, N - c0);
+}
+
+// Update of a level whose pivots share target rows: one CTA per listed target, its
+// sources applied in ascending pivot order.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_update_listed(DevSym S, T *__restrict__ slab, int64_t q0)
+{
+    __shared__ __align__(16) T sa[kTile * kTileK];
+    __shared__ __align__(16) T sb[kTile * kTileK];
+    const int64_t q = q0 + blockIdx.x;
+    const int32_t t = S.mt_row[q], c = S.mt_col[q];
+    const int M = S.size[t], N = S.size[c];
+    const int tn = (N + kTile - 1) / kTile;
+    const int tm = (M + kTile - 1) / kTile;
+    if ((int)blockIdx.y >= tm * tn)
+        return;
+    const int r0 = (blockIdx.y / tn) * kTile, c0 = (blockIdx.y % tn) * kTile;
+    T *cb = slab + S.blk_off[S.mt_tgt[q]] + (int64_t)r0 * N + c0;
+    TileAcc<T> acc;
+    tile_load(acc, cb, N, M - r0, N - c0);
+    for (int64_t s = S.mt_src_ptr[q]; s < S.mt_src_ptr[q + 1]; ++s)
+    {
+        const int K = S.size[S.mt_src_k[s]];
+        const T *ab = slab + S.blk_off[S.mt_src_l[s]] + (int64_t)r0 * K;
+        const T *bb = slab + S.blk_off[S.mt_src_u[s]] + c0;
+        tile_sub_ab(acc, ab, K, bb, N, M - r0, N - c0, K, sa, sb);
+    }
+    tile_store(acc, cb, N, M - r0, N - c0);
+}
+
+// ----------------------------------------------------------------------------------
+// Solve. Vectors are dof x nrhs row-major in type V.
+//
+// Partial products of one block against the vector: out[i][r] = sum_q blk[i][q] * y[q][r]
+// for an m x K block; one warp per output row.
+template <typename T, typename V>
+__device__ __forceinline__ void block_gemv(const T *__restrict__ blk, int m, int K, const V *__restrict__ y,
+                                           V *__restrict__ out, int nrhs)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int i = warp; i < m; i += nw)
+    {
+        for (int r = 0; r < nrhs; ++r)
+        {
+            V s = 0;
+            for (int q = lane; q < K; q += 32)
+                s += (V)blk[(int64_t)i * K + q] * y[(int64_t)q * nrhs + r];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+                s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0)
+                out[(int64_t)i * nrhs + r] = s;
+        }
+    }
+}
+
+// Forward partials: unit u = one lower block (k, s) of a pivot in [p0, p1).
+template <typename T, typename V>
+__global__ void __launch_bounds__(kThreads)
+    k_fwd_partial(DevSym S, const T *__restrict__ slab, const V *__restrict__ y, V *__restrict__ scratch, int64_t p0,
+                  int64_t p1, int nrhs)
+{
+    const int64_t u = S.fwd_pref[p0] + blockIdx.x;
+    const int64_t p = find_owner(S.fwd_pref, p0, p1, u);
+    const int64_t k = S.piv[p];
+    const int64_t j = u - S.fwd_pref[p];
+    const int64_t blk = S.row_ptr[k] + j;
+    const int32_t s = S.cols[blk];
+    const int m = S.size[k];
+    const int64_t row = S.fwd_rows[p] - S.fwd_rows[p0] + j * m;
+    block_gemv(slab + S.blk_off[blk], m, S.size[s], y + S.dof_off[s] * nrhs, scratch + row * nrhs, nrhs);
+}
+
+// Forward finish of pivot k: y_k <- D_k^{-1} (y_k - sum of its partials), partials summed
+// in ascending source order (block_system_apply_operations, src/blocks.c:729-769).
+template <typename T, typename V>
+__global__ void __launch_bounds__(kThreads)
+    k_fwd_final(DevSym S, const T *__restrict__ slab, V *__restrict__ y, const V *__restrict__ scratch, int64_t p0,
+                int nrhs)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int64_t p = p0 + blockIdx.x;
+    const int64_t k = S.piv[p];
+    const int m = S.size[k];
+    const int64_t nparts = S.diag_pos[k] - S.row_ptr[k];
+    V *acc = reinterpret_cast<V *>(smem_raw); // m * nrhs
+    V *yk = y + S.dof_off[k] * nrhs;
+    const V *part = scratch + (S.fwd_rows[p] - S.fwd_rows[p0]) * nrhs;
+    for (int i = threadIdx.x; i < m * nrhs; i += blockDim.x)
+    {
+        V v = yk[i];
+        for (int64_t j = 0; j < nparts; ++j)
+            v -= part[j * m * nrhs + i];
+        acc[i] = v;
+    }
+    __syncthreads();
+    const T *d = slab + S.blk_off[S.diag_pos[k]];
+    // unit lower, then upper; one warp per right-hand side
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int r = warp; r < nrhs; r += nw)
+    {
+        for (int i = 0; i < m; ++i)
+        {
+            const V xi = acc[i * nrhs + r];
+            __syncwarp();
+            for (int q = i + 1 + lane; q < m; q += 32)
+                acc[q * nrhs + r] -= (V)d[(int64_t)q * m + i] * xi;
+            __syncwarp();
+        }
+        for (int i = m - 1; i >= 0; --i)
+        {
+            V xi = acc[i * nrhs + r] / (V)d[(int64_t)i * m + i];
+            __syncwarp();
+            if (lane == 0)
+                acc[i * nrhs + r] = xi;
+            for (int q = lane; q < i; q += 32)
+                acc[q * nrhs + r] -= (V)d[(int64_t)q * m + i] * xi;
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < m * nrhs; i += blockDim.x)
+        yk[i] = acc[i];
+}
+
+// Backward partials: unit u = one upper block (k, c).
+template <typename T, typename V>
+__global__ void __launch_bounds__(kThreads)
+    k_bwd_partial(DevSym S, const T *__restrict__ slab, const V *__restrict__ y, V *__restrict__ scratch, int64_t p0,
+                  int64_t p1, int nrhs)
+{
+    const int64_t u = S.trsm_pref[p0] + blockIdx.x;
+    const int64_t p = find_owner(S.trsm_pref, p0, p1, u);
+    const int64_t k = S.piv[p];
+    const int64_t j = u - S.trsm_pref[p];
+    const int64_t blk = S.diag_pos[k] + 1 + j;
+    const int32_t c = S.cols[blk];
+    const int m = S.size[k];
+    const int64_t row = S.bwd_rows[p] - S.bwd_rows[p0] + j * m;
+    block_gemv(slab + S.blk_off[blk], m, S.size[c], y + S.dof_off[c] * nrhs, scratch + row * nrhs, nrhs);
+}
+
+// Backward finish: y_k -= sum of the partials of its upper blocks
+// (block_system_solve_u, src/blocks.c:771-800).
+template <typename V>
+__global__ void __launch_bounds__(kThreads)
+    k_bwd_final(DevSym S, V *__restrict__ y, const V *__restrict__ scratch, int64_t p0, int nrhs)
+{
+    const int64_t p = p0 + blockIdx.x;
+    const int64_t k = S.piv[p];
+    const int m = S.size[k];
+    const int64_t nparts = S.row_ptr[k + 1] - S.diag_pos[k] - 1;
+    V *yk = y + S.dof_off[k] * nrhs;
+    const V *part = scratch + (S.bwd_rows[p] - S.bwd_rows[p0]) * nrhs;
+    for (int i = threadIdx.x; i < m * nrhs; i += blockDim.x)
+    {
+        V v = yk[i];
+        for (int64_t j = 0; j < nparts; ++j)
+            v -= part[j * m * nrhs + i];
+        yk[i] = v;
+    }
+}
+
+// ----------------------------------------------------------------------------------
+// FP64 residual r = b - A x over the original pattern; one warp per scalar row.
+__global__ void __launch_bounds__(kThreads)
+    k_residual(DevSym S, const double *__restrict__ a, const double *__restrict__ b, const double *__restrict__ x,
+               double *__restrict__ r, int64_t dof, int nrhs)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (g >= dof)
+        return;
+    // block row owning scalar row g
+    int64_t lo = 0, hi = S.n;
+    while (hi - lo > 1)
+    {
+        const int64_t mid = (lo + hi) >> 1;
+        if (S.dof_off[mid] <= g)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    const int64_t br = lo;
+    const int64_t i = g - S.dof_off[br];
+    for (int rr = 0; rr < nrhs; ++rr)
+    {
+        double s = 0;
+        for (int64_t j = S.a_row_ptr[br]; j < S.a_row_ptr[br + 1]; ++j)
+        {
+            const int32_t c = S.a_cols[j];
+            const int nc = S.size[c];
+            const double *row = a + S.a_val_off[j] + i * nc;
+            const double *xc = x + S.dof_off[c] * nrhs;
+            for (int q = lane; q < nc; q += 32)
+                s += row[q] * xc[(int64_t)q * nrhs + rr];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0)
+            r[g * nrhs + rr] = b[g * nrhs + rr] - s;
+    }
+}
+
+// Per-column sums of squares, deterministic two-pass: pass 1 writes one partial per CTA.
+__global__ void __launch_bounds__(kThreads)
+    k_sumsq_partial(const double *__restrict__ v, int64_t rows, int nrhs, double *__restrict__ partial)
+{
+    __shared__ double red[kThreads];
+    for (int r = 0; r < nrhs; ++r)
+    {
+        double s = 0;
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x)
+        {
+            const double x = v[i * nrhs + r];
+            s += x * x;
+        }
+        red[threadIdx.x] = s;
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1)
+        {
+            if ((int)threadIdx.x < o)
+                red[threadIdx.x] += red[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0)
+            partial[(int64_t)blockIdx.x * nrhs + r] = red[0];
+        __syncthreads();
+    }
+}
+
+__global__ void k_sumsq_final(const double *__restrict__ partial, int nparts, int nrhs, double *__restrict__ out)
+{
+    for (int r = threadIdx.x; r < nrhs; r += blockDim.x)
+    {
+        double s = 0;
+        for (int i = 0; i < nparts; ++i)
+            s += partial[(int64_t)i * nrhs + r];
+        out[r] = s;
+    }
+}
+
+template <typename A, typename B> __global__ void k_convert(const A *__restrict__ src, B *__restrict__ dst, int64_t n)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = (B)src[i];
+}
+
+// x += d (d in the correction precision).
+template <typename V> __global__ void k_add_correction(double *__restrict__ x, const V *__restrict__ d, int64_t n)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] += (double)d[i];
+}
+
+// Single dense block kernels for the fine-grained surface.
+__global__ void k_dense_lu(double *a, int m, int *status)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *s = reinterpret_cast<double *>(smem_raw);
+    for (int i = threadIdx.x; i < m * m; i += blockDim.x)
+        s[i] = a[i];
+    __syncthreads();
+    lu_inplace(s, m, m, status, 0);
+    for (int i = threadIdx.x; i < m * m; i += blockDim.x)
+        a[i] = s[i];
+}
+
+__global__ void k_dense_lu_global(double *a, int m, int *status)
+{
+    lu_inplace(a, m, m, status, 0);
+}
+
+// c = a * b or c -= a * b for one dense row-major product; grid: 64x64 output tiles.
+__global__ void __launch_bounds__(kThreads) k_dense_gemm(const double *a, const double *b, double *c, int m, int k,
+                                                         int n, int subtract)
+{
+    __shared__ __align__(16) double sa[kTile * kTileK];
+    __shared__ __align__(16) double sb[kTile * kTileK];
+    const int r0 = blockIdx.y * kTile, c0 = blockIdx.x * kTile;
+    TileAcc<double> acc;
+    if (subtract)
+        tile_load(acc, c + (int64_t)r0 * n + c0, n, m - r0, n - c0);
+    else
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j)
+                acc.v[i][j] = 0;
+    tile_sub_ab(acc, a + (int64_t)r0 * k, k, b + c0, n, m - r0, n - c0, k, sa, sb);
+    if (!subtract)
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j)
+                acc.v[i][j] = -acc.v[i][j];
+    tile_store(acc, c + (int64_t)r0 * n + c0, n, m - r0, n - c0);
+}
+
+// One strip of 64 columns per CTA.
+__global__ void k_dense_lu_solve(const double *lu, int m, double *b, int ncols)
+{
+    const int c0 = blockIdx.x * kTile;
+    const int w = min(kTile, ncols - c0);
+    lu_solve_strip(lu, m, b + c0, ncols, m, w);
+}
+
+} // namespace hyb

@@ -1,0 +1,208 @@
+/*
+ * hybsol_b200.h - C ABI of the B200-native block-sparse LU (decompose + solve).
+ *
+ * A drop-in for the hot path of j4nr0th/hybridized-solver: the reference's
+ * `BlockSystem.decompose()` / `BlockSystem.solve()` (src/block_system.c:1143-1335),
+ * whose core is the hidden-visibility "block_system interface" of src/blocks.h:65-131.
+ * That interface is not exported by the reference (MODULE_INTERNAL, src/module.h:3-5);
+ * the entry points below are the exported equivalents a binding calls instead. The
+ * package's CPython extension `hybsol._mod` binds exactly these.
+ *
+ * Conventions
+ *  - Plain C types only: no CUDA or torch types cross this boundary.
+ *  - Block-CSR patterns: `row_ptr[n+1]`, `cols[row_ptr[n]]`, columns strictly ascending in
+ *    each row, every row holding its diagonal block. Block (r, c) is `sizes[r] x sizes[c]`
+ *    and its values are row-major; a value array holds the blocks in CSR order.
+ *  - Dense vectors are `dof x nrhs`, row-major (C-contiguous `(dof, nrhs)`; nrhs = 1 is the
+ *    reference's 1-D vector).
+ *  - Every call returns a `hyb_status` (0 = success). The first four codes are the
+ *    reference's `result_t` (src/module.h:67-73) with the same values.
+ *  - One handle is used by one host thread at a time (the reference has no per-object
+ *    lock either, src/block_system.c); its device work is ordered on the handle's stream.
+ */
+#ifndef HYBSOL_B200_H
+#define HYBSOL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HYB_API __attribute__((visibility("default")))
+
+typedef enum
+{
+    HYB_SUCCESS = 0,             /* RESULT_SUCCESS */
+    HYB_BLOCK_NOT_IN_SYSTEM = 1, /* RESULT_BLOCK_NOT_IN_SYSTEM */
+    HYB_FAILED_ALLOC = 2,        /* RESULT_FAILED_ALLOC (host or device memory) */
+    HYB_MAX_COLORS = 3,          /* RESULT_MAX_COLORS */
+    HYB_INVALID_ARGUMENT = 16,   /* bad index, size, pattern or pointer */
+    HYB_MISSING_DIAGONAL = 17,   /* a row has no diagonal block */
+    HYB_NOT_DECOMPOSED = 18,     /* solve/factor access before decompose */
+    HYB_CUDA_ERROR = 19,         /* a CUDA runtime call failed (see hyb_last_cuda_error) */
+    HYB_NO_DEVICE = 20,          /* no usable sm_100 device */
+    HYB_ZERO_PIVOT = 21,         /* a diagonal-block pivot was exactly zero */
+    HYB_NON_FINITE = 22,         /* a pivot or factor entry is inf/nan */
+    HYB_NOT_CONVERGED = 23,      /* iterative refinement missed its tolerance */
+    HYB_TOO_LARGE = 24           /* request beyond a documented size limit */
+} hyb_status;
+
+typedef enum
+{
+    HYB_PRECISION_FP64 = 0, /* plain form: FP64 factors and solves (the drop-in) */
+    HYB_PRECISION_MIXED = 1 /* FP32 factors (BF16x3 tensor-core updates) + FP64 refinement */
+} hyb_precision;
+
+typedef enum
+{
+    HYB_ORDERING_FIRST = 0, /* src/blocks.c:918 block_system_compute_ordering_first */
+    HYB_ORDERING_GREEDY = 1, /* src/blocks.c:966 block_system_compute_ordering_greedy */
+    HYB_ORDERING_BALANCED = 2 /* src/blocks.c:1054 block_system_compute_ordering_balanced */
+} hyb_ordering_strategy;
+
+typedef enum
+{
+    HYB_MEMORY_HOST = 0,  /* pointer is host memory (pageable or pinned) */
+    HYB_MEMORY_DEVICE = 1 /* pointer is device memory of the handle's device */
+} hyb_memory;
+
+typedef struct hyb_system hyb_system;
+
+typedef struct
+{
+    uint64_t n_levels;         /* stages of the dependency schedule */
+    uint64_t filled_blocks;    /* stored blocks after fill */
+    uint64_t factor_values;    /* scalars in the factors (unpadded) */
+    double factor_flops;       /* exact algorithmic flops of the factorization */
+    uint64_t zero_pivots;      /* diagonal pivots that were exactly zero */
+    uint64_t non_finite;       /* diagonal pivots that came out inf/nan */
+    int64_t first_bad_pivot;   /* lowest block row with a bad pivot, -1 if none */
+} hyb_decompose_info;
+
+typedef struct
+{
+    uint32_t iterations;       /* refinement steps taken (0 for the plain form) */
+    double relative_residual;  /* max over columns of ||b - A x||_2 / ||b||_2 (FP64), -1 if not computed */
+} hyb_solve_info;
+
+/* Library ----------------------------------------------------------------------- */
+
+HYB_API const char *hyb_status_string(int status);
+HYB_API const char *hyb_last_cuda_error(void);
+HYB_API int hyb_version(void);
+/* Non-zero when a device of compute capability 10.x is visible. */
+HYB_API int hyb_device_available(void);
+
+/* Ordering (host, integer, bit-exact) -------------------------------------------- */
+
+/* Coloring ordering of a block-CSR pattern: `ordering[i]` is the new index of block i.
+ * Replaces block_system_compute_ordering_{first,greedy,balanced} + order_from_colors
+ * (src/blocks.c:802-1141) as called by compute_reordering (src/block_system.c:1693-1788).
+ * `max_colors` = 0 means "the largest row length" (src/block_system.c:1725-1733). */
+HYB_API int hyb_compute_ordering(uint64_t n, const uint64_t *row_ptr, const uint64_t *cols, int strategy,
+                                 uint64_t max_colors, uint64_t *ordering);
+
+/* Host-only symbolic analysis ---------------------------------------------------- */
+
+typedef struct
+{
+    uint64_t filled_blocks;   /* blocks after fill */
+    uint64_t factor_values;   /* scalars after fill (unpadded) */
+    uint64_t n_levels;        /* stages of the dependency schedule */
+    uint64_t nops;            /* operations() entries: lower blocks + block rows */
+    uint64_t slab_bytes_fp64; /* device bytes of the FP64 factor slab (blocks padded to 256 B) */
+    double factor_flops;      /* exact algorithmic flops of the factorization */
+} hyb_analysis;
+
+/* Runs the symbolic phase on the host alone (no GPU needed): the fill the reference's
+ * elimination creates (src/blocks.c:557-727 in the order of src/blocks.c:360-514), the
+ * schedule statistics, and optionally the filled pattern (`filled_row_ptr[n+1]`,
+ * `filled_cols[filled_blocks]`) and the operation list in the reference's single-thread
+ * order (`ops[2*nops]`, as hyb_operations). Pass NULL arrays to query the sizes first. */
+HYB_API int hyb_analyze(uint64_t n, const uint64_t *block_sizes, const uint64_t *row_ptr, const uint64_t *cols,
+                        hyb_analysis *out, uint64_t *filled_row_ptr, uint64_t *filled_cols, int64_t *ops);
+
+/* System lifecycle ---------------------------------------------------------------- */
+
+/* Creates a system on the current CUDA device with a fixed block pattern and runs the
+ * symbolic phase: the fill of the reference's elimination (src/blocks.c:557-727 applied
+ * in the order of src/blocks.c:360-514), the dependency levels and the per-level work
+ * lists. Replaces BlockSystem(*sizes) + add_block pattern building
+ * (src/block_system.c:59-134, src/blocks.c:3-75). Values start at zero. */
+HYB_API int hyb_system_create(uint64_t n, const uint64_t *block_sizes, const uint64_t *row_ptr,
+                              const uint64_t *cols, hyb_system **out);
+HYB_API int hyb_system_destroy(hyb_system *sys);
+/* Deep copy (pattern, values, factors, op list): BlockSystem.copy (src/block_system.c:1343-1444). */
+HYB_API int hyb_system_copy(const hyb_system *sys, hyb_system **out);
+
+/* Loads the values of the original pattern (CSR order). Clears any decomposition, so
+ * the same handle can be factored again with new values (a refactorization). */
+HYB_API int hyb_system_set_values(hyb_system *sys, const double *values, int memory);
+/* Size of the value array hyb_system_set_values expects (scalars). */
+HYB_API uint64_t hyb_system_value_count(const hyb_system *sys);
+/* Total unknowns (sum of block sizes). */
+HYB_API uint64_t hyb_system_dof(const hyb_system *sys);
+/* The handle's CUDA stream (a cudaStream_t as void*), for callers that time or order work. */
+HYB_API void *hyb_system_stream(const hyb_system *sys);
+
+/* Decomposition and solve -------------------------------------------------------- */
+
+/* Factors the system in the given precision: replaces block_system_decompose
+ * (src/blocks.c:360-514; binding src/block_system.c:1143-1187). The plain form computes
+ * the reference's factors (unpivoted; U with identity diagonal blocks, diagonal blocks
+ * holding their own Doolittle LU, lower blocks the Schur-complemented A) to rounding.
+ * A zero pivot is not an error, as in the reference (the factor gets inf/nan); it is
+ * counted in `info`. `info` may be NULL. */
+HYB_API int hyb_decompose(hyb_system *sys, int precision, hyb_decompose_info *info);
+
+/* Solves A x = b for `nrhs` right-hand sides: replaces block_system_apply_operations +
+ * block_system_solve_u (src/blocks.c:729-800; binding src/block_system.c:1259-1335).
+ * `b` and `x` may alias. In the mixed form the solve iterates refinement until
+ * ||b - A x|| / ||b|| <= tol (FP64 residual against the original A) or `max_iter` steps;
+ * tol <= 0 selects 1e-12. In the plain form tol/max_iter are ignored and the residual is
+ * only computed when `info` is non-NULL and `tol` > 0. Returns HYB_NOT_CONVERGED (with
+ * x holding the last iterate) when refinement misses the tolerance. */
+HYB_API int hyb_solve(hyb_system *sys, const double *b, double *x, uint64_t nrhs, int memory, double tol,
+                      uint32_t max_iter, hyb_solve_info *info);
+
+/* FP64 residual r = b - A x against the original values (device or host vectors). */
+HYB_API int hyb_residual(hyb_system *sys, const double *b, const double *x, double *r, uint64_t nrhs, int memory);
+
+/* Access after decomposition ------------------------------------------------------ */
+
+/* Number of blocks in row `row` of the filled pattern (before decomposition: original). */
+HYB_API int hyb_row_count(const hyb_system *sys, uint64_t row, uint64_t *count);
+/* Column indices of row `row` (get_row_block_indices, src/block_system.c:312-349). */
+HYB_API int hyb_row_cols(const hyb_system *sys, uint64_t row, uint64_t *cols);
+/* Copies block (row, col) to host memory as FP64 (get_block, src/block_system.c:364-396):
+ * the factor after decomposition, the loaded value before. */
+HYB_API int hyb_get_block(const hyb_system *sys, uint64_t row, uint64_t col, double *out);
+/* Operation list in the reference's single-thread order (operations(),
+ * src/block_system.c:1198-1254; order of src/blocks.c:360-514 with one thread):
+ * ops[2i] = row, ops[2i+1] = source column or -1 for INVDIA. Call with ops = NULL to get
+ * the count. */
+HYB_API int hyb_operations(const hyb_system *sys, uint64_t *nops, int64_t *ops);
+/* Kernel launches issued by the last hyb_decompose / hyb_solve call (counted on the host). */
+HYB_API uint64_t hyb_last_launch_count(const hyb_system *sys);
+
+/* Dense single-block kernels on device (the fine-grained surface of
+ * src/block_system.c:938-1141) -------------------------------------------------- */
+
+/* In-place unpivoted LU of an m x m row-major block (matrix_lu_decompose, src/blocks.c:254-283). */
+HYB_API int hyb_block_lu(uint64_t m, double *a, int memory);
+/* out = LU^{-1} b for an m x ncols block (matrix_lu_solve, src/blocks.c:285-316); b may alias out. */
+HYB_API int hyb_block_lu_solve(uint64_t m, const double *lu, uint64_t ncols, const double *b, double *out,
+                               int memory);
+/* Row-major block product: c = a * b (subtract = 0, matrix_multiply, src/blocks.c:200-222) or
+ * c -= a * b (subtract = 1, matrix_multiply_sub_inplace, src/blocks.c:224-244); a is m x k,
+ * b is k x n, c is m x n and must not alias a or b. */
+HYB_API int hyb_block_gemm(uint64_t m, uint64_t k, uint64_t n, const double *a, const double *b, double *c,
+                           int subtract, int memory);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HYBSOL_B200_H */

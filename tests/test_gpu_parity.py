@@ -1,0 +1,260 @@
+"""Parity of the B200 factorization and solve with the oracle and the reference.
+
+Plain FP64 form (the drop-in): factors block-for-block within 1e-12 relative (per block,
+relative to the block's largest entry) of the oracle, which is bit-identical to the
+reference; identical filled pattern and operation list; solutions within 1e-12 relative.
+Mixed form: FP32 factors refined in FP64 to a relative residual <= 1e-12, solution
+within 1e-11 relative of the oracle's. Larger systems, beyond the oracle's reach in a
+test, are checked through size-independent properties: the FP64 residual against A and
+the agreement of the plain and mixed forms.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden, rel_err, reorder_rhs
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL_FACTOR = 1e-12
+TOL_X = 1e-12
+TOL_X_MIXED = 1e-11
+
+
+def _native_from(gpu, mat):
+    order = gpu.compute_ordering(mat.row_ptr, mat.cols, "first")
+    pm = mat.permuted(order)
+    return order, pm, gpu.NativeSystem.from_matrix(pm)
+
+
+def _check_factors(ns, osys, pm):
+    worst = 0.0
+    for i in range(pm.n_blocks):
+        cols = ns.row_cols(i)
+        assert cols == osys.get_row_block_indices(i), i
+        for c in cols:
+            got = ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c])))
+            ref = osys.get_block(i, c)
+            worst = max(worst, rel_err(got, ref))
+    assert worst < TOL_FACTOR, worst
+    return worst
+
+
+def _mesh(n, p, seed, nrhs=1):
+    from hybsol.b200 import meshgen
+
+    return meshgen.mesh_system(n, p, seed=seed, nrhs=nrhs)
+
+
+@pytest.mark.parametrize(
+    ("n", "p", "nrhs"),
+    [(16, 4, 1), (8, 8, 1), (6, "rand", 4), (4, 10, 2), (1, 3, 1)],
+)
+def test_mesh_fp64_matches_oracle(gpu, n, p, nrhs):
+    from hybsol.b200 import meshgen
+
+    pp = meshgen.random_orders(n, 2, 10, seed=11) if p == "rand" else p
+    mat, b = _mesh(n, pp, seed=3, nrhs=nrhs)
+    order, pm, ns = _native_from(gpu, mat)
+    bn = reorder_rhs(mat.sizes, order, b)
+    osys = O.OracleSystem.from_csr(pm.sizes, pm.row_ptr, pm.cols, pm.vals)
+    osys.decompose()
+    info = ns.decompose(gpu.FP64)
+    assert info["zero_pivots"] == 0 and info["non_finite"] == 0
+    _check_factors(ns, osys, pm)
+    assert ns.operations() == osys.operations()
+    x, sinfo = ns.solve(bn)
+    assert rel_err(x, osys.solve(bn)) < TOL_X
+    assert sinfo["relative_residual"] < 1e-13
+
+
+def test_golden_mesh16_solution(gpu):
+    """The reference's own solution of the 16x16 p=4 system (golden vector)."""
+    g = golden("mesh16_p4.npz")
+    mat, _ = _mesh(16, 4, seed=0)
+    order, pm, ns = _native_from(gpu, mat)
+    assert np.array_equal(order.astype(np.int64), g["order_first"])
+    ns.decompose(gpu.FP64)
+    x, _ = ns.solve(g["rhs_new_layout"])
+    assert rel_err(x, g["x_new_layout"]) < TOL_X
+    frp = np.concatenate([[0], np.cumsum([len(ns.row_cols(i)) for i in range(pm.n_blocks)])])
+    assert np.array_equal(frp, g["filled_row_ptr"])
+    ops = np.array([(o[0], o[1] if len(o) == 2 else -1) for o in ns.operations()])
+    assert np.array_equal(ops, g["ops"])
+    sums = np.array(
+        [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))).sum() for i in range(pm.n_blocks) for c in ns.row_cols(i)]
+    )
+    scale = np.sqrt(g["block_sumsq"]) + 1e-300
+    assert np.max(np.abs(sums - g["block_sum"]) / scale) < 1e-12
+
+
+def test_golden_mesh6_uneven_four_rhs(gpu):
+    g = golden("mesh6_prand.npz")
+    mat, _ = _mesh(6, g["p"], seed=5, nrhs=4)
+    order, pm, ns = _native_from(gpu, mat)
+    ns.decompose(gpu.FP64)
+    x, _ = ns.solve(g["rhs_new_layout"])
+    assert rel_err(x, g["x_new_layout"]) < TOL_X
+
+
+@pytest.mark.parametrize(("n", "p", "nrhs"), [(16, 4, 1), (8, 8, 4), (6, "rand", 4)])
+def test_mesh_mixed_refines_to_fp64(gpu, n, p, nrhs):
+    from hybsol.b200 import meshgen
+
+    pp = meshgen.random_orders(n, 2, 10, seed=11) if p == "rand" else p
+    mat, b = _mesh(n, pp, seed=4, nrhs=nrhs)
+    order, pm, ns = _native_from(gpu, mat)
+    bn = reorder_rhs(mat.sizes, order, b)
+    osys = O.OracleSystem.from_csr(pm.sizes, pm.row_ptr, pm.cols, pm.vals)
+    osys.decompose()
+    ns.decompose(gpu.MIXED)
+    x, sinfo = ns.solve(bn, tol=1e-12)
+    assert sinfo["converged"] and sinfo["relative_residual"] <= 1e-12
+    assert 1 <= sinfo["iterations"] <= 10
+    assert rel_err(x, osys.solve(bn)) < TOL_X_MIXED
+
+
+def test_many_systems_in_one_handle(gpu):
+    """Independent systems stacked block-diagonally factor in shared stages."""
+    from hybsol.b200 import meshgen
+
+    mats, rhs = [], []
+    for k, (side, p) in enumerate([(3, 3), (5, 4), (4, 6), (2, 5)]):
+        m, b = meshgen.mesh_system(side, p, seed=20 + k, nrhs=2)
+        mats.append(m)
+        rhs.append(b)
+    big = meshgen.block_diagonal(mats)
+    b = np.concatenate(rhs)
+    order, pm, ns = _native_from(gpu, big)
+    bn = reorder_rhs(big.sizes, order, b)
+    osys = O.OracleSystem.from_csr(pm.sizes, pm.row_ptr, pm.cols, pm.vals)
+    osys.decompose()
+    ns.decompose(gpu.FP64)
+    _check_factors(ns, osys, pm)
+    x, _ = ns.solve(bn)
+    assert rel_err(x, osys.solve(bn)) < TOL_X
+    ns.decompose(gpu.MIXED)
+    x2, info = ns.solve(bn)
+    assert info["converged"] and rel_err(x2, x) < TOL_X_MIXED
+
+
+def _random_system(rng, nb, max_size, density, sym=True, dom=True):
+    sizes = rng.integers(1, max_size + 1, nb)
+    rows = []
+    vals = {}
+    for i in range(nb):
+        for j in range(nb):
+            if i == j or rng.random() < density:
+                vals[(i, j)] = rng.random((sizes[i], sizes[j]))
+                if sym:
+                    vals.setdefault((j, i), rng.random((sizes[j], sizes[i])))
+    for i in range(nb):
+        if dom:
+            vals[(i, i)] = vals[(i, i)] + 2 * nb * max_size * np.eye(sizes[i])
+    from hybsol.b200.meshgen import _assemble
+
+    keys = sorted(vals)
+    rows = np.array([k[0] for k in keys])
+    cols = np.array([k[1] for k in keys])
+    return _assemble(sizes.astype(np.int64), rows, cols, [vals[k] for k in keys])
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_random_sparse_systems(gpu, seed):
+    rng = np.random.default_rng(seed)
+    mat = _random_system(rng, int(rng.integers(3, 40)), int(rng.integers(1, 12)), float(rng.uniform(0.05, 0.5)), sym=seed % 2 == 0)
+    osys = O.OracleSystem.from_csr(mat.sizes, mat.row_ptr, mat.cols, mat.vals)
+    osys.decompose()
+    ns = gpu.NativeSystem.from_matrix(mat)
+    ns.decompose(gpu.FP64)
+    _check_factors(ns, osys, mat)
+    assert ns.operations() == osys.operations()
+    b = rng.uniform(-1, 1, mat.dof)
+    x, _ = ns.solve(b)
+    assert rel_err(x, osys.solve(b)) < TOL_X
+
+
+@pytest.mark.parametrize("size", [1, 31, 64, 65, 100, 130, 200])
+def test_block_sizes_across_tiles(gpu, size):
+    """Blocks smaller than, equal to and larger than the 64-wide tiles, and diagonal
+    blocks too large for shared memory (the global-memory LU/TRSM paths)."""
+    rng = np.random.default_rng(size)
+    sizes = np.array([size, max(1, size // 2), size, 3], dtype=np.int64)
+    nb = len(sizes)
+    vals, keys = [], []
+    for i in range(nb):
+        for j in range(nb):
+            keys.append((i, j))
+            v = rng.standard_normal((sizes[i], sizes[j])) / np.sqrt(sizes[j])
+            if i == j:
+                v += 4 * np.eye(sizes[i])
+            vals.append(v)
+    from hybsol.b200.meshgen import _assemble
+
+    mat = _assemble(sizes, np.array([k[0] for k in keys]), np.array([k[1] for k in keys]), vals)
+    osys = O.OracleSystem.from_csr(mat.sizes, mat.row_ptr, mat.cols, mat.vals)
+    osys.decompose()
+    ns = gpu.NativeSystem.from_matrix(mat)
+    ns.decompose(gpu.FP64)
+    _check_factors(ns, osys, mat)
+    b = rng.uniform(-1, 1, (mat.dof, 3))
+    x, _ = ns.solve(b)
+    assert rel_err(x, osys.solve(b)) < TOL_X
+
+
+def test_zero_pivot_is_reported_not_raised(gpu):
+    from hybsol.b200.meshgen import _assemble
+
+    mat = _assemble(
+        np.array([2, 2]), np.array([0, 0, 1, 1]), np.array([0, 1, 0, 1]),
+        [np.array([[0.0, 1.0], [1.0, 1.0]]), np.eye(2), np.eye(2), np.eye(2) * 3],
+    )  # fmt: skip
+    ns = gpu.NativeSystem.from_matrix(mat)
+    info = ns.decompose(gpu.FP64)
+    assert info["zero_pivots"] >= 1 and info["first_bad_pivot"] == 0
+
+
+def test_refactorization_reuses_the_handle(gpu):
+    mat, b = _mesh(8, 4, seed=9)
+    order, pm, ns = _native_from(gpu, mat)
+    bn = reorder_rhs(mat.sizes, order, b)
+    ns.decompose(gpu.FP64)
+    x1, _ = ns.solve(bn)
+    ns.set_values(pm.vals * 2.0)
+    ns.decompose(gpu.FP64)
+    x2, _ = ns.solve(bn)
+    assert rel_err(x2, x1 / 2.0) < 1e-13
+    cp = ns.copy()
+    x3, _ = cp.solve(bn)
+    assert np.array_equal(x3, x2)
+
+
+@pytest.mark.parametrize("n", [32, 48])
+def test_larger_mesh_properties(gpu, n):
+    """Above the oracle's comfortable size: FP64 residual and plain/mixed agreement."""
+    mat, b = _mesh(n, 8, seed=1)
+    order, pm, ns = _native_from(gpu, mat)
+    bn = reorder_rhs(mat.sizes, order, b)
+    ns.decompose(gpu.FP64)
+    x64, i64 = ns.solve(bn)
+    assert i64["relative_residual"] < 1e-13
+    r = ns.residual(bn, x64)
+    assert np.linalg.norm(r) / np.linalg.norm(bn) < 1e-13
+    ns.decompose(gpu.MIXED)
+    xm, im = ns.solve(bn, tol=1e-12)
+    assert im["converged"] and im["relative_residual"] <= 1e-12
+    assert rel_err(xm, x64) < TOL_X_MIXED
+
+
+def test_dense_single_block_kernels(gpu):
+    rng = np.random.default_rng(5)
+    for m in (1, 5, 64, 100, 300):
+        a = rng.standard_normal((m, m)) + m * np.eye(m)
+        lu = gpu.block_lu(a)
+        ref = O.lu_decompose(a)
+        assert rel_err(lu, ref) < 1e-12
+        b = rng.standard_normal((m, 70))
+        assert rel_err(gpu.block_lu_solve(lu, b), O.lu_solve(ref, b)) < 1e-12
