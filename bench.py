@@ -1,0 +1,532 @@
+#!/usr/bin/env python
+"""Benchmark: decompose + solve of a hybridized quad-mesh block system on B200.
+
+Metric (the reference's headline): decompose+solve time in ms, FP32+refinement
+("mixed") against plain FP64, to a relative FP64 residual of 1e-12, on one GPU.
+
+Workload: the quad-mesh block system of the reference's hybridized solver, N x N
+elements (default 128 x 128), order p (default 8): 64x64 element blocks, 8x8 edge blocks,
+element<->edge couplings, seeded values, one right-hand side, ordered by the reference's
+first-fit coloring (edges first). The 256 x 256 mesh of the original target needs 1.1 TB
+of FP64 factors and cannot be held by one GPU; 128 x 128 (137.5 GB FP64) is the largest
+that fits, so it is the default.
+
+A step = load the values (device-resident for `value`, pinned host for `e2e`), factor,
+and solve one right-hand side (the mixed form iterates refinement to 1e-12). The symbolic
+phase (fill pattern and schedule) runs once per pattern before timing and is reported as
+`analysis_ms`.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--mesh 128] [--p 8]
+  python bench.py --impl reference ...   # the reference's own CPU path, rank 0 only
+
+Under torchrun with N > 1 every rank factors its own copy (replicas: one system does
+not shard), timing is max over ranks, and value is the per-step time (weak scaling).
+"""
+
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "hybridized-solver_b200"))
+
+METRIC = "decompose+solve ms: FP32+refine vs plain FP64 on one B200 at 1e-12 residual"
+TOL = 1e-12
+FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+CPU_SAMPLE_MESH = 20  # reference CPU sample: 20x20 elements at the same p
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--mesh", type=int, default=128)
+    ap.add_argument("--p", type=int, default=8)
+    ap.add_argument("--cpu-sample-mesh", type=int, default=CPU_SAMPLE_MESH)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-profile", action="store_true", help="do not time the dominant kernel with events")
+    return ap.parse_args()
+
+
+def workload_config(n, p, extra=None):
+    cfg = {
+        "workload": f"hybridized quad mesh {n}x{n} elements, p={p} (element blocks {p * p}x{p * p}, edge blocks "
+        f"{p}x{p}), 1 RHS, seed 0, reference first-fit coloring order",
+        "mesh": f"{n}x{n}",
+        "p": p,
+        "nrhs": 1,
+        "tolerance": TOL,
+        "l2": "inputs larger than L2 (factor slab >> 126 MB)",
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ---------------------------------------------------------------------------------
+# workload
+
+
+def build_workload(n, p):
+    import numpy as np
+
+    from hybsol.b200 import meshgen, native
+
+    mat, b = meshgen.mesh_system(n, p, seed=0)
+    order = native.compute_ordering(mat.row_ptr, mat.cols, "first")
+    pm = mat.permuted(order)
+    off_o = np.concatenate([[0], np.cumsum(mat.sizes)])
+    off_n = np.concatenate([[0], np.cumsum(pm.sizes)])
+    bn = np.empty_like(b)
+    for i in range(mat.n_blocks):
+        bn[off_n[order[i]] : off_n[order[i] + 1]] = b[off_o[i] : off_o[i + 1]]
+    return pm, bn
+
+
+# ---------------------------------------------------------------------------------
+# clocks
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms while the timed region runs."""
+
+    FIELDS = (
+        "index,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+            self.proc = subprocess.Popen(cmd, stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.file is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.file.flush()
+        with open(self.file.name) as f:
+            rows = [r for r in csv.reader(io.StringIO(f.read())) if len(r) >= 10]
+        os.unlink(self.file.name)
+        mine = [r for r in rows if self.uuid and self.uuid in r[1]] or rows
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in mine:
+            try:
+                sm.append(float(r[2]))
+                smax.append(float(r[3]))
+                power.append(float(r[4]))
+            except ValueError:
+                continue
+            for name, v in zip(names, r[6:10]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        loaded = [s for s, pw in zip(sm, power) if pw > 0.3 * max(power)] or sm
+        return {
+            "sm_mhz": statistics.median(loaded),
+            "sm_max_mhz": max(smax),
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+            "power_w_max": max(power),
+        }
+
+
+# ---------------------------------------------------------------------------------
+# reference CPU path
+
+
+def reference_sample(n, p, steps, warmup, threads):
+    """Decompose+solve of the reference extension (compiled from its sources) on a mesh."""
+    import numpy as np
+
+    from hybsol.b200 import meshgen
+    from oracle import oracle as O
+
+    ref = O.load_reference()
+    mat, b = meshgen.mesh_system(n, p, seed=0)
+    times = []
+    for it in range(warmup + steps):
+        s = ref.BlockSystem(*[int(x) for x in mat.sizes])
+        for r, c, v in mat.iter_blocks():
+            s.add_block(r, c, v)
+        order = s.compute_reordering("first")
+        s.reorder_blocks(order)
+        bn = s.unorder_vector(order, b)
+        t0 = time.perf_counter()
+        s.decompose(threads)
+        x = s.solve(bn)
+        dt = time.perf_counter() - t0
+        if it >= warmup:
+            times.append(dt)
+    xo = s.reorder_vector(order, x)
+    res = float(np.linalg.norm(mat.matvec(xo) - b) / np.linalg.norm(b))
+    return times, res
+
+
+def analyze_flops(n, p):
+    from hybsol.b200 import native
+
+    pm, _ = build_workload(n, p)
+    return native.analyze(pm.sizes, pm.row_ptr, pm.cols)["factor_flops"]
+
+
+def cpu_baseline(full_flops, p, sample_mesh, steps=1, warmup=0):
+    from oracle import oracle as O
+
+    cores = O.cpu_count()
+    os.environ["OMP_NUM_THREADS"] = str(cores)
+    times, res = reference_sample(sample_mesh, p, steps, warmup, cores)
+    sample_flops = analyze_flops(sample_mesh, p)
+    best = min(times)
+    scale = full_flops / sample_flops
+    return {
+        "value": best * 1e3 * scale,
+        "unit": "ms",
+        "cores": cores,
+        "kind": "reference",
+        "sample": (
+            f"reference extension (oracle/_ref, built from the reference's src/*.c) decompose(n_threads={cores}) + "
+            f"solve on the {sample_mesh}x{sample_mesh} p={p} mesh ({sample_flops / 1e9:.1f} GFLOP): "
+            f"{best * 1e3:.1f} ms ({sample_flops / best / 1e9:.1f} GFLOP/s, residual {res:.1e}), scaled by "
+            f"GFLOP to the {full_flops / 1e9:.0f}-GFLOP workload"
+        ),
+        "sample_ms": best * 1e3,
+        "sample_gflops": sample_flops / best / 1e9,
+    }
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+
+    if not O.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference extension not built (oracle/_ref missing)"}))
+        return 0
+    full = analyze_flops(args.mesh, args.p)
+    cores = O.cpu_count()
+    os.environ["OMP_NUM_THREADS"] = str(cores)
+    times, res = reference_sample(args.cpu_sample_mesh, args.p, args.steps, args.warmup, cores)
+    sample_flops = analyze_flops(args.cpu_sample_mesh, args.p)
+    scale = full / sample_flops
+    ms = statistics.mean(times) * 1e3 * scale
+    cpu = {
+        "value": ms,
+        "unit": "ms",
+        "cores": cores,
+        "kind": "reference",
+        "sample": f"{args.cpu_sample_mesh}x{args.cpu_sample_mesh} p={args.p} mesh per step "
+        f"({sample_flops / 1e9:.1f} GFLOP, {statistics.mean(times) * 1e3:.1f} ms, residual {res:.1e}), "
+        f"scaled by GFLOP to the {full / 1e9:.0f}-GFLOP workload",
+    }
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": ms,
+        "unit": "ms",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": workload_config(args.mesh, args.p, {"factor_gflop": full / 1e9}),
+        "cpu_baseline": cpu,
+        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------------
+# our arm
+
+
+def load_peaks():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        return json.loads(path.read_text()), "measured"
+    return dict(FALLBACK_PEAKS), "fallback"
+
+
+def gemm_peak(dtype):
+    """cuBLAS GEMM throughput (TFLOP/s) measured here, the denominator for FP64/FP32 kernels."""
+    import torch
+
+    n = 8192
+    a = torch.randn(n, n, dtype=dtype, device="cuda")
+    b = torch.randn(n, n, dtype=dtype, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = 1e30
+    for _ in range(5):
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * n**3 / (best * 1e-3) / 1e12
+
+
+def run_ours(args):
+    import ctypes
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from hybsol.b200 import native
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    if not native.device_available():
+        raise RuntimeError("bench.py needs an sm_100 GPU")
+    lib = native.lib()
+    peaks, peak_src = load_peaks()
+    fp64_peak = gemm_peak(torch.float64)
+    fp32_peak = gemm_peak(torch.float32)
+
+    t0 = time.perf_counter()
+    pm, bn = build_workload(args.mesh, args.p)
+    gen_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ns = native.NativeSystem(pm.sizes, pm.row_ptr, pm.cols)
+    analysis_ms = (time.perf_counter() - t0) * 1e3
+    ana = native.analyze(pm.sizes, pm.row_ptr, pm.cols)
+    flops = ana["factor_flops"]
+    stream = torch.cuda.ExternalStream(ns.stream)
+
+    d_vals = torch.from_numpy(pm.vals).to("cuda")
+    d_b = torch.from_numpy(bn).to("cuda")
+    d_x = torch.empty_like(d_b)
+    if not args.no_profile:
+        lib.hyb_profile_enable(ns._h, 1)
+
+    def device_step(prec):
+        """One step with inputs resident in HBM; returns (launches, solve info)."""
+        launches = 0
+        native._check(lib.hyb_system_set_values(ns._h, native._ptr(d_vals), native.MEMORY_DEVICE), "set_values")
+        ns.decompose(prec)
+        launches += ns.last_launch_count()
+        info = ns.solve_device(d_b, d_x, 1, tol=TOL, max_iter=30, residual=(prec == native.MIXED))
+        launches += ns.last_launch_count()
+        return launches, info
+
+    def timed_form(prec):
+        for _ in range(args.warmup):
+            device_step(prec)
+        barrier()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        launches, info = 0, None
+        for k in range(args.steps):
+            starts[k].record(stream)
+            lk, info = device_step(prec)
+            ends[k].record(stream)
+            launches += lk
+        barrier()
+        ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+        prof = native.KernelProfile()
+        have_prof = lib.hyb_profile_read(ns._h, ctypes.byref(prof)) == 0 and prof.launches > 0
+        return statistics.mean(ms), launches, info, (prof if have_prof else None)
+
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    with ClockSampler(uuid) as clocks:
+        fp64_ms, fp64_launches, fp64_info, fp64_prof = timed_form(native.FP64)
+        x64 = d_x.cpu().numpy()
+        r64 = ns.residual(bn, x64)
+        fp64_relres = float(np.linalg.norm(r64) / np.linalg.norm(bn))
+        mixed_ms, mixed_launches, mixed_info, mixed_prof = timed_form(native.MIXED)
+        xm = d_x.cpu().numpy()
+    clk = clocks.summary()
+    fp64_ms = max_over_ranks(fp64_ms)
+    mixed_ms = max_over_ranks(mixed_ms)
+    err_vs_fp64 = float(np.abs(xm - x64).max() / np.abs(x64).max())
+
+    # end to end through the C ABI: pinned host values and RHS in, solution out
+    h_vals = torch.from_numpy(pm.vals).pin_memory()
+    h_b = torch.from_numpy(bn).pin_memory()
+    h_x = torch.empty_like(h_b).pin_memory()
+    sinfo = native.SolveInfo()
+
+    def e2e_step():
+        native._check(lib.hyb_system_set_values(ns._h, native._ptr(h_vals), native.MEMORY_HOST), "set_values")
+        ns.decompose(native.MIXED)
+        st = lib.hyb_solve(
+            ns._h, native._ptr(h_b), native._ptr(h_x), 1, native.MEMORY_HOST, TOL, 30, ctypes.byref(sinfo)
+        )
+        native._check(st, "hyb_solve")
+
+    e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    barrier()
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps)
+
+    def roofline(prof, bound, peak, unit, elem_bytes, peak_note, step_ms):
+        if prof is None:
+            return None
+        avg_ms = prof.total_ms / prof.launches
+        if bound == "tensor":
+            per_launch = prof.flops / prof.launches
+            achieved = per_launch / (avg_ms * 1e-3) / 1e12
+        else:
+            per_launch = elem_bytes * (2 * prof.c_elems + prof.ab_elems) / prof.launches
+            achieved = per_launch / (avg_ms * 1e-3) / 1e9
+        return {
+            "bound": bound,
+            "achieved": achieved,
+            "peak": peak,
+            "unit": unit,
+            "frac": achieved / peak,
+            "traffic": None,
+            "kernel": "Schur-complement update (k_update64_f64 / k_update)",
+            "launches": prof.launches,
+            "avg_launch_ms": avg_ms,
+            "share_of_step": prof.total_ms / step_ms,
+            "peak_source": peak_note,
+            "algorithmic_per_launch": per_launch,
+        }
+
+    rf64 = roofline(fp64_prof, "tensor", fp64_peak, "TFLOP/s", 8, "cuBLAS DGEMM 8192^3 measured in this run", fp64_ms)
+    rmix = roofline(
+        mixed_prof, "tensor", fp32_peak, "TFLOP/s", 4, "cuBLAS SGEMM 8192^3 measured in this run", mixed_ms
+    )
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        if O.reference_available():
+            cpu = cpu_baseline(flops, args.p, args.cpu_sample_mesh)
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": mixed_ms,
+            "unit": "ms",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": mixed_ms,
+            "higher_is_better": False,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 factors + f64 refinement",
+            "data": "synthetic",
+            "config": workload_config(
+                args.mesh,
+                args.p,
+                {
+                    "dof": int(pm.dof),
+                    "blocks": int(pm.n_blocks),
+                    "blocks_after_fill": int(ana["filled_blocks"]),
+                    "levels": int(ana["n_levels"]),
+                    "factor_gflop": flops / 1e9,
+                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                },
+            ),
+            "fp64_ms": fp64_ms,
+            "mixed_speedup_vs_fp64": fp64_ms / mixed_ms,
+            "fp64_tflops": flops / (fp64_ms * 1e-3) / 1e12,
+            "mixed_tflops": flops / (mixed_ms * 1e-3) / 1e12,
+            "accuracy": {
+                "fp64_relative_residual": fp64_relres,
+                "mixed_relative_residual": mixed_info["relative_residual"],
+                "mixed_refinement_iterations": mixed_info["iterations"],
+                "mixed_rel_err_vs_fp64_solution": err_vs_fp64,
+            },
+            "analysis_ms": analysis_ms,
+            "workload_build_s": gen_s,
+            "e2e": {
+                "value": e2e_ms,
+                "unit": "ms",
+                "h2d_bytes_per_step": int(h_vals.numel() * 8 + h_b.numel() * 8),
+                "d2h_bytes_per_step": int(h_x.numel() * 8),
+                "path": "C ABI with pinned host buffers: hyb_system_set_values + hyb_decompose(mixed) + hyb_solve",
+            },
+            "gpu_launches": int(mixed_launches),
+            "gpu_launches_fp64": int(fp64_launches),
+            "roofline": rmix,
+            "roofline_fp64": rf64,
+            "peaks": {"fp64_tflops_cublas": fp64_peak, "fp32_tflops_cublas": fp32_peak, "source": peak_src, **peaks},
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    ns.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

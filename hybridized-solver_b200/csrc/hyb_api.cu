@@ -15,6 +15,7 @@
 #include <memory>
 #include <new>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 using hyb::DevSym;
@@ -105,9 +106,15 @@ struct hyb_system
     std::map<std::pair<int, int>, std::unique_ptr<GraphExec>> g_solve; // (precision, nrhs)
     uint64_t launches = 0;
     uint64_t last_launches = 0;
+    // profiling: one event pair per level around the Schur-update kernel
+    bool profile = false;
+    std::vector<cudaEvent_t> prof_ev;
+    std::vector<int64_t> prof_levels; // level of each event pair
+    int prof_precision = -1;
 
     ~hyb_system()
     {
+        free_profile_events();
         g_factor[0].reset();
         g_factor[1].reset();
         g_solve.clear();
@@ -119,6 +126,14 @@ struct hyb_system
         free_solve_buffers();
         if (stream)
             cudaStreamDestroy(stream);
+    }
+
+    void free_profile_events()
+    {
+        for (cudaEvent_t e : prof_ev)
+            cudaEventDestroy(e);
+        prof_ev.clear();
+        prof_levels.clear();
     }
 
     void free_solve_buffers()
@@ -160,6 +175,7 @@ int upload_symbolic(hyb_system *h)
         {S.lcol_blk.data(), S.lcol_blk.size() * 4, (const void **)&d.lcol_blk},
         {S.piv.data(), S.piv.size() * 4, (const void **)&d.piv},
         {S.trsm_pref.data(), S.trsm_pref.size() * 8, (const void **)&d.trsm_pref},
+        {S.lu_pref.data(), S.lu_pref.size() * 8, (const void **)&d.lu_pref},
         {S.upd_pref.data(), S.upd_pref.size() * 8, (const void **)&d.upd_pref},
         {S.fwd_pref.data(), S.fwd_pref.size() * 8, (const void **)&d.fwd_pref},
         {S.fwd_rows.data(), S.fwd_rows.size() * 8, (const void **)&d.fwd_rows},
@@ -216,6 +232,16 @@ template <typename T> int enqueue_factor(hyb_system *h, T *slab, uint64_t &launc
     {
         const int64_t p0 = S.lvl_ptr[l], p1 = S.lvl_ptr[l + 1];
         const Symbolic::LevelShape &sh = S.shape[l];
+        if (sh.piv64)
+        {
+            // 1+2 fused: 64x64 diagonal LU and the solves of the pivot rows' upper blocks
+            const int64_t units = S.lu_pref[p1] - S.lu_pref[p0];
+            hyb::k_lu_trsm64<T><<<(unsigned)units, hyb::kThreads, 0, st>>>(ds, slab, p0, p1, ds.lu_pref,
+                                                                          h->d_status);
+            ++launches;
+        }
+        else
+        {
         // 1. diagonal LU
         const int lu_bytes = lu_smem_bytes<T>(sh.max_piv);
         if (lu_bytes <= optin)
@@ -235,7 +261,20 @@ template <typename T> int enqueue_factor(hyb_system *h, T *slab, uint64_t &launc
                 hyb::k_trsm<T, false><<<grid, hyb::kThreads, 0, st>>>(ds, slab, p0, p1);
             ++launches;
         }
-        // 3. Schur-complement updates
+        }
+        // 3. Schur-complement updates (optionally bracketed by profiling events)
+        const bool timed = h->profile && (S.lvl_listed[l] ? S.mt_lvl_ptr[l + 1] > S.mt_lvl_ptr[l]
+                                                          : S.upd_pref[p1] > S.upd_pref[p0]);
+        if (timed)
+        {
+            cudaEvent_t e0, e1;
+            HYB_CUDA(cudaEventCreate(&e0));
+            HYB_CUDA(cudaEventCreate(&e1));
+            h->prof_ev.push_back(e0);
+            h->prof_ev.push_back(e1);
+            h->prof_levels.push_back(l);
+            HYB_CUDA(cudaEventRecord(e0, st));
+        }
         const unsigned tiles = (unsigned)(((sh.max_row + hyb::kTile - 1) / hyb::kTile) *
                                           ((sh.max_col + hyb::kTile - 1) / hyb::kTile));
         if (S.lvl_listed[l])
@@ -252,10 +291,24 @@ template <typename T> int enqueue_factor(hyb_system *h, T *slab, uint64_t &launc
             const int64_t nu = S.upd_pref[p1] - S.upd_pref[p0];
             if (nu > 0)
             {
+                if constexpr (std::is_same_v<T, double>)
+                {
+                    if (sh.uniform64)
+                    {
+                        hyb::k_update64_f64<<<(unsigned)nu, hyb::kUpd64Threads, hyb::kUpd64Smem, st>>>(
+                            ds, slab, p0, p1, h->d_status);
+                        ++launches;
+                        if (timed)
+                            HYB_CUDA(cudaEventRecord(h->prof_ev.back(), st));
+                        continue;
+                    }
+                }
                 hyb::k_update<T><<<dim3((unsigned)nu, tiles), hyb::kThreads, 0, st>>>(ds, slab, p0, p1);
                 ++launches;
             }
         }
+        if (timed)
+            HYB_CUDA(cudaEventRecord(h->prof_ev.back(), st));
     }
     HYB_CUDA(cudaGetLastError());
     return HYB_SUCCESS;
@@ -277,8 +330,12 @@ template <typename T, typename V> int enqueue_solve(hyb_system *h, const T *slab
             hyb::k_fwd_partial<T, V><<<(unsigned)units, hyb::kThreads, 0, st>>>(ds, slab, y, scratch, p0, p1, nrhs);
             ++launches;
         }
-        const int bytes = S.shape[l].max_piv * nrhs * (int)sizeof(V);
-        hyb::k_fwd_final<T, V><<<(unsigned)(p1 - p0), hyb::kThreads, bytes, st>>>(ds, slab, y, scratch, p0, nrhs);
+        const int mp = S.shape[l].max_piv;
+        const int acc_bytes = (mp * nrhs * (int)sizeof(V) + 15) / 16 * 16;
+        const int diag_bytes = mp * (mp | 1) * (int)sizeof(T);
+        const int stage = acc_bytes + diag_bytes <= smem_optin() ? 1 : 0;
+        hyb::k_fwd_final<T, V><<<(unsigned)(p1 - p0), hyb::kThreads, acc_bytes + (stage ? diag_bytes : 0), st>>>(
+            ds, slab, y, scratch, p0, nrhs, stage);
         ++launches;
     }
     for (int64_t l = S.n_levels - 1; l >= 0; --l)
@@ -627,6 +684,7 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
         allow_smem(hyb::k_fwd_final<double, double>);
         allow_smem(hyb::k_fwd_final<float, float>);
         allow_smem(hyb::k_dense_lu);
+        allow_smem(hyb::k_update64_f64);
         attrs_set = true;
     }
     h->last_launches = 0;
@@ -650,8 +708,11 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
         HYB_CUDA(cudaMemsetAsync(h->d_f64, 0, slab * sizeof(double), h->stream));
         hyb::k_scatter<double><<<sgrid, hyb::kThreads, 0, h->stream>>>(h->ds, h->d_a, h->d_f64, S.nnz_a());
         h->last_launches += 1;
-        const int rc = run_graph(h, h->g_factor[0],
-                                 [&](uint64_t &count) { return enqueue_factor<double>(h, h->d_f64, count); });
+        const int rc = run_graph(h, h->g_factor[0], [&](uint64_t &count) {
+            h->free_profile_events();
+            h->prof_precision = HYB_PRECISION_FP64;
+            return enqueue_factor<double>(h, h->d_f64, count);
+        });
         if (rc != HYB_SUCCESS)
             return rc;
     }
@@ -673,14 +734,22 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
         HYB_CUDA(cudaMemsetAsync(h->d_f32, 0, slab * sizeof(float), h->stream));
         hyb::k_scatter<float><<<sgrid, hyb::kThreads, 0, h->stream>>>(h->ds, h->d_a, h->d_f32, S.nnz_a());
         h->last_launches += 1;
-        const int rc =
-            run_graph(h, h->g_factor[1], [&](uint64_t &count) { return enqueue_factor<float>(h, h->d_f32, count); });
+        const int rc = run_graph(h, h->g_factor[1], [&](uint64_t &count) {
+            h->free_profile_events();
+            h->prof_precision = HYB_PRECISION_MIXED;
+            return enqueue_factor<float>(h, h->d_f32, count);
+        });
         if (rc != HYB_SUCCESS)
             return rc;
     }
     int st[hyb::ST_WORDS];
     HYB_CUDA(cudaMemcpyAsync(st, h->d_status, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
     HYB_CUDA(cudaStreamSynchronize(h->stream));
+    if (st[hyb::ST_TIMEOUT])
+    {
+        g_cuda_error = "a device-side wait ran out of its iteration limit";
+        return HYB_CUDA_ERROR;
+    }
     h->factored = precision;
     h->launches += h->last_launches;
     if (info)
@@ -916,6 +985,42 @@ HYB_API int hyb_operations(const hyb_system *h, uint64_t *nops, int64_t *ops)
 HYB_API uint64_t hyb_last_launch_count(const hyb_system *h)
 {
     return h ? h->last_launches : 0;
+}
+
+HYB_API int hyb_profile_enable(hyb_system *h, int enable)
+{
+    if (check_handle(h))
+        return HYB_INVALID_ARGUMENT;
+    if (h->profile != (enable != 0))
+    {
+        h->profile = enable != 0;
+        // the factorization graphs are recaptured with (or without) the event nodes
+        h->g_factor[0].reset();
+        h->g_factor[1].reset();
+        h->free_profile_events();
+    }
+    return HYB_SUCCESS;
+}
+
+HYB_API int hyb_profile_read(const hyb_system *h, hyb_kernel_profile *out)
+{
+    if (check_handle(h) || !out)
+        return HYB_INVALID_ARGUMENT;
+    *out = hyb_kernel_profile{};
+    if (!h->profile || h->factored < 0 || h->factored != h->prof_precision)
+        return HYB_NOT_DECOMPOSED;
+    for (size_t i = 0; i < h->prof_levels.size(); ++i)
+    {
+        float ms = 0;
+        HYB_CUDA(cudaEventElapsedTime(&ms, h->prof_ev[2 * i], h->prof_ev[2 * i + 1]));
+        const auto &sh = h->S.shape[h->prof_levels[i]];
+        out->launches += 1;
+        out->total_ms += ms;
+        out->flops += sh.upd_flops;
+        out->c_elems += sh.upd_c_elems;
+        out->ab_elems += sh.upd_ab_elems;
+    }
+    return HYB_SUCCESS;
 }
 
 HYB_API int hyb_block_lu(uint64_t m, double *a, int memory)

@@ -47,6 +47,7 @@ struct Symbolic
     std::vector<int64_t> lvl_ptr;   // [L+1]
     std::vector<int32_t> piv;       // [n]
     std::vector<int64_t> trsm_pref; // [n+1] prefix (in piv order) of upper-block counts
+    std::vector<int64_t> lu_pref;   // [n+1] prefix of max(1, upper-block count): fused LU+solve units
     std::vector<int64_t> upd_pref;  // [n+1] prefix of |lower column| * |upper row|
     std::vector<int64_t> fwd_pref;  // [n+1] prefix of lower-row block counts (forward solve units)
     std::vector<int64_t> fwd_rows;  // [n+1] prefix of lower-row block count * pivot size (scratch rows)
@@ -72,6 +73,10 @@ struct Symbolic
         int32_t max_col = 0;  // largest target column block
         int32_t max_up = 0;   // largest upper-block column size of a pivot row
         bool uniform64 = false; // every pivot, target row and column block is 64
+        bool piv64 = false;     // every pivot and every upper block of its row is 64 wide
+        double upd_flops = 0;   // algorithmic flops of the level's Schur updates
+        double upd_c_elems = 0; // scalars of the update targets (each read and written once)
+        double upd_ab_elems = 0; // scalars of the lower-column and upper-row operand blocks
     };
     std::vector<LevelShape> shape;
 

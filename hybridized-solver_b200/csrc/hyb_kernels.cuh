@@ -33,6 +33,7 @@ struct DevSym
     const int32_t *lcol_blk;
     const int32_t *piv;
     const int64_t *trsm_pref;
+    const int64_t *lu_pref;
     const int64_t *upd_pref;
     const int64_t *fwd_pref;
     const int64_t *fwd_rows;
@@ -234,6 +235,150 @@ __global__ void __launch_bounds__(kThreads) k_trsm(DevSym S, T *__restrict__ sla
 }
 
 // ----------------------------------------------------------------------------------
+// 64x64 pivots (the element rows of a p=8 mesh): LU of the diagonal block and the solve
+// of one upper block fused in one CTA of 256 threads.
+constexpr int kLd65 = 65; // odd shared-memory row stride: rows 4 apart sit in different banks
+
+// Right-looking LU of the 64x64 block in shared memory `d` (row stride kLd65), registers
+// 4x4 per thread, one barrier per pivot: step i publishes row i+1 and column i+1 for the
+// next step through double-buffered shared rows. Multipliers use the pivot's reciprocal.
+template <typename T>
+__device__ void lu64_shared(T *d, T *rowbuf, T *colbuf, int *status, int row_id)
+{
+    const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+    T v[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+            v[a][b] = d[(ty * 4 + a) * kLd65 + tx * 4 + b];
+    if (ty == 0)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+            rowbuf[tx * 4 + b] = v[0][b];
+    if (tx == 0)
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+            colbuf[ty * 4 + a] = v[a][0];
+    __syncthreads();
+    for (int i = 0; i < 64; ++i)
+    {
+        const int cur = (i & 1) * 64, nxt = 64 - cur;
+        const T p = rowbuf[cur + i];
+        if (tid == 0 && status != nullptr && (p == T(0) || !finite_val(p)))
+        {
+            atomicAdd(status + (p == T(0) ? ST_ZERO_PIVOTS : ST_NON_FINITE), 1);
+            atomicMin(status + ST_FIRST_BAD, row_id);
+        }
+        const T rp = T(1) / p;
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+        {
+            const int r = ty * 4 + a;
+            if (r <= i)
+                continue;
+            const T l = colbuf[cur + r] * rp;
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+            {
+                const int c = tx * 4 + b;
+                if (c == i)
+                    v[a][b] = l;
+                else if (c > i)
+                    v[a][b] -= l * rowbuf[cur + c];
+            }
+        }
+        if (i + 1 < 64)
+        {
+            const int n1 = i + 1;
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+                {
+                    const int r = ty * 4 + a, c = tx * 4 + b;
+                    if (r == n1 && c >= n1)
+                        rowbuf[nxt + c] = v[a][b];
+                    if (c == n1 && r > n1)
+                        colbuf[nxt + r] = v[a][b];
+                }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+            d[(ty * 4 + a) * kLd65 + tx * 4 + b] = v[a][b];
+    __syncthreads();
+}
+
+// X = U^{-1} L^{-1} B for a 64x64 block B in place in global memory, D factored in shared
+// memory. Four lanes share a column; lane q of a column holds rows q, q+4, ..., q+60 in
+// registers, so each substitution step is one shuffle and predicated FMAs, no barrier.
+template <typename T> __device__ void trsm64_columns(const T *d, T *gb)
+{
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int col = tid >> 2, q = tid & 3, base = lane & ~3;
+    T x[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+        x[j] = gb[(4 * j + q) * 64 + col];
+#pragma unroll
+    for (int i = 0; i < 63; ++i)
+    {
+        const T xi = __shfl_sync(0xffffffffu, x[i >> 2], base + (i & 3));
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+            if (4 * j + q > i)
+                x[j] -= d[(4 * j + q) * kLd65 + i] * xi;
+    }
+#pragma unroll
+    for (int i = 63; i >= 0; --i)
+    {
+        const T xi = __shfl_sync(0xffffffffu, x[i >> 2], base + (i & 3)) / d[i * kLd65 + i];
+        if ((i & 3) == q)
+            x[i >> 2] = xi;
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+            if (4 * j + q < i)
+                x[j] -= d[(4 * j + q) * kLd65 + i] * xi;
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+        gb[(4 * j + q) * 64 + col] = x[j];
+}
+
+// One CTA per upper block of the level's (64-row) pivots; every CTA factors its pivot's
+// diagonal block in shared memory (the first CTA of each pivot writes it back) and then
+// solves its block. A pivot without upper blocks gets one CTA for the LU alone: the grid
+// is the level's work units with empty pivots counted once (see enqueue_factor).
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+    k_lu_trsm64(DevSym S, T *__restrict__ slab, int64_t p0, int64_t p1, const int64_t *__restrict__ unit_pref,
+                int *status)
+{
+    __shared__ T d[64 * kLd65];
+    __shared__ T rowbuf[128];
+    __shared__ T colbuf[128];
+    const int64_t u = unit_pref[p0] + blockIdx.x;
+    const int64_t p = find_owner(unit_pref, p0, p1, u);
+    const int64_t k = S.piv[p];
+    const int64_t j = u - unit_pref[p];
+    T *gd = slab + S.blk_off[S.diag_pos[k]];
+    for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
+        d[(i >> 6) * kLd65 + (i & 63)] = gd[i];
+    __syncthreads();
+    lu64_shared(d, rowbuf, colbuf, j == 0 ? status : nullptr, (int)k);
+    if (j == 0)
+        for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
+            gd[i] = d[(i >> 6) * kLd65 + (i & 63)];
+    const int64_t blk = S.diag_pos[k] + 1 + j;
+    if (blk < S.row_ptr[k + 1])
+        trsm64_columns(d, slab + S.blk_off[blk]);
+}
+
+// ----------------------------------------------------------------------------------
 // Generic tiled update of one 64x64 output tile: acc -= A * B with A (M x K, lda) and
 // B (K x N, ldb), both row-major; 256 threads, 4x4 outputs each.
 template <typename T> struct TileAcc
@@ -338,6 +483,154 @@ __global__ void __launch_bounds__(kThreads) k_update(DevSym S, T *__restrict__ s
     tile_store(acc, cb, N, M - r0, N - c0);
 }
 
+// ----------------------------------------------------------------------------------
+// Bulk async copies (the non-tensor TMA path) into shared memory, completed on an
+// mbarrier. Waits are bounded: a wait that runs out records ST_TIMEOUT and the CTA skips
+// its arithmetic instead of spinning forever.
+enum
+{
+    ST_TIMEOUT = 3
+};
+constexpr uint32_t kSpinLimit = 1u << 24;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase)
+{
+    for (uint32_t i = 0; i < kSpinLimit; ++i)
+    {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(smem_u32(bar)), "r"(phase)
+                     : "memory");
+        if (done)
+            return true;
+    }
+    return false;
+}
+
+// FP64 tensor-core MMA: d(8x8) += a(8x4) * b(4x8). Lane l holds a[l/4][l%4],
+// b[l%4][l/4] and d[l/4][2*(l%4)], d[l/4][2*(l%4)+1].
+__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+constexpr int kLd64 = 68; // padded shared-memory row (doubles): conflict-free fragment reads
+constexpr int kUpd64Threads = 128;
+constexpr int kUpd64Smem = 2 * 64 * kLd64 * 8 + 16;
+
+// Uniform-64 FP64 update, the dominant work of a mesh factorization: one CTA per target
+// block, C(64x64) -= A(t,k) * U(k,c). A and U arrive by 128 bulk row copies into padded
+// shared memory while the CTA reads C into DMMA accumulator fragments; four warps each
+// own a 32x32 quarter of C (16 m8n8k4 tiles). Work units as in k_update.
+__global__ void __launch_bounds__(kUpd64Threads)
+    k_update64_f64(DevSym S, double *__restrict__ slab, int64_t p0, int64_t p1, int *status)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *sa = reinterpret_cast<double *>(smem_raw);
+    double *sb = sa + 64 * kLd64;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sb + 64 * kLd64);
+
+    const int64_t u = S.upd_pref[p0] + blockIdx.x;
+    const int64_t p = find_owner(S.upd_pref, p0, p1, u);
+    const int64_t k = S.piv[p];
+    const int64_t local = u - S.upd_pref[p];
+    const int64_t n_up = S.row_ptr[k + 1] - S.diag_pos[k] - 1;
+    const int64_t li = S.lcol_ptr[k] + local / n_up;
+    const int64_t bu = S.diag_pos[k] + 1 + local % n_up;
+    const int32_t t = S.lcol_row[li];
+    const int32_t c = S.cols[bu];
+    const int64_t tgt = find_col(S.cols, S.row_ptr[t], S.row_ptr[t + 1], c);
+    const double *ga = slab + S.blk_off[S.lcol_blk[li]];
+    const double *gb = slab + S.blk_off[bu];
+    double *gc = slab + S.blk_off[tgt];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0)
+    {
+        mbar_init(bar, 1);
+        mbar_expect_tx(bar, 2 * 64 * 64 * 8);
+    }
+    __syncthreads();
+    if (warp == 0)
+    {
+        // 64 rows of A and 64 rows of U, 512 bytes each, two per lane
+        for (int r = lane; r < 64; r += 32)
+        {
+            bulk_g2s(sa + r * kLd64, ga + r * 64, 512, bar);
+            bulk_g2s(sb + r * kLd64, gb + r * 64, 512, bar);
+        }
+    }
+    const int g = lane >> 2, q = lane & 3;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    double acc[4][4][2];
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+        {
+            const double2 v = *reinterpret_cast<const double2 *>(gc + (wm + mi * 8 + g) * 64 + wn + ni * 8 + 2 * q);
+            acc[mi][ni][0] = v.x;
+            acc[mi][ni][1] = v.y;
+        }
+    if (!mbar_wait(bar, 0))
+    {
+        if (lane == 0)
+            atomicOr(status + ST_TIMEOUT, 1);
+        return;
+    }
+#pragma unroll 4
+    for (int kk = 0; kk < 64; kk += 4)
+    {
+        double av[4], bv[4];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+            av[mi] = -sa[(wm + mi * 8 + g) * kLd64 + kk + q];
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+            bv[ni] = sb[(kk + q) * kLd64 + wn + ni * 8 + g];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+                dmma_8x8x4(acc[mi][ni][0], acc[mi][ni][1], av[mi], bv[ni]);
+    }
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+            *reinterpret_cast<double2 *>(gc + (wm + mi * 8 + g) * 64 + wn + ni * 8 + 2 * q) =
+                make_double2(acc[mi][ni][0], acc[mi][ni][1]);
+}
+
 // Update of a level whose pivots share target rows: one CTA per listed target, its
 // sources applied in ascending pivot order.
 template <typename T>
@@ -414,7 +707,7 @@ __global__ void __launch_bounds__(kThreads)
 template <typename T, typename V>
 __global__ void __launch_bounds__(kThreads)
     k_fwd_final(DevSym S, const T *__restrict__ slab, V *__restrict__ y, const V *__restrict__ scratch, int64_t p0,
-                int nrhs)
+                int nrhs, int stage_diag)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int64_t p = p0 + blockIdx.x;
@@ -431,8 +724,21 @@ __global__ void __launch_bounds__(kThreads)
             v -= part[j * m * nrhs + i];
         acc[i] = v;
     }
+    // The diagonal block goes to shared memory with an odd row stride (column reads of the
+    // substitution hit distinct banks) when it fits next to the accumulator.
+    const T *gd = slab + S.blk_off[S.diag_pos[k]];
+    const T *d = gd;
+    int ldd = m;
+    const size_t acc_bytes = ((size_t)m * nrhs * sizeof(V) + 15) / 16 * 16;
+    if (stage_diag)
+    {
+        T *sd = reinterpret_cast<T *>(smem_raw + acc_bytes);
+        ldd = m | 1;
+        for (int i = threadIdx.x; i < m * m; i += blockDim.x)
+            sd[(i / m) * ldd + i % m] = gd[i];
+        d = sd;
+    }
     __syncthreads();
-    const T *d = slab + S.blk_off[S.diag_pos[k]];
     // unit lower, then upper; one warp per right-hand side
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int r = warp; r < nrhs; r += nw)
@@ -442,17 +748,17 @@ __global__ void __launch_bounds__(kThreads)
             const V xi = acc[i * nrhs + r];
             __syncwarp();
             for (int q = i + 1 + lane; q < m; q += 32)
-                acc[q * nrhs + r] -= (V)d[(int64_t)q * m + i] * xi;
+                acc[q * nrhs + r] -= (V)d[(int64_t)q * ldd + i] * xi;
             __syncwarp();
         }
         for (int i = m - 1; i >= 0; --i)
         {
-            V xi = acc[i * nrhs + r] / (V)d[(int64_t)i * m + i];
+            V xi = acc[i * nrhs + r] / (V)d[(int64_t)i * ldd + i];
             __syncwarp();
             if (lane == 0)
                 acc[i * nrhs + r] = xi;
             for (int q = lane; q < i; q += 32)
-                acc[q * nrhs + r] -= (V)d[(int64_t)q * m + i] * xi;
+                acc[q * nrhs + r] -= (V)d[(int64_t)q * ldd + i] * xi;
             __syncwarp();
         }
     }

@@ -226,11 +226,13 @@ int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, co
 
     // ---- Per-pivot work prefixes (piv order) and flop count.
     S.trsm_pref.assign(n + 1, 0);
+    S.lu_pref.assign(n + 1, 0);
     S.upd_pref.assign(n + 1, 0);
     S.fwd_pref.assign(n + 1, 0);
     S.fwd_rows.assign(n + 1, 0);
     S.bwd_rows.assign(n + 1, 0);
     double flops = 0;
+    std::vector<double> piv_upd_flops(n), piv_upd_c(n), piv_upd_ab(n);
     for (int64_t p = 0; p < n; ++p)
     {
         const int64_t k = S.piv[p];
@@ -239,6 +241,7 @@ int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, co
         const int64_t n_lr = S.diag_pos[k] - S.row_ptr[k];
         const double m = S.size[k];
         S.trsm_pref[p + 1] = S.trsm_pref[p] + n_up;
+        S.lu_pref[p + 1] = S.lu_pref[p] + std::max<int64_t>(1, n_up);
         S.upd_pref[p + 1] = S.upd_pref[p] + n_lc * n_up;
         S.fwd_pref[p + 1] = S.fwd_pref[p] + n_lr;
         S.fwd_rows[p + 1] = S.fwd_rows[p] + n_lr * S.size[k];
@@ -249,6 +252,9 @@ int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, co
         for (int64_t j = S.lcol_ptr[k]; j < S.lcol_ptr[k + 1]; ++j)
             lc_rows += S.size[S.lcol_row[j]];
         flops += 2.0 / 3.0 * m * m * m + 2.0 * m * m * up_cols + 2.0 * lc_rows * m * up_cols;
+        piv_upd_flops[p] = 2.0 * lc_rows * m * up_cols;
+        piv_upd_c[p] = lc_rows * up_cols;
+        piv_upd_ab[p] = m * (lc_rows + up_cols);
     }
     S.factor_flops = flops;
 
@@ -266,17 +272,22 @@ int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, co
     for (int64_t l = 0; l < S.n_levels; ++l)
     {
         Symbolic::LevelShape &sh = S.shape[l];
-        bool uniform = true;
+        bool uniform = true, piv64 = true;
         bool conflict = false;
         for (int64_t p = S.lvl_ptr[l]; p < S.lvl_ptr[l + 1]; ++p)
         {
             const int64_t k = S.piv[p];
+            sh.upd_flops += piv_upd_flops[p];
+            sh.upd_c_elems += piv_upd_c[p];
+            sh.upd_ab_elems += piv_upd_ab[p];
             sh.max_piv = std::max(sh.max_piv, S.size[k]);
             uniform &= S.size[k] == 64;
+            piv64 &= S.size[k] == 64;
             for (int64_t j = S.diag_pos[k] + 1; j < S.row_ptr[k + 1]; ++j)
             {
                 sh.max_up = std::max(sh.max_up, S.size[S.cols[j]]);
                 uniform &= S.size[S.cols[j]] == 64;
+                piv64 &= S.size[S.cols[j]] == 64;
             }
             const bool has_up = S.row_ptr[k + 1] > S.diag_pos[k] + 1;
             for (int64_t j = S.lcol_ptr[k]; j < S.lcol_ptr[k + 1]; ++j)
@@ -294,6 +305,7 @@ int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, co
         }
         sh.max_col = sh.max_up;
         sh.uniform64 = uniform;
+        sh.piv64 = piv64;
         S.max_fwd_scratch_rows =
             std::max(S.max_fwd_scratch_rows, S.fwd_rows[S.lvl_ptr[l + 1]] - S.fwd_rows[S.lvl_ptr[l]]);
         S.max_bwd_scratch_rows =

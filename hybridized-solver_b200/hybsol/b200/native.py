@@ -64,6 +64,19 @@ class Analysis(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class KernelProfile(ctypes.Structure):
+    _fields_ = [
+        ("launches", ctypes.c_uint64),
+        ("total_ms", ctypes.c_double),
+        ("flops", ctypes.c_double),
+        ("c_elems", ctypes.c_double),
+        ("ab_elems", ctypes.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class HybError(RuntimeError):
     """A C-ABI call returned a non-success status."""
 
@@ -116,6 +129,8 @@ EXPORTS = {
     "hyb_get_block": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, _f64p]),
     "hyb_operations": (ctypes.c_int, [ctypes.c_void_p, _u64p, _i64p]),
     "hyb_last_launch_count": (ctypes.c_uint64, [ctypes.c_void_p]),
+    "hyb_profile_enable": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "hyb_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(KernelProfile)]),
     "hyb_block_lu": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_void_p, ctypes.c_int]),
     "hyb_block_lu_solve": (
         ctypes.c_int,

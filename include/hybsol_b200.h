@@ -187,6 +187,23 @@ HYB_API int hyb_operations(const hyb_system *sys, uint64_t *nops, int64_t *ops);
 /* Kernel launches issued by the last hyb_decompose / hyb_solve call (counted on the host). */
 HYB_API uint64_t hyb_last_launch_count(const hyb_system *sys);
 
+/* Profiling (no counterpart in the reference, which has no tracing) ------------- */
+
+typedef struct
+{
+    uint64_t launches; /* Schur-update kernel launches timed */
+    double total_ms;   /* sum of their device durations (CUDA events on the handle's stream) */
+    double flops;      /* algorithmic flops they performed */
+    double c_elems;    /* target scalars each read and written once */
+    double ab_elems;   /* operand scalars (lower-column and upper-row blocks) */
+} hyb_kernel_profile;
+
+/* When enabled, later decompositions record CUDA events around every level's
+ * Schur-update kernel inside the factorization graph; hyb_profile_read returns the
+ * totals of the last decomposition. */
+HYB_API int hyb_profile_enable(hyb_system *sys, int enable);
+HYB_API int hyb_profile_read(const hyb_system *sys, hyb_kernel_profile *update);
+
 /* Dense single-block kernels on device (the fine-grained surface of
  * src/block_system.c:938-1141) -------------------------------------------------- */
 
