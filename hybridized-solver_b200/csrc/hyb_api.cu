@@ -3,6 +3,7 @@
 // solves.
 #include "hyb_internal.h"
 #include "hyb_kernels.cuh"
+#include "hyb_umma.cuh"
 
 #include "hybsol_b200.h"
 
@@ -56,9 +57,13 @@ int smem_optin()
     return g_smem_optin;
 }
 
-template <typename K> void allow_smem(K kernel)
+// Lets `kernel` use up to `bytes` of dynamic shared memory; a failure is reported by the
+// return code and cleared, so a later launch check does not pick it up.
+template <typename K> cudaError_t allow_smem(K kernel, int bytes)
 {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin());
+    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaGetLastError();
+    return e;
 }
 
 __global__ void k_status_init(int *st)
@@ -90,6 +95,10 @@ struct hyb_system
     Symbolic S;
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr; // lookahead pivots (joined into `stream` inside graphs)
+    cudaEvent_t ev_prio = nullptr, ev_piv = nullptr, ev_join = nullptr;
+    bool lookahead = true;
+    bool umma = true; // mixed-form updates of 64-blocks on the tcgen05 tensor cores
     void *arena = nullptr;
     DevSym ds{};
     double *d_a = nullptr; // original values (FP64, CSR order)
@@ -124,6 +133,11 @@ struct hyb_system
         cudaFree(d_f64);
         cudaFree(d_f32);
         free_solve_buffers();
+        for (cudaEvent_t e : {ev_prio, ev_piv, ev_join})
+            if (e)
+                cudaEventDestroy(e);
+        if (stream2)
+            cudaStreamDestroy(stream2);
         if (stream)
             cudaStreamDestroy(stream);
     }
@@ -151,6 +165,17 @@ struct hyb_system
 namespace
 {
 
+cudaError_t create_streams(hyb_system *h)
+{
+    cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking);
+    for (cudaEvent_t *ev : {&h->ev_prio, &h->ev_piv, &h->ev_join})
+        if (e == cudaSuccess)
+            e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+    return e;
+}
+
 // Copies the symbolic arrays into one device allocation and fills the DevSym view.
 int upload_symbolic(hyb_system *h)
 {
@@ -177,6 +202,7 @@ int upload_symbolic(hyb_system *h)
         {S.trsm_pref.data(), S.trsm_pref.size() * 8, (const void **)&d.trsm_pref},
         {S.lu_pref.data(), S.lu_pref.size() * 8, (const void **)&d.lu_pref},
         {S.upd_pref.data(), S.upd_pref.size() * 8, (const void **)&d.upd_pref},
+        {S.upd2_pref.data(), S.upd2_pref.size() * 8, (const void **)&d.upd2_pref},
         {S.fwd_pref.data(), S.fwd_pref.size() * 8, (const void **)&d.fwd_pref},
         {S.fwd_rows.data(), S.fwd_rows.size() * 8, (const void **)&d.fwd_rows},
         {S.bwd_rows.data(), S.bwd_rows.size() * 8, (const void **)&d.bwd_rows},
@@ -219,50 +245,137 @@ template <typename T> int trsm_smem_bytes(int m)
     return (m * m + m * hyb::kTile) * (int)sizeof(T);
 }
 
-// Issues the whole factorization on the handle's stream (also used under capture).
-template <typename T> int enqueue_factor(hyb_system *h, T *slab, uint64_t &launches)
+// LU of the diagonal blocks of level l and the solves of their rows' upper blocks.
+// Launch errors are caught at the launch that caused them, naming the kernel and level.
+#define HYB_LAUNCHED(what, level)                                                                                      \
+    do                                                                                                                 \
+    {                                                                                                                  \
+        cudaError_t e_ = cudaGetLastError();                                                                           \
+        if (e_ != cudaSuccess)                                                                                         \
+            return cuda_fail(e_, (std::string(what) + " launch at level " + std::to_string(level)).c_str());          \
+    } while (0)
+
+template <typename T> int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cudaStream_t st, uint64_t &launches)
 {
     const Symbolic &S = h->S;
     const DevSym &ds = h->ds;
-    cudaStream_t st = h->stream;
     const int optin = smem_optin();
+    const int64_t p0 = S.lvl_ptr[l], p1 = S.lvl_ptr[l + 1];
+    const Symbolic::LevelShape &sh = S.shape[l];
+    if (sh.piv64)
+    {
+        // fused: 64x64 diagonal LU and the solves of the pivot rows' upper blocks
+        const int64_t units = S.lu_pref[p1] - S.lu_pref[p0];
+        hyb::k_lu_trsm64<T><<<(unsigned)units, hyb::kThreads, hyb::lu_trsm64_smem<T>(), st>>>(ds, slab, p0, p1,
+                                                                                              ds.lu_pref, h->d_status);
+        ++launches;
+        HYB_LAUNCHED("k_lu_trsm64", l);
+        return HYB_SUCCESS;
+    }
+    const int lu_bytes = lu_smem_bytes<T>(sh.max_piv);
+    if (lu_bytes <= optin)
+        hyb::k_lu<T, true><<<(unsigned)(p1 - p0), hyb::kThreads, lu_bytes, st>>>(ds, slab, p0, h->d_status);
+    else
+        hyb::k_lu<T, false><<<(unsigned)(p1 - p0), hyb::kThreads, 0, st>>>(ds, slab, p0, h->d_status);
+    ++launches;
+    HYB_LAUNCHED("k_lu", l);
+    const int64_t n_trsm = S.trsm_pref[p1] - S.trsm_pref[p0];
+    if (n_trsm > 0)
+    {
+        dim3 grid((unsigned)n_trsm, (unsigned)((sh.max_up + hyb::kTile - 1) / hyb::kTile));
+        const int bytes = trsm_smem_bytes<T>(sh.max_piv);
+        if (bytes <= optin)
+            hyb::k_trsm<T, true><<<grid, hyb::kThreads, bytes, st>>>(ds, slab, p0, p1);
+        else
+            hyb::k_trsm<T, false><<<grid, hyb::kThreads, 0, st>>>(ds, slab, p0, p1);
+        ++launches;
+        HYB_LAUNCHED("k_trsm", l);
+    }
+    return HYB_SUCCESS;
+}
+
+// Schur-complement updates of level l: mode 0 all of them, 1 / 2 the lookahead split.
+template <typename T> int enqueue_update(hyb_system *h, T *slab, int64_t l, cudaStream_t st, int mode,
+                                         uint64_t &launches)
+{
+    const Symbolic &S = h->S;
+    const DevSym &ds = h->ds;
+    const int64_t p0 = S.lvl_ptr[l], p1 = S.lvl_ptr[l + 1];
+    const Symbolic::LevelShape &sh = S.shape[l];
+    const unsigned tiles =
+        (unsigned)(((sh.max_row + hyb::kTile - 1) / hyb::kTile) * ((sh.max_col + hyb::kTile - 1) / hyb::kTile));
+    if (S.lvl_listed[l])
+    {
+        const int64_t q0 = S.mt_lvl_ptr[l], nq = S.mt_lvl_ptr[l + 1] - q0;
+        if (nq > 0)
+        {
+            hyb::k_update_listed<T><<<dim3((unsigned)nq, tiles), hyb::kThreads, 0, st>>>(ds, slab, q0);
+            ++launches;
+            HYB_LAUNCHED("k_update_listed", l);
+        }
+        return HYB_SUCCESS;
+    }
+    const int64_t nu =
+        mode == 0 ? S.upd_pref[p1] - S.upd_pref[p0] : (mode == 1 ? sh.la_prio_units : sh.la_rest_units);
+    if (nu <= 0)
+        return HYB_SUCCESS;
+    if constexpr (std::is_same_v<T, double>)
+    {
+        if (sh.uniform64)
+        {
+            hyb::k_update64_f64<<<(unsigned)nu, hyb::kUpd64Threads, hyb::kUpd64Smem, st>>>(
+                ds, slab, p0, p1, mode, sh.la_i0, sh.la_j0, h->d_status);
+            ++launches;
+            HYB_LAUNCHED("k_update64_f64", l);
+            return HYB_SUCCESS;
+        }
+    }
+    else
+    {
+        // mixed form: split-BF16 products on the tensor cores, two target rows per CTA
+        // (the small lookahead part stays on the CUDA-core kernel)
+        if (sh.uniform64 && h->umma && mode != 1)
+        {
+            const int64_t pairs = mode == 0 ? S.upd2_pref[p1] - S.upd2_pref[p0] : sh.la_rest_pairs;
+            if (pairs > 0)
+            {
+                hyb::k_update64_umma<<<(unsigned)pairs, hyb::kUmmaThreads, hyb::kUmmaSmem, st>>>(
+                    ds, slab, p0, p1, mode, sh.la_i0, sh.la_j0, h->d_status);
+                ++launches;
+                HYB_LAUNCHED("k_update64_umma", l);
+            }
+            return HYB_SUCCESS;
+        }
+    }
+    hyb::k_update<T><<<dim3((unsigned)nu, tiles), hyb::kThreads, 0, st>>>(ds, slab, p0, p1, mode, sh.la_i0,
+                                                                         sh.la_j0);
+    ++launches;
+    HYB_LAUNCHED("k_update", l);
+    return HYB_SUCCESS;
+}
+
+// Issues the whole factorization (used under graph capture). Levels run in order on the
+// handle's stream; where a level and the next each have one pivot, the next pivot's LU
+// and row solves run on the second stream as soon as the update of its own row and
+// column is done, overlapping the rest of this level's update (lookahead).
+template <typename T> int enqueue_factor(hyb_system *h, T *slab, uint64_t &launches)
+{
+    const Symbolic &S = h->S;
+    cudaStream_t st = h->stream, st2 = h->stream2;
+    HYB_CUDA(cudaGetLastError()); // nothing earlier may be blamed on this schedule
     k_status_init<<<1, 32, 0, st>>>(h->d_status);
     ++launches;
+    int rc = HYB_SUCCESS;
+    bool next_pivots_issued = false, forked = false;
     for (int64_t l = 0; l < S.n_levels; ++l)
     {
         const int64_t p0 = S.lvl_ptr[l], p1 = S.lvl_ptr[l + 1];
         const Symbolic::LevelShape &sh = S.shape[l];
-        if (sh.piv64)
-        {
-            // 1+2 fused: 64x64 diagonal LU and the solves of the pivot rows' upper blocks
-            const int64_t units = S.lu_pref[p1] - S.lu_pref[p0];
-            hyb::k_lu_trsm64<T><<<(unsigned)units, hyb::kThreads, 0, st>>>(ds, slab, p0, p1, ds.lu_pref,
-                                                                          h->d_status);
-            ++launches;
-        }
-        else
-        {
-        // 1. diagonal LU
-        const int lu_bytes = lu_smem_bytes<T>(sh.max_piv);
-        if (lu_bytes <= optin)
-            hyb::k_lu<T, true><<<(unsigned)(p1 - p0), hyb::kThreads, lu_bytes, st>>>(ds, slab, p0, h->d_status);
-        else
-            hyb::k_lu<T, false><<<(unsigned)(p1 - p0), hyb::kThreads, 0, st>>>(ds, slab, p0, h->d_status);
-        ++launches;
-        // 2. upper blocks of the pivot rows
-        const int64_t n_trsm = S.trsm_pref[p1] - S.trsm_pref[p0];
-        if (n_trsm > 0)
-        {
-            dim3 grid((unsigned)n_trsm, (unsigned)((sh.max_up + hyb::kTile - 1) / hyb::kTile));
-            const int bytes = trsm_smem_bytes<T>(sh.max_piv);
-            if (bytes <= optin)
-                hyb::k_trsm<T, true><<<grid, hyb::kThreads, bytes, st>>>(ds, slab, p0, p1);
-            else
-                hyb::k_trsm<T, false><<<grid, hyb::kThreads, 0, st>>>(ds, slab, p0, p1);
-            ++launches;
-        }
-        }
-        // 3. Schur-complement updates (optionally bracketed by profiling events)
+        if (next_pivots_issued)
+            HYB_CUDA(cudaStreamWaitEvent(st, h->ev_piv, 0));
+        else if ((rc = enqueue_pivots<T>(h, slab, l, st, launches)) != HYB_SUCCESS)
+            return rc;
+        next_pivots_issued = false;
         const bool timed = h->profile && (S.lvl_listed[l] ? S.mt_lvl_ptr[l + 1] > S.mt_lvl_ptr[l]
                                                           : S.upd_pref[p1] > S.upd_pref[p0]);
         if (timed)
@@ -273,42 +386,35 @@ template <typename T> int enqueue_factor(hyb_system *h, T *slab, uint64_t &launc
             h->prof_ev.push_back(e0);
             h->prof_ev.push_back(e1);
             h->prof_levels.push_back(l);
-            HYB_CUDA(cudaEventRecord(e0, st));
+            // external records become event nodes of the captured graph (a plain record
+            // under capture is only a dependency marker and never fires)
+            HYB_CUDA(cudaEventRecordWithFlags(e0, st, cudaEventRecordExternal));
         }
-        const unsigned tiles = (unsigned)(((sh.max_row + hyb::kTile - 1) / hyb::kTile) *
-                                          ((sh.max_col + hyb::kTile - 1) / hyb::kTile));
-        if (S.lvl_listed[l])
+        if (sh.lookahead && h->lookahead)
         {
-            const int64_t q0 = S.mt_lvl_ptr[l], nq = S.mt_lvl_ptr[l + 1] - q0;
-            if (nq > 0)
-            {
-                hyb::k_update_listed<T><<<dim3((unsigned)nq, tiles), hyb::kThreads, 0, st>>>(ds, slab, q0);
-                ++launches;
-            }
+            if ((rc = enqueue_update<T>(h, slab, l, st, 1, launches)) != HYB_SUCCESS)
+                return rc;
+            HYB_CUDA(cudaEventRecord(h->ev_prio, st));
+            HYB_CUDA(cudaStreamWaitEvent(st2, h->ev_prio, 0));
+            if ((rc = enqueue_pivots<T>(h, slab, l + 1, st2, launches)) != HYB_SUCCESS)
+                return rc;
+            HYB_CUDA(cudaEventRecord(h->ev_piv, st2));
+            if ((rc = enqueue_update<T>(h, slab, l, st, 2, launches)) != HYB_SUCCESS)
+                return rc;
+            next_pivots_issued = true;
+            forked = true;
         }
-        else
+        else if ((rc = enqueue_update<T>(h, slab, l, st, 0, launches)) != HYB_SUCCESS)
         {
-            const int64_t nu = S.upd_pref[p1] - S.upd_pref[p0];
-            if (nu > 0)
-            {
-                if constexpr (std::is_same_v<T, double>)
-                {
-                    if (sh.uniform64)
-                    {
-                        hyb::k_update64_f64<<<(unsigned)nu, hyb::kUpd64Threads, hyb::kUpd64Smem, st>>>(
-                            ds, slab, p0, p1, h->d_status);
-                        ++launches;
-                        if (timed)
-                            HYB_CUDA(cudaEventRecord(h->prof_ev.back(), st));
-                        continue;
-                    }
-                }
-                hyb::k_update<T><<<dim3((unsigned)nu, tiles), hyb::kThreads, 0, st>>>(ds, slab, p0, p1);
-                ++launches;
-            }
+            return rc;
         }
         if (timed)
-            HYB_CUDA(cudaEventRecord(h->prof_ev.back(), st));
+            HYB_CUDA(cudaEventRecordWithFlags(h->prof_ev.back(), st, cudaEventRecordExternal));
+    }
+    if (forked)
+    {
+        HYB_CUDA(cudaEventRecord(h->ev_join, st2));
+        HYB_CUDA(cudaStreamWaitEvent(st, h->ev_join, 0));
     }
     HYB_CUDA(cudaGetLastError());
     return HYB_SUCCESS;
@@ -575,7 +681,7 @@ HYB_API int hyb_system_create(uint64_t n, const uint64_t *block_sizes, const uin
         return HYB_FAILED_ALLOC;
     }
     HYB_CUDA(cudaGetDevice(&h->device));
-    HYB_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    HYB_CUDA(create_streams(h.get()));
     int rc = upload_symbolic(h.get());
     if (rc != HYB_SUCCESS)
         return rc;
@@ -612,7 +718,9 @@ HYB_API int hyb_system_copy(const hyb_system *src, hyb_system **out)
         return HYB_FAILED_ALLOC;
     }
     h->device = src->device;
-    HYB_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->lookahead = src->lookahead;
+    h->umma = src->umma;
+    HYB_CUDA(create_streams(h.get()));
     int rc = upload_symbolic(h.get());
     if (rc != HYB_SUCCESS)
         return rc;
@@ -653,6 +761,32 @@ HYB_API void *hyb_system_stream(const hyb_system *h)
     return h ? (void *)h->stream : nullptr;
 }
 
+HYB_API int hyb_system_set_option(hyb_system *h, int option, int64_t value)
+{
+    if (check_handle(h))
+        return HYB_INVALID_ARGUMENT;
+    switch (option)
+    {
+    case HYB_OPTION_LOOKAHEAD:
+        if (h->lookahead != (value != 0))
+        {
+            h->lookahead = value != 0;
+            h->g_factor[0].reset();
+            h->g_factor[1].reset();
+        }
+        return HYB_SUCCESS;
+    case HYB_OPTION_TENSOR_CORE_MIXED:
+        if (h->umma != (value != 0))
+        {
+            h->umma = value != 0;
+            h->g_factor[1].reset();
+        }
+        return HYB_SUCCESS;
+    default:
+        return HYB_INVALID_ARGUMENT;
+    }
+}
+
 HYB_API int hyb_system_set_values(hyb_system *h, const double *values, int memory)
 {
     if (check_handle(h) || (!values && h->S.a_val_off.back() > 0))
@@ -677,14 +811,22 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
     static bool attrs_set = false;
     if (!attrs_set)
     {
-        allow_smem(hyb::k_lu<double, true>);
-        allow_smem(hyb::k_lu<float, true>);
-        allow_smem(hyb::k_trsm<double, true>);
-        allow_smem(hyb::k_trsm<float, true>);
-        allow_smem(hyb::k_fwd_final<double, double>);
-        allow_smem(hyb::k_fwd_final<float, float>);
-        allow_smem(hyb::k_dense_lu);
-        allow_smem(hyb::k_update64_f64);
+        const int optin = smem_optin();
+        const cudaError_t errs[] = {
+            allow_smem(hyb::k_lu<double, true>, optin),
+            allow_smem(hyb::k_lu<float, true>, optin),
+            allow_smem(hyb::k_trsm<double, true>, optin),
+            allow_smem(hyb::k_trsm<float, true>, optin),
+            allow_smem(hyb::k_fwd_final<double, double>, optin),
+            allow_smem(hyb::k_fwd_final<float, float>, optin),
+            allow_smem(hyb::k_update64_f64, hyb::kUpd64Smem),
+            allow_smem(hyb::k_lu_trsm64<double>, hyb::lu_trsm64_smem<double>()),
+            allow_smem(hyb::k_lu_trsm64<float>, hyb::lu_trsm64_smem<float>()),
+            allow_smem(hyb::k_update64_umma, hyb::kUmmaSmem),
+        };
+        for (cudaError_t e : errs)
+            if (e != cudaSuccess)
+                return cuda_fail(e, "cudaFuncSetAttribute(MaxDynamicSharedMemorySize)");
         attrs_set = true;
     }
     h->last_launches = 0;
@@ -1012,7 +1154,12 @@ HYB_API int hyb_profile_read(const hyb_system *h, hyb_kernel_profile *out)
     for (size_t i = 0; i < h->prof_levels.size(); ++i)
     {
         float ms = 0;
-        HYB_CUDA(cudaEventElapsedTime(&ms, h->prof_ev[2 * i], h->prof_ev[2 * i + 1]));
+        const cudaError_t e = cudaEventElapsedTime(&ms, h->prof_ev[2 * i], h->prof_ev[2 * i + 1]);
+        if (e != cudaSuccess)
+        {
+            cudaGetLastError();
+            return cuda_fail(e, "cudaEventElapsedTime");
+        }
         const auto &sh = h->S.shape[h->prof_levels[i]];
         out->launches += 1;
         out->total_ms += ms;
@@ -1038,7 +1185,7 @@ HYB_API int hyb_block_lu(uint64_t m, double *a, int memory)
     if (memory != HYB_MEMORY_DEVICE)
         HYB_CUDA(cudaMemcpy(d, a, bytes, cudaMemcpyHostToDevice));
     k_status_init<<<1, 32>>>(st);
-    allow_smem(hyb::k_dense_lu);
+    allow_smem(hyb::k_dense_lu, smem_optin());
     if ((int)bytes <= smem_optin())
         hyb::k_dense_lu<<<1, hyb::kThreads, bytes>>>(d, (int)m, st);
     else

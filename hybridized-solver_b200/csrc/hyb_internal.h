@@ -49,6 +49,7 @@ struct Symbolic
     std::vector<int64_t> trsm_pref; // [n+1] prefix (in piv order) of upper-block counts
     std::vector<int64_t> lu_pref;   // [n+1] prefix of max(1, upper-block count): fused LU+solve units
     std::vector<int64_t> upd_pref;  // [n+1] prefix of |lower column| * |upper row|
+    std::vector<int64_t> upd2_pref; // [n+1] prefix of ceil(|lower column| / 2) * |upper row| (row pairs)
     std::vector<int64_t> fwd_pref;  // [n+1] prefix of lower-row block counts (forward solve units)
     std::vector<int64_t> fwd_rows;  // [n+1] prefix of lower-row block count * pivot size (scratch rows)
     std::vector<int64_t> bwd_rows;  // [n+1] prefix of upper-row block count * pivot size
@@ -77,6 +78,17 @@ struct Symbolic
         double upd_flops = 0;   // algorithmic flops of the level's Schur updates
         double upd_c_elems = 0; // scalars of the update targets (each read and written once)
         double upd_ab_elems = 0; // scalars of the lower-column and upper-row operand blocks
+        // Lookahead: when this level and the next each have one pivot and this level's
+        // update reaches the next pivot's row or column, the update is split into the
+        // targets in that row/column (la_i0: position of the next pivot in this pivot's
+        // lower column, la_j0: in its upper row; -1 if absent) and the rest, so the next
+        // pivot can be factored while the rest runs.
+        bool lookahead = false;
+        int32_t la_i0 = -1;
+        int32_t la_j0 = -1;
+        int64_t la_prio_units = 0;
+        int64_t la_rest_units = 0;
+        int64_t la_rest_pairs = 0; // row-pair units of the rest (kernels that take two target rows)
     };
     std::vector<LevelShape> shape;
 

@@ -35,6 +35,7 @@ struct DevSym
     const int64_t *trsm_pref;
     const int64_t *lu_pref;
     const int64_t *upd_pref;
+    const int64_t *upd2_pref;
     const int64_t *fwd_pref;
     const int64_t *fwd_rows;
     const int64_t *bwd_rows;
@@ -271,37 +272,73 @@ __device__ void lu64_shared(T *d, T *rowbuf, T *colbuf, int *status, int row_id)
             atomicMin(status + ST_FIRST_BAD, row_id);
         }
         const T rp = T(1) / p;
+        // this thread's slices of the pivot row and column, read once per step
+        T urow[4], lcol[4];
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+            urow[b] = rowbuf[cur + tx * 4 + b];
 #pragma unroll
         for (int a = 0; a < 4; ++a)
-        {
-            const int r = ty * 4 + a;
-            if (r <= i)
-                continue;
-            const T l = colbuf[cur + r] * rp;
+            lcol[a] = colbuf[cur + ty * 4 + a];
+        // Branch-free rank-1 update: multipliers of rows at or above i and pivot-row entries
+        // at or left of i are zeroed, so the 16 FMAs leave those entries unchanged; only
+        // the four threads holding column i then store its multipliers.
+        T lm[4], um[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+            lm[a] = ty * 4 + a > i ? lcol[a] * rp : T(0);
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+            um[b] = tx * 4 + b > i ? urow[b] : T(0);
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
 #pragma unroll
             for (int b = 0; b < 4; ++b)
-            {
-                const int c = tx * 4 + b;
-                if (c == i)
-                    v[a][b] = l;
-                else if (c > i)
-                    v[a][b] -= l * rowbuf[cur + c];
-            }
-        }
-        if (i + 1 < 64)
+                v[a][b] -= lm[a] * um[b];
+        if (tx == (i >> 2))
         {
-            const int n1 = i + 1;
+            const int bi = i & 3;
 #pragma unroll
             for (int a = 0; a < 4; ++a)
+            {
+                if (ty * 4 + a > i)
+                {
+                    v[a][0] = bi == 0 ? lm[a] : v[a][0];
+                    v[a][1] = bi == 1 ? lm[a] : v[a][1];
+                    v[a][2] = bi == 2 ? lm[a] : v[a][2];
+                    v[a][3] = bi == 3 ? lm[a] : v[a][3];
+                }
+            }
+        }
+        // publish row i+1 (held by the threads with ty == (i+1)/4) and column i+1
+        const int n1 = i + 1;
+        if (n1 < 64)
+        {
+            const int ar = n1 & 3, bc = n1 & 3;
+            if (ty == (n1 >> 2))
+            {
 #pragma unroll
                 for (int b = 0; b < 4; ++b)
                 {
-                    const int r = ty * 4 + a, c = tx * 4 + b;
-                    if (r == n1 && c >= n1)
-                        rowbuf[nxt + c] = v[a][b];
-                    if (c == n1 && r > n1)
-                        colbuf[nxt + r] = v[a][b];
+                    T rv = v[0][b];
+                    rv = ar == 1 ? v[1][b] : rv;
+                    rv = ar == 2 ? v[2][b] : rv;
+                    rv = ar == 3 ? v[3][b] : rv;
+                    rowbuf[nxt + tx * 4 + b] = rv;
                 }
+            }
+            if (tx == (n1 >> 2))
+            {
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+                {
+                    T cv = v[a][0];
+                    cv = bc == 1 ? v[a][1] : cv;
+                    cv = bc == 2 ? v[a][2] : cv;
+                    cv = bc == 3 ? v[a][3] : cv;
+                    colbuf[nxt + ty * 4 + a] = cv;
+                }
+            }
         }
         __syncthreads();
     }
@@ -313,40 +350,65 @@ __device__ void lu64_shared(T *d, T *rowbuf, T *colbuf, int *status, int row_id)
     __syncthreads();
 }
 
-// X = U^{-1} L^{-1} B for a 64x64 block B in place in global memory, D factored in shared
-// memory. Four lanes share a column; lane q of a column holds rows q, q+4, ..., q+60 in
-// registers, so each substitution step is one shuffle and predicated FMAs, no barrier.
-template <typename T> __device__ void trsm64_columns(const T *d, T *gb)
+// Transposed copy of a factored 64x64 block for the column solves: dt[c][r] = D[r][c], each
+// row of dt split into four 16-entry quarters with two padding entries between them, so
+// the four quarter-reads of a warp fall in distinct banks.
+constexpr int kLdT = 72;
+
+__device__ __forceinline__ int dt_idx(int c, int r)
+{
+    return c * kLdT + r + 2 * (r >> 4);
+}
+
+// X = U^{-1} L^{-1} B for a 64x64 block B in place in global memory. The factored block is
+// held in shared memory as two transposed, pre-masked triangles: dtl[i][r] = L[r][i] for
+// r > i (zero elsewhere) and dtu[i][r] = U[r][i] for r < i (zero elsewhere), with the
+// pivots in diag. Four lanes share a column; lane q of a column holds rows 16q .. 16q+15
+// in registers, so a substitution step is one shuffle, eight 16-byte shared loads and 16
+// FMAs, with no barrier and no per-row test.
+template <typename T> __device__ void trsm64_columns(const T *dtl, const T *dtu, const T *diag, T *gb)
 {
     const int tid = threadIdx.x, lane = tid & 31;
     const int col = tid >> 2, q = tid & 3, base = lane & ~3;
     T x[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j)
-        x[j] = gb[(4 * j + q) * 64 + col];
+        x[j] = gb[(16 * q + j) * 64 + col];
 #pragma unroll
     for (int i = 0; i < 63; ++i)
     {
-        const T xi = __shfl_sync(0xffffffffu, x[i >> 2], base + (i & 3));
+        const T *dc = dtl + i * kLdT + 18 * q; // L[16q + j][i] = dc[j]
+        T dv[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j)
-            if (4 * j + q > i)
-                x[j] -= d[(4 * j + q) * kLd65 + i] * xi;
+            dv[j] = dc[j];
+        const T xi = __shfl_sync(0xffffffffu, x[i & 15], base + (i >> 4));
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+            x[j] -= dv[j] * xi;
     }
 #pragma unroll
     for (int i = 63; i >= 0; --i)
     {
-        const T xi = __shfl_sync(0xffffffffu, x[i >> 2], base + (i & 3)) / d[i * kLd65 + i];
-        if ((i & 3) == q)
-            x[i >> 2] = xi;
+        const T *dc = dtu + i * kLdT + 18 * q; // U[16q + j][i] = dc[j]
+        T dv[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j)
-            if (4 * j + q < i)
-                x[j] -= d[(4 * j + q) * kLd65 + i] * xi;
+            dv[j] = dc[j];
+        const T xi = __shfl_sync(0xffffffffu, x[i & 15], base + (i >> 4)) / diag[i];
+        x[i & 15] = (i >> 4) == q ? xi : x[i & 15];
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+            x[j] -= dv[j] * xi;
     }
 #pragma unroll
     for (int j = 0; j < 16; ++j)
-        gb[(4 * j + q) * 64 + col] = x[j];
+        gb[(16 * q + j) * 64 + col] = x[j];
+}
+
+template <typename T> constexpr int lu_trsm64_smem()
+{
+    return (64 * kLd65 + 2 * 64 * kLdT + 64 + 256) * (int)sizeof(T);
 }
 
 // One CTA per upper block of the level's (64-row) pivots; every CTA factors its pivot's
@@ -354,13 +416,17 @@ template <typename T> __device__ void trsm64_columns(const T *d, T *gb)
 // solves its block. A pivot without upper blocks gets one CTA for the LU alone: the grid
 // is the level's work units with empty pivots counted once (see enqueue_factor).
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 1)
     k_lu_trsm64(DevSym S, T *__restrict__ slab, int64_t p0, int64_t p1, const int64_t *__restrict__ unit_pref,
                 int *status)
 {
-    __shared__ T d[64 * kLd65];
-    __shared__ T rowbuf[128];
-    __shared__ T colbuf[128];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *d = reinterpret_cast<T *>(smem_raw);
+    T *dtl = d + 64 * kLd65;
+    T *dtu = dtl + 64 * kLdT;
+    T *diag = dtu + 64 * kLdT;
+    T *rowbuf = diag + 64;
+    T *colbuf = rowbuf + 128;
     const int64_t u = unit_pref[p0] + blockIdx.x;
     const int64_t p = find_owner(unit_pref, p0, p1, u);
     const int64_t k = S.piv[p];
@@ -374,8 +440,19 @@ __global__ void __launch_bounds__(kThreads)
         for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
             gd[i] = d[(i >> 6) * kLd65 + (i & 63)];
     const int64_t blk = S.diag_pos[k] + 1 + j;
-    if (blk < S.row_ptr[k + 1])
-        trsm64_columns(d, slab + S.blk_off[blk]);
+    if (blk >= S.row_ptr[k + 1])
+        return;
+    for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
+    {
+        const int c = i >> 6, r = i & 63;
+        const T v = d[r * kLd65 + c];
+        dtl[dt_idx(c, r)] = r > c ? v : T(0);
+        dtu[dt_idx(c, r)] = r < c ? v : T(0);
+        if (r == c)
+            diag[c] = v;
+    }
+    __syncthreads();
+    trsm64_columns(dtl, dtu, diag, slab + S.blk_off[blk]);
 }
 
 // ----------------------------------------------------------------------------------
@@ -451,20 +528,66 @@ __device__ __forceinline__ void tile_sub_ab(TileAcc<T> &acc, const T *__restrict
     }
 }
 
-// Update of a level whose pivots touch disjoint target rows. grid.x enumerates
-// (pivot, lower row i, upper column j) through upd_pref; grid.y the 64x64 tiles.
+// Work units of an update launch. mode 0: grid.x enumerates every (pivot, lower row i,
+// upper column j) of the level's pivots through upd_pref. Lookahead launches (one pivot):
+// mode 1 takes the pairs in row i0 and column j0 only (the next pivot's row and column),
+// mode 2 every other pair.
+struct UpdUnit
+{
+    int64_t k, li, bu; // pivot, index into lcol_*, index into cols (the upper block)
+};
+
+__device__ __forceinline__ UpdUnit update_unit(const DevSym &S, int64_t p0, int64_t p1, int mode, int i0, int j0)
+{
+    int64_t p = p0, local = blockIdx.x;
+    if (mode == 0)
+    {
+        const int64_t u = S.upd_pref[p0] + blockIdx.x;
+        p = find_owner(S.upd_pref, p0, p1, u);
+        local = u - S.upd_pref[p];
+    }
+    const int64_t k = S.piv[p];
+    const int64_t n_up = S.row_ptr[k + 1] - S.diag_pos[k] - 1;
+    int64_t i, j;
+    if (mode == 0)
+    {
+        i = local / n_up;
+        j = local % n_up;
+    }
+    else if (mode == 1)
+    {
+        if (i0 >= 0 && local < n_up)
+        {
+            i = i0;
+            j = local;
+        }
+        else
+        {
+            const int64_t l2 = local - (i0 >= 0 ? n_up : 0);
+            i = (i0 >= 0 && l2 >= i0) ? l2 + 1 : l2;
+            j = j0;
+        }
+    }
+    else
+    {
+        const int64_t nu = n_up - (j0 >= 0 ? 1 : 0);
+        const int64_t a = local / nu, b = local % nu;
+        i = (i0 >= 0 && a >= i0) ? a + 1 : a;
+        j = (j0 >= 0 && b >= j0) ? b + 1 : b;
+    }
+    return {k, S.lcol_ptr[k] + i, S.diag_pos[k] + 1 + j};
+}
+
+// Update of a level whose pivots touch disjoint target rows; grid.x: work units (see
+// update_unit), grid.y: the 64x64 tiles of a target block.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_update(DevSym S, T *__restrict__ slab, int64_t p0, int64_t p1)
+__global__ void __launch_bounds__(kThreads)
+    k_update(DevSym S, T *__restrict__ slab, int64_t p0, int64_t p1, int mode, int i0, int j0)
 {
     __shared__ __align__(16) T sa[kTile * kTileK];
     __shared__ __align__(16) T sb[kTile * kTileK];
-    const int64_t u = S.upd_pref[p0] + blockIdx.x;
-    const int64_t p = find_owner(S.upd_pref, p0, p1, u);
-    const int64_t k = S.piv[p];
-    const int64_t local = u - S.upd_pref[p];
-    const int64_t n_up = S.row_ptr[k + 1] - S.diag_pos[k] - 1;
-    const int64_t li = S.lcol_ptr[k] + local / n_up;
-    const int64_t bu = S.diag_pos[k] + 1 + local % n_up;
+    const UpdUnit w = update_unit(S, p0, p1, mode, i0, j0);
+    const int64_t k = w.k, li = w.li, bu = w.bu;
     const int32_t t = S.lcol_row[li];
     const int32_t c = S.cols[bu];
     const int M = S.size[t], N = S.size[c], K = S.size[k];
@@ -552,20 +675,16 @@ constexpr int kUpd64Smem = 2 * 64 * kLd64 * 8 + 16;
 // shared memory while the CTA reads C into DMMA accumulator fragments; four warps each
 // own a 32x32 quarter of C (16 m8n8k4 tiles). Work units as in k_update.
 __global__ void __launch_bounds__(kUpd64Threads)
-    k_update64_f64(DevSym S, double *__restrict__ slab, int64_t p0, int64_t p1, int *status)
+    k_update64_f64(DevSym S, double *__restrict__ slab, int64_t p0, int64_t p1, int mode, int i0, int j0,
+                   int *status)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double *sa = reinterpret_cast<double *>(smem_raw);
     double *sb = sa + 64 * kLd64;
     uint64_t *bar = reinterpret_cast<uint64_t *>(sb + 64 * kLd64);
 
-    const int64_t u = S.upd_pref[p0] + blockIdx.x;
-    const int64_t p = find_owner(S.upd_pref, p0, p1, u);
-    const int64_t k = S.piv[p];
-    const int64_t local = u - S.upd_pref[p];
-    const int64_t n_up = S.row_ptr[k + 1] - S.diag_pos[k] - 1;
-    const int64_t li = S.lcol_ptr[k] + local / n_up;
-    const int64_t bu = S.diag_pos[k] + 1 + local % n_up;
+    const UpdUnit w = update_unit(S, p0, p1, mode, i0, j0);
+    const int64_t li = w.li, bu = w.bu;
     const int32_t t = S.lcol_row[li];
     const int32_t c = S.cols[bu];
     const int64_t tgt = find_col(S.cols, S.row_ptr[t], S.row_ptr[t + 1], c);

@@ -228,6 +228,7 @@ int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, co
     S.trsm_pref.assign(n + 1, 0);
     S.lu_pref.assign(n + 1, 0);
     S.upd_pref.assign(n + 1, 0);
+    S.upd2_pref.assign(n + 1, 0);
     S.fwd_pref.assign(n + 1, 0);
     S.fwd_rows.assign(n + 1, 0);
     S.bwd_rows.assign(n + 1, 0);
@@ -243,6 +244,7 @@ int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, co
         S.trsm_pref[p + 1] = S.trsm_pref[p] + n_up;
         S.lu_pref[p + 1] = S.lu_pref[p] + std::max<int64_t>(1, n_up);
         S.upd_pref[p + 1] = S.upd_pref[p] + n_lc * n_up;
+        S.upd2_pref[p + 1] = S.upd2_pref[p] + (n_lc + 1) / 2 * n_up;
         S.fwd_pref[p + 1] = S.fwd_pref[p] + n_lr;
         S.fwd_rows[p + 1] = S.fwd_rows[p] + n_lr * S.size[k];
         S.bwd_rows[p + 1] = S.bwd_rows[p] + n_up * S.size[k];
@@ -350,6 +352,34 @@ int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, co
                 S.mt_src_ptr.push_back((int64_t)S.mt_src_k.size());
         }
         S.mt_lvl_ptr[l + 1] = (int64_t)S.mt_tgt.size();
+    }
+
+    // ---- Lookahead between consecutive single-pivot levels.
+    for (int64_t l = 0; l + 1 < S.n_levels; ++l)
+    {
+        Symbolic::LevelShape &sh = S.shape[l];
+        if (S.lvl_listed[l] || S.lvl_ptr[l + 1] - S.lvl_ptr[l] != 1 || S.lvl_ptr[l + 2] - S.lvl_ptr[l + 1] != 1)
+            continue;
+        const int64_t k = S.piv[S.lvl_ptr[l]], kn = S.piv[S.lvl_ptr[l + 1]];
+        const int64_t n_lc = S.lcol_ptr[k + 1] - S.lcol_ptr[k];
+        const int64_t n_up = S.row_ptr[k + 1] - S.diag_pos[k] - 1;
+        if (n_lc == 0 || n_up == 0)
+            continue;
+        int32_t i0 = -1, j0 = -1;
+        for (int64_t a = 0; a < n_lc; ++a)
+            if (S.lcol_row[S.lcol_ptr[k] + a] == kn)
+                i0 = (int32_t)a;
+        for (int64_t b = 0; b < n_up; ++b)
+            if (S.cols[S.diag_pos[k] + 1 + b] == kn)
+                j0 = (int32_t)b;
+        if (i0 < 0 && j0 < 0)
+            continue;
+        sh.lookahead = true;
+        sh.la_i0 = i0;
+        sh.la_j0 = j0;
+        sh.la_prio_units = (i0 >= 0 ? n_up : 0) + (j0 >= 0 ? n_lc : 0) - (i0 >= 0 && j0 >= 0 ? 1 : 0);
+        sh.la_rest_units = (n_lc - (i0 >= 0)) * (n_up - (j0 >= 0));
+        sh.la_rest_pairs = (n_lc - (i0 >= 0) + 1) / 2 * (n_up - (j0 >= 0));
     }
     return HYB_SUCCESS;
 }

@@ -106,6 +106,7 @@ EXPORTS = {
     "hyb_system_value_count": (ctypes.c_uint64, [ctypes.c_void_p]),
     "hyb_system_dof": (ctypes.c_uint64, [ctypes.c_void_p]),
     "hyb_system_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "hyb_system_set_option": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64]),
     "hyb_decompose": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(DecomposeInfo)]),
     "hyb_solve": (
         ctypes.c_int,
@@ -269,6 +270,12 @@ class NativeSystem:
         h = ctypes.c_void_p()
         _check(lib().hyb_system_copy(self._h, ctypes.byref(h)), "hyb_system_copy")
         return NativeSystem(None, None, None, _handle=h)
+
+    def set_lookahead(self, enable: bool):
+        _check(lib().hyb_system_set_option(self._h, 0, 1 if enable else 0), "hyb_system_set_option")
+
+    def set_tensor_core_mixed(self, enable: bool):
+        _check(lib().hyb_system_set_option(self._h, 1, 1 if enable else 0), "hyb_system_set_option")
 
     @property
     def stream(self) -> int:

@@ -147,6 +147,20 @@ HYB_API uint64_t hyb_system_dof(const hyb_system *sys);
 /* The handle's CUDA stream (a cudaStream_t as void*), for callers that time or order work. */
 HYB_API void *hyb_system_stream(const hyb_system *sys);
 
+typedef enum
+{
+    /* 1 (default): between consecutive single-pivot stages, factor the next pivot on a
+     * second stream while the current stage's update finishes; 0: strictly in order.
+     * Both give the same factors. */
+    HYB_OPTION_LOOKAHEAD = 0,
+    /* 1 (default): in the mixed form, the 64x64 Schur updates run on the tcgen05 tensor
+     * cores as three BF16 products of a hi/lo split; 0: FP32 CUDA-core updates. */
+    HYB_OPTION_TENSOR_CORE_MIXED = 1
+} hyb_option;
+
+/* Sets a schedule option of the handle (takes effect at the next decomposition). */
+HYB_API int hyb_system_set_option(hyb_system *sys, int option, int64_t value);
+
 /* Decomposition and solve -------------------------------------------------------- */
 
 /* Factors the system in the given precision: replaces block_system_decompose

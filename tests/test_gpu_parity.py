@@ -217,6 +217,45 @@ def test_zero_pivot_is_reported_not_raised(gpu):
     assert info["zero_pivots"] >= 1 and info["first_bad_pivot"] == 0
 
 
+@pytest.mark.parametrize("prec", [0, 1])
+def test_lookahead_schedule_matches_in_order(gpu, prec):
+    """The lookahead schedule (next pivot on a second stream) gives the in-order factors."""
+    mat, b = _mesh(12, 8, seed=13)
+    order, pm, ns = _native_from(gpu, mat)
+    bn = reorder_rhs(mat.sizes, order, b)
+    ns.decompose(prec)
+    blocks = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
+    ns.set_lookahead(False)
+    ns.set_values(pm.vals)
+    ns.decompose(prec)
+    blocks2 = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
+    assert all(np.array_equal(x, y) for x, y in zip(blocks, blocks2))
+
+
+@pytest.mark.parametrize("n", [5, 12])
+def test_tensor_core_mixed_matches_cuda_core_mixed(gpu, n):
+    """The tcgen05 split-BF16 updates and the FP32 CUDA-core updates both refine to 1e-12
+    and agree on the solution; the tensor-core factors stay within BF16x3 accuracy."""
+    mat, b = _mesh(n, 8, seed=17)
+    order, pm, ns = _native_from(gpu, mat)
+    bn = reorder_rhs(mat.sizes, order, b)
+    ns.decompose(gpu.FP64)
+    x64, _ = ns.solve(bn)
+    f64 = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
+    ns.set_values(pm.vals)
+    ns.decompose(gpu.MIXED)
+    ftc = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
+    xtc, itc = ns.solve(bn)
+    ns.set_tensor_core_mixed(False)
+    ns.set_values(pm.vals)
+    ns.decompose(gpu.MIXED)
+    xcc, icc = ns.solve(bn)
+    assert itc["converged"] and icc["converged"]
+    assert rel_err(xtc, x64) < TOL_X_MIXED and rel_err(xcc, x64) < TOL_X_MIXED
+    worst = max(rel_err(a, b) for a, b in zip(ftc, f64))
+    assert worst < 1e-3, worst
+
+
 def test_refactorization_reuses_the_handle(gpu):
     mat, b = _mesh(8, 4, seed=9)
     order, pm, ns = _native_from(gpu, mat)
