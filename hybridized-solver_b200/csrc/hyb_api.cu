@@ -333,10 +333,11 @@ template <typename T> int enqueue_update(hyb_system *h, T *slab, int64_t l, cuda
     else
     {
         // mixed form: split-BF16 products on the tensor cores, two target rows per CTA
-        // (the small lookahead part stays on the CUDA-core kernel)
-        if (sh.uniform64 && h->umma && mode != 1)
+        if (sh.uniform64 && h->umma)
         {
-            const int64_t pairs = mode == 0 ? S.upd2_pref[p1] - S.upd2_pref[p0] : sh.la_rest_pairs;
+            const int64_t pairs = mode == 0   ? S.upd2_pref[p1] - S.upd2_pref[p0]
+                                  : mode == 1 ? sh.la_prio_pairs
+                                              : sh.la_rest_pairs;
             if (pairs > 0)
             {
                 hyb::k_update64_umma<<<(unsigned)pairs, hyb::kUmmaThreads, hyb::kUmmaSmem, st>>>(

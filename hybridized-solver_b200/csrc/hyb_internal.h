@@ -88,6 +88,7 @@ struct Symbolic
         int32_t la_j0 = -1;
         int64_t la_prio_units = 0;
         int64_t la_rest_units = 0;
+        int64_t la_prio_pairs = 0; // units of the two-row kernels: row i0 one row at a time, column j0 in pairs
         int64_t la_rest_pairs = 0; // row-pair units of the rest (kernels that take two target rows)
     };
     std::vector<LevelShape> shape;

@@ -380,6 +380,7 @@ int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, co
         sh.la_prio_units = (i0 >= 0 ? n_up : 0) + (j0 >= 0 ? n_lc : 0) - (i0 >= 0 && j0 >= 0 ? 1 : 0);
         sh.la_rest_units = (n_lc - (i0 >= 0)) * (n_up - (j0 >= 0));
         sh.la_rest_pairs = (n_lc - (i0 >= 0) + 1) / 2 * (n_up - (j0 >= 0));
+        sh.la_prio_pairs = (i0 >= 0 ? n_up : 0) + (j0 >= 0 ? (n_lc - (i0 >= 0) + 1) / 2 : 0);
     }
     return HYB_SUCCESS;
 }

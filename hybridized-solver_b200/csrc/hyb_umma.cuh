@@ -86,8 +86,10 @@ __device__ __forceinline__ void split_store4(unsigned char *hi, unsigned char *l
 // Uniform-64 FP32 update on the tensor cores. One CTA owns two target blocks of the same
 // column block c and consecutive rows t_a, t_b of the pivot's lower column (M = 128 rows,
 // N = 64): C(t,c) -= A(t,k) * U(k,c). Units: mode 0 enumerates row pairs of every pivot
-// of the level through upd2_pref; mode 2 (one pivot, lookahead rest) the row pairs and
-// columns other than the next pivot's (i0, j0).
+// of the level through upd2_pref; with one pivot and lookahead, mode 1 takes row i0
+// (one row per unit, every column) and then column j0 (row pairs of the other rows), and
+// mode 2 the row pairs and columns other than (i0, j0). Each target row's arithmetic is
+// the same whichever rows share its tile, so all modes give identical results.
 __global__ void __launch_bounds__(kUmmaThreads)
     k_update64_umma(DevSym S, float *__restrict__ slab, int64_t p0, int64_t p1, int mode, int i0, int j0,
                     int *status)
@@ -113,21 +115,49 @@ __global__ void __launch_bounds__(kUmmaThreads)
     const int64_t k = S.piv[p];
     const int64_t n_lc = S.lcol_ptr[k + 1] - S.lcol_ptr[k];
     const int64_t n_up = S.row_ptr[k + 1] - S.diag_pos[k] - 1;
-    const int64_t rows = n_lc - (mode == 2 && i0 >= 0 ? 1 : 0);
-    const int64_t cols = n_up - (mode == 2 && j0 >= 0 ? 1 : 0);
-    const int64_t pr = local / cols;
-    int64_t jj = local % cols;
-    int64_t ia = 2 * pr, ib = 2 * pr + 1;
-    const bool has_b = ib < rows;
-    if (mode == 2)
+    int64_t ia, ib, jj;
+    bool has_b;
+    if (mode == 1 && i0 >= 0 && local < n_up)
     {
+        ia = i0; // the next pivot's row, alone
+        ib = i0;
+        jj = local;
+        has_b = false;
+    }
+    else if (mode == 1)
+    {
+        // the next pivot's column: row pairs of every row except i0
+        const int64_t pr = local - (i0 >= 0 ? n_up : 0);
+        const int64_t rows = n_lc - (i0 >= 0 ? 1 : 0);
+        ia = 2 * pr;
+        ib = 2 * pr + 1;
+        has_b = ib < rows;
         if (i0 >= 0)
         {
             ia += ia >= i0;
             ib += ib >= i0;
         }
-        if (j0 >= 0)
-            jj += jj >= j0;
+        jj = j0;
+    }
+    else
+    {
+        const int64_t rows = n_lc - (mode == 2 && i0 >= 0 ? 1 : 0);
+        const int64_t cols = n_up - (mode == 2 && j0 >= 0 ? 1 : 0);
+        const int64_t pr = local / cols;
+        jj = local % cols;
+        ia = 2 * pr;
+        ib = 2 * pr + 1;
+        has_b = ib < rows;
+        if (mode == 2)
+        {
+            if (i0 >= 0)
+            {
+                ia += ia >= i0;
+                ib += ib >= i0;
+            }
+            if (j0 >= 0)
+                jj += jj >= j0;
+        }
     }
     const int64_t la = S.lcol_ptr[k] + ia, lb = S.lcol_ptr[k] + ib;
     const int64_t bu = S.diag_pos[k] + 1 + jj;
