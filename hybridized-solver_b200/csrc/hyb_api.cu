@@ -1273,3 +1273,73 @@ HYB_API int hyb_block_gemm(uint64_t m, uint64_t k, uint64_t n, const double *a, 
 }
 
 } // extern "C"
+
+// ------------------------------------------------------------------------------------
+// Allocation-free FP64 solve (hyb_solve_fp64_noalloc).
+//
+// The per-stage partial block products of the substitution go to this fixed array
+// instead of buffers the handle allocates. In host code `g_noalloc_scratch` only names
+// the symbol; its device address is looked up once per device with cudaGetSymbolAddress.
+// The partials are written before they are read in every stage, so the contents a previous
+// call left need no clearing.
+static __device__ __align__(256) double g_noalloc_scratch[HYB_NOALLOC_SCRATCH_DOUBLES];
+
+namespace
+{
+constexpr int kMaxDevices = 64;
+double *g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device (looked up on first use).
+int noalloc_scratch(int device, double **out)
+{
+    if (device < 0 || device >= kMaxDevices)
+        return HYB_INVALID_ARGUMENT;
+    if (!g_noalloc_ptr[device])
+    {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        g_noalloc_ptr[device] = static_cast<double *>(p);
+    }
+    *out = g_noalloc_ptr[device];
+    return HYB_SUCCESS;
+}
+} // namespace
+
+extern "C" HYB_API int hyb_solve_fp64_noalloc(hyb_system *h, const double *b, double *x, uint64_t nrhs)
+{
+    if (check_handle(h) || !b || !x || nrhs == 0 || nrhs > 1024)
+        return HYB_INVALID_ARGUMENT;
+    if (h->factored != HYB_PRECISION_FP64 || !h->d_f64)
+        return HYB_NOT_DECOMPOSED;
+    const Symbolic &S = h->S;
+    const int64_t need = std::max(S.max_fwd_scratch_rows, S.max_bwd_scratch_rows) * (int64_t)nrhs;
+    if (need > (int64_t)HYB_NOALLOC_SCRATCH_DOUBLES)
+    {
+        g_cuda_error = "solve scratch of " + std::to_string(need) + " doubles exceeds the fixed array of " +
+                       std::to_string(HYB_NOALLOC_SCRATCH_DOUBLES);
+        return HYB_TOO_LARGE;
+    }
+    for (int64_t l = 0; l < S.n_levels; ++l)
+        if ((int64_t)S.shape[l].max_piv * (int64_t)nrhs * 8 > smem_optin())
+            return HYB_TOO_LARGE;
+    int dev = 0;
+    HYB_CUDA(cudaGetDevice(&dev));
+    if (dev != h->device)
+        return HYB_INVALID_ARGUMENT;
+    double *scratch = nullptr;
+    int rc = noalloc_scratch(dev, &scratch);
+    if (rc != HYB_SUCCESS)
+        return rc;
+    const int64_t dof = S.dof_off[S.n];
+    if (x != b)
+        HYB_CUDA(cudaMemcpyAsync(x, b, dof * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    uint64_t launches = 0;
+    rc = enqueue_solve<double, double>(h, h->d_f64, x, scratch, (int)nrhs, launches);
+    if (rc != HYB_SUCCESS)
+        return rc;
+    HYB_CUDA(cudaStreamSynchronize(h->stream));
+    h->last_launches = launches;
+    return HYB_SUCCESS;
+}

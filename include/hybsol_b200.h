@@ -184,6 +184,25 @@ HYB_API int hyb_solve(hyb_system *sys, const double *b, double *x, uint64_t nrhs
 /* FP64 residual r = b - A x against the original values (device or host vectors). */
 HYB_API int hyb_residual(hyb_system *sys, const double *b, const double *x, double *r, uint64_t nrhs, int memory);
 
+/* Allocation-free FP64 solve. No counterpart in the reference: it exists for callers that
+ * must not allocate device memory when they solve -- for example a host application
+ * whose own memory pool already holds the device memory it may use (a cudaMalloc there
+ * fails or breaks its budget), or a time-stepping loop that cannot afford the device-wide
+ * synchronization cudaMalloc/cudaFree imply. Such a caller creates and factors the
+ * handle (HYB_PRECISION_FP64) up front and then calls this entry point, which performs
+ * no allocation of any kind: `b` and `x` are the caller's device buffers (dof x nrhs,
+ * row-major; they may alias) and the solve's scratch for partial block products lives in
+ * a fixed array inside this library, HYB_NOALLOC_SCRATCH_DOUBLES doubles (8 MiB) that every
+ * GPU which loads the library keeps until the process exits. Requests whose scratch would
+ * exceed it (per stage: pivot rows x lower blocks x nrhs) are rejected with HYB_TOO_LARGE.
+ * The first call on a device looks up that array's device address (once per device, with
+ * the device current); make that first call before any stream capture. All calls share
+ * the one array: calls that overlap on the GPU -- from two threads, or on two handles of
+ * the same device -- race on it. The call returns after the solve has finished on the
+ * handle's stream. The results equal hyb_solve's for the same factors. */
+#define HYB_NOALLOC_SCRATCH_DOUBLES (1u << 20)
+HYB_API int hyb_solve_fp64_noalloc(hyb_system *sys, const double *b, double *x, uint64_t nrhs);
+
 /* Access after decomposition ------------------------------------------------------ */
 
 /* Number of blocks in row `row` of the filled pattern (before decomposition: original). */
