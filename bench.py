@@ -58,7 +58,29 @@ def parse_args():
     ap.add_argument("--cpu-sample-mesh", type=int, default=CPU_SAMPLE_MESH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-profile", action="store_true", help="do not time the dominant kernel with events")
+    ap.add_argument(
+        "--single",
+        action="store_true",
+        help="one decompose + solve per form and nothing else (the command ncu captures run)",
+    )
     return ap.parse_args()
+
+
+def run_single(args):
+    """One FP64 and one mixed decompose + solve of the workload, for profilers."""
+    import numpy as np
+
+    from hybsol.b200 import native
+
+    pm, bn = build_workload(args.mesh, args.p)
+    ns = native.NativeSystem.from_matrix(pm)
+    for prec in (native.FP64, native.MIXED):
+        ns.set_values(pm.vals)
+        ns.decompose(prec)
+        x, info = ns.solve(bn)
+        assert np.isfinite(x).all() and info["relative_residual"] < 1e-10, info
+    ns.close()
+    return 0
 
 
 def workload_config(n, p, extra=None):
@@ -525,6 +547,8 @@ def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.single:
+        return run_single(args)
     return run_ours(args)
 
 

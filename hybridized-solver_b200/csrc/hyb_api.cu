@@ -57,11 +57,37 @@ int smem_optin()
     return g_smem_optin;
 }
 
+// Dynamic shared memory the forward solve stage may take (its static ticket flag aside).
+int solve_smem_cap()
+{
+    return smem_optin() - 1024;
+}
+
+// Streaming multiprocessors of the current device.
+int g_sm_count = 0;
+
+int sm_count()
+{
+    if (g_sm_count == 0)
+    {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        g_sm_count = v > 0 ? v : 1;
+    }
+    return g_sm_count;
+}
+
 // Lets `kernel` use up to `bytes` of dynamic shared memory; a failure is reported by the
 // return code and cleared, so a later launch check does not pick it up.
 template <typename K> cudaError_t allow_smem(K kernel, int bytes)
 {
-    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    // dynamic + static shared memory may not exceed the opt-in limit
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 std::min<int>(bytes, smem_optin() - (int)fa.sharedSizeBytes));
     cudaGetLastError();
     return e;
 }
@@ -103,9 +129,13 @@ struct hyb_system
     DevSym ds{};
     double *d_a = nullptr; // original values (FP64, CSR order)
     int *d_status = nullptr;
+    int *d_tickets = nullptr; // per pivot: partial products of the solve stage already published
     int factored = -1; // -1, HYB_PRECISION_FP64 or HYB_PRECISION_MIXED
     double *d_f64 = nullptr;
     float *d_f32 = nullptr;
+    // BF16 operand splits of tensor-core levels, two level-parity halves of split_half bytes
+    unsigned char *d_ops = nullptr;
+    size_t split_half = 0;
     // solve buffers, sized for buf_nrhs right-hand sides
     int64_t buf_nrhs = 0;
     double *d_b = nullptr, *d_x = nullptr, *d_r = nullptr, *d_scr64 = nullptr, *d_part = nullptr, *d_norm = nullptr;
@@ -130,8 +160,10 @@ struct hyb_system
         cudaFree(arena);
         cudaFree(d_a);
         cudaFree(d_status);
+        cudaFree(d_tickets);
         cudaFree(d_f64);
         cudaFree(d_f32);
+        cudaFree(d_ops);
         free_solve_buffers();
         for (cudaEvent_t e : {ev_prio, ev_piv, ev_join})
             if (e)
@@ -203,7 +235,10 @@ int upload_symbolic(hyb_system *h)
         {S.lu_pref.data(), S.lu_pref.size() * 8, (const void **)&d.lu_pref},
         {S.upd_pref.data(), S.upd_pref.size() * 8, (const void **)&d.upd_pref},
         {S.upd2_pref.data(), S.upd2_pref.size() * 8, (const void **)&d.upd2_pref},
+        {S.split_pref.data(), S.split_pref.size() * 8, (const void **)&d.split_pref},
+        {S.tc_pref.data(), S.tc_pref.size() * 8, (const void **)&d.tc_pref},
         {S.fwd_pref.data(), S.fwd_pref.size() * 8, (const void **)&d.fwd_pref},
+        {S.fwdu_pref.data(), S.fwdu_pref.size() * 8, (const void **)&d.fwdu_pref},
         {S.fwd_rows.data(), S.fwd_rows.size() * 8, (const void **)&d.fwd_rows},
         {S.bwd_rows.data(), S.bwd_rows.size() * 8, (const void **)&d.bwd_rows},
         {S.mt_tgt.data(), S.mt_tgt.size() * 4, (const void **)&d.mt_tgt},
@@ -255,6 +290,37 @@ template <typename T> int trsm_smem_bytes(int m)
             return cuda_fail(e_, (std::string(what) + " launch at level " + std::to_string(level)).c_str());          \
     } while (0)
 
+// Whether level l's Schur update runs on the tensor cores (mixed form, 64-blocks).
+template <typename T> bool tc_level(const hyb_system *h, int64_t l)
+{
+    return std::is_same_v<T, float> && h->umma && h->d_ops && !h->S.lvl_listed[l] && h->S.shape[l].uniform64;
+}
+
+unsigned char *level_ops(hyb_system *h, int64_t l)
+{
+    return h->d_ops + (size_t)(l & 1) * h->split_half;
+}
+
+// BF16 split of a tensor-core level's operands, once its pivots are factored.
+template <typename T> int enqueue_split(hyb_system *h, T *slab, int64_t l, cudaStream_t st, uint64_t &launches)
+{
+    if constexpr (std::is_same_v<T, float>)
+    {
+        const Symbolic &S = h->S;
+        if (!tc_level<T>(h, l))
+            return HYB_SUCCESS;
+        const int64_t p0 = S.lvl_ptr[l], p1 = S.lvl_ptr[l + 1];
+        const int64_t blocks = S.split_pref[p1] - S.split_pref[p0];
+        if (blocks > 0)
+        {
+            hyb::k_split64<<<(unsigned)blocks, hyb::kSplitThreads, 0, st>>>(h->ds, slab, level_ops(h, l), p0, p1);
+            ++launches;
+            HYB_LAUNCHED("k_split64", l);
+        }
+    }
+    return HYB_SUCCESS;
+}
+
 template <typename T> int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cudaStream_t st, uint64_t &launches)
 {
     const Symbolic &S = h->S;
@@ -270,7 +336,7 @@ template <typename T> int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cuda
                                                                                               ds.lu_pref, h->d_status);
         ++launches;
         HYB_LAUNCHED("k_lu_trsm64", l);
-        return HYB_SUCCESS;
+        return enqueue_split<T>(h, slab, l, st, launches);
     }
     const int lu_bytes = lu_smem_bytes<T>(sh.max_piv);
     if (lu_bytes <= optin)
@@ -291,7 +357,7 @@ template <typename T> int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cuda
         ++launches;
         HYB_LAUNCHED("k_trsm", l);
     }
-    return HYB_SUCCESS;
+    return enqueue_split<T>(h, slab, l, st, launches);
 }
 
 // Schur-complement updates of level l: mode 0 all of them, 1 / 2 the lookahead split.
@@ -332,18 +398,19 @@ template <typename T> int enqueue_update(hyb_system *h, T *slab, int64_t l, cuda
     }
     else
     {
-        // mixed form: split-BF16 products on the tensor cores, two target rows per CTA
-        if (sh.uniform64 && h->umma)
+        // mixed form: split-BF16 products on the tensor cores, persistent CTAs (two per SM)
+        if (tc_level<T>(h, l))
         {
-            const int64_t pairs = mode == 0   ? S.upd2_pref[p1] - S.upd2_pref[p0]
-                                  : mode == 1 ? sh.la_prio_pairs
-                                              : sh.la_rest_pairs;
-            if (pairs > 0)
+            const int64_t tiles = mode == 0   ? S.tc_pref[p1] - S.tc_pref[p0]
+                                  : mode == 1 ? sh.la_prio_tiles
+                                              : sh.la_rest_tiles;
+            if (tiles > 0)
             {
-                hyb::k_update64_umma<<<(unsigned)pairs, hyb::kUmmaThreads, hyb::kUmmaSmem, st>>>(
-                    ds, slab, p0, p1, mode, sh.la_i0, sh.la_j0, h->d_status);
+                const unsigned grid = (unsigned)std::min<int64_t>(tiles, 2 * (int64_t)sm_count());
+                hyb::k_update64_tc<<<grid, hyb::kTcThreads, hyb::kTcSmem, st>>>(
+                    ds, slab, level_ops(h, l), p0, p1, mode, sh.la_i0, sh.la_j0, tiles, h->d_status);
                 ++launches;
-                HYB_LAUNCHED("k_update64_umma", l);
+                HYB_LAUNCHED("k_update64_tc", l);
             }
             return HYB_SUCCESS;
         }
@@ -428,21 +495,18 @@ template <typename T, typename V> int enqueue_solve(hyb_system *h, const T *slab
     const Symbolic &S = h->S;
     const DevSym &ds = h->ds;
     cudaStream_t st = h->stream;
+    // tickets return to zero after every stage; clearing them guards against an aborted solve
+    HYB_CUDA(cudaMemsetAsync(h->d_tickets, 0, S.n * sizeof(int), st));
     for (int64_t l = 0; l < S.n_levels; ++l)
     {
         const int64_t p0 = S.lvl_ptr[l], p1 = S.lvl_ptr[l + 1];
-        const int64_t units = S.fwd_pref[p1] - S.fwd_pref[p0];
-        if (units > 0)
-        {
-            hyb::k_fwd_partial<T, V><<<(unsigned)units, hyb::kThreads, 0, st>>>(ds, slab, y, scratch, p0, p1, nrhs);
-            ++launches;
-        }
+        const int64_t units = S.fwdu_pref[p1] - S.fwdu_pref[p0];
         const int mp = S.shape[l].max_piv;
         const int acc_bytes = (mp * nrhs * (int)sizeof(V) + 15) / 16 * 16;
         const int diag_bytes = mp * (mp | 1) * (int)sizeof(T);
-        const int stage = acc_bytes + diag_bytes <= smem_optin() ? 1 : 0;
-        hyb::k_fwd_final<T, V><<<(unsigned)(p1 - p0), hyb::kThreads, acc_bytes + (stage ? diag_bytes : 0), st>>>(
-            ds, slab, y, scratch, p0, nrhs, stage);
+        const int stage = acc_bytes + diag_bytes <= solve_smem_cap() ? 1 : 0;
+        hyb::k_fwd_stage<T, V><<<(unsigned)units, hyb::kThreads, acc_bytes + (stage ? diag_bytes : 0), st>>>(
+            ds, slab, y, scratch, h->d_tickets, p0, p1, nrhs, stage);
         ++launches;
     }
     for (int64_t l = S.n_levels - 1; l >= 0; --l)
@@ -451,9 +515,9 @@ template <typename T, typename V> int enqueue_solve(hyb_system *h, const T *slab
         const int64_t units = S.trsm_pref[p1] - S.trsm_pref[p0];
         if (units == 0)
             continue;
-        hyb::k_bwd_partial<T, V><<<(unsigned)units, hyb::kThreads, 0, st>>>(ds, slab, y, scratch, p0, p1, nrhs);
-        hyb::k_bwd_final<V><<<(unsigned)(p1 - p0), hyb::kThreads, 0, st>>>(ds, y, scratch, p0, nrhs);
-        launches += 2;
+        hyb::k_bwd_stage<T, V><<<(unsigned)units, hyb::kThreads, 0, st>>>(ds, slab, y, scratch, h->d_tickets, p0,
+                                                                         p1, nrhs);
+        ++launches;
     }
     HYB_CUDA(cudaGetLastError());
     return HYB_SUCCESS;
@@ -689,6 +753,8 @@ HYB_API int hyb_system_create(uint64_t n, const uint64_t *block_sizes, const uin
     HYB_CUDA(cudaMalloc(&h->d_a, std::max<int64_t>(1, h->S.a_val_off.back()) * sizeof(double)));
     HYB_CUDA(cudaMemsetAsync(h->d_a, 0, std::max<int64_t>(1, h->S.a_val_off.back()) * sizeof(double), h->stream));
     HYB_CUDA(cudaMalloc(&h->d_status, hyb::ST_WORDS * sizeof(int)));
+    HYB_CUDA(cudaMalloc(&h->d_tickets, h->S.n * sizeof(int)));
+    HYB_CUDA(cudaMemsetAsync(h->d_tickets, 0, h->S.n * sizeof(int), h->stream));
     HYB_CUDA(cudaStreamSynchronize(h->stream));
     *out = h.release();
     return HYB_SUCCESS;
@@ -728,6 +794,8 @@ HYB_API int hyb_system_copy(const hyb_system *src, hyb_system **out)
     const size_t a_bytes = std::max<int64_t>(1, h->S.a_val_off.back()) * sizeof(double);
     HYB_CUDA(cudaMalloc(&h->d_a, a_bytes));
     HYB_CUDA(cudaMalloc(&h->d_status, hyb::ST_WORDS * sizeof(int)));
+    HYB_CUDA(cudaMalloc(&h->d_tickets, h->S.n * sizeof(int)));
+    HYB_CUDA(cudaMemsetAsync(h->d_tickets, 0, h->S.n * sizeof(int), h->stream));
     HYB_CUDA(cudaStreamSynchronize(src->stream));
     HYB_CUDA(cudaMemcpyAsync(h->d_a, src->d_a, a_bytes, cudaMemcpyDeviceToDevice, h->stream));
     const size_t slab = std::max<int64_t>(1, h->S.slab_elems());
@@ -818,12 +886,12 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
             allow_smem(hyb::k_lu<float, true>, optin),
             allow_smem(hyb::k_trsm<double, true>, optin),
             allow_smem(hyb::k_trsm<float, true>, optin),
-            allow_smem(hyb::k_fwd_final<double, double>, optin),
-            allow_smem(hyb::k_fwd_final<float, float>, optin),
+            allow_smem(hyb::k_fwd_stage<double, double>, optin),
+            allow_smem(hyb::k_fwd_stage<float, float>, optin),
             allow_smem(hyb::k_update64_f64, hyb::kUpd64Smem),
             allow_smem(hyb::k_lu_trsm64<double>, hyb::lu_trsm64_smem<double>()),
             allow_smem(hyb::k_lu_trsm64<float>, hyb::lu_trsm64_smem<float>()),
-            allow_smem(hyb::k_update64_umma, hyb::kUmmaSmem),
+            allow_smem(hyb::k_update64_tc, hyb::kTcSmem),
         };
         for (cudaError_t e : errs)
             if (e != cudaSuccess)
@@ -873,6 +941,12 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
             HYB_CUDA(cudaMalloc(&h->d_f32, slab * sizeof(float)));
             h->g_factor[1].reset();
             h->g_solve.clear();
+        }
+        if (h->umma && !h->d_ops && S.max_split_blocks > 0)
+        {
+            h->split_half = (size_t)S.max_split_blocks * hyb::kSplitBytes;
+            HYB_CUDA(cudaMalloc(&h->d_ops, 2 * h->split_half));
+            h->g_factor[1].reset();
         }
         HYB_CUDA(cudaMemsetAsync(h->d_f32, 0, slab * sizeof(float), h->stream));
         hyb::k_scatter<float><<<sgrid, hyb::kThreads, 0, h->stream>>>(h->ds, h->d_a, h->d_f32, S.nnz_a());
@@ -937,7 +1011,7 @@ HYB_API int hyb_solve(hyb_system *h, const double *b, double *x, uint64_t nrhs, 
         return HYB_NOT_DECOMPOSED;
     const Symbolic &S = h->S;
     for (int64_t l = 0; l < S.n_levels; ++l)
-        if ((int64_t)S.shape[l].max_piv * (int64_t)nrhs * 8 > smem_optin())
+        if ((int64_t)S.shape[l].max_piv * (int64_t)nrhs * 8 > solve_smem_cap())
             return HYB_TOO_LARGE;
     int rc = ensure_solve_buffers(h, (int64_t)nrhs);
     if (rc != HYB_SUCCESS)
@@ -1322,7 +1396,7 @@ extern "C" HYB_API int hyb_solve_fp64_noalloc(hyb_system *h, const double *b, do
         return HYB_TOO_LARGE;
     }
     for (int64_t l = 0; l < S.n_levels; ++l)
-        if ((int64_t)S.shape[l].max_piv * (int64_t)nrhs * 8 > smem_optin())
+        if ((int64_t)S.shape[l].max_piv * (int64_t)nrhs * 8 > solve_smem_cap())
             return HYB_TOO_LARGE;
     int dev = 0;
     HYB_CUDA(cudaGetDevice(&dev));

@@ -50,7 +50,10 @@ struct Symbolic
     std::vector<int64_t> lu_pref;   // [n+1] prefix of max(1, upper-block count): fused LU+solve units
     std::vector<int64_t> upd_pref;  // [n+1] prefix of |lower column| * |upper row|
     std::vector<int64_t> upd2_pref; // [n+1] prefix of ceil(|lower column| / 2) * |upper row| (row pairs)
-    std::vector<int64_t> fwd_pref;  // [n+1] prefix of lower-row block counts (forward solve units)
+    std::vector<int64_t> split_pref; // [n+1] prefix of n_lc + n_up: blocks whose BF16 split a tensor-core level stages
+    std::vector<int64_t> tc_pref;    // [n+1] prefix of n_lc * ceil(n_up / 2): tensor-core update tiles
+    std::vector<int64_t> fwd_pref;  // [n+1] prefix of lower-row block counts
+    std::vector<int64_t> fwdu_pref; // [n+1] prefix of max(1, lower-row block count): forward solve units
     std::vector<int64_t> fwd_rows;  // [n+1] prefix of lower-row block count * pivot size (scratch rows)
     std::vector<int64_t> bwd_rows;  // [n+1] prefix of upper-row block count * pivot size
 
@@ -90,9 +93,12 @@ struct Symbolic
         int64_t la_rest_units = 0;
         int64_t la_prio_pairs = 0; // units of the two-row kernels: row i0 one row at a time, column j0 in pairs
         int64_t la_rest_pairs = 0; // row-pair units of the rest (kernels that take two target rows)
+        int64_t la_prio_tiles = 0; // tensor-core tiles (one target row x two columns): row i0, then column j0
+        int64_t la_rest_tiles = 0; // tensor-core tiles of the rest
     };
     std::vector<LevelShape> shape;
 
+    int64_t max_split_blocks = 0;     // max over uniform-64 levels of the split_pref span
     int64_t max_fwd_scratch_rows = 0; // max over levels of fwd_rows span
     int64_t max_bwd_scratch_rows = 0;
     double factor_flops = 0;          // exact algorithmic flops of the factorization

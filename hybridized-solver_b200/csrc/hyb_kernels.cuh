@@ -36,7 +36,10 @@ struct DevSym
     const int64_t *lu_pref;
     const int64_t *upd_pref;
     const int64_t *upd2_pref;
+    const int64_t *split_pref;
+    const int64_t *tc_pref;
     const int64_t *fwd_pref;
+    const int64_t *fwdu_pref;
     const int64_t *fwd_rows;
     const int64_t *bwd_rows;
     const int32_t *mt_tgt;
@@ -608,13 +611,27 @@ __global__ void __launch_bounds__(kThreads)
 
 // ----------------------------------------------------------------------------------
 // Bulk async copies (the non-tensor TMA path) into shared memory, completed on an
-// mbarrier. Waits are bounded: a wait that runs out records ST_TIMEOUT and the CTA skips
-// its arithmetic instead of spinning forever.
+// mbarrier. Waits are bounded in time: a wait that runs out records ST_TIMEOUT and the CTA
+// skips its arithmetic instead of spinning forever; once ST_TIMEOUT is set, CTAs that start
+// later return at once, so a failed schedule ends within about one wait limit.
 enum
 {
     ST_TIMEOUT = 3
 };
-constexpr uint32_t kSpinLimit = 1u << 24;
+constexpr uint64_t kWaitLimitNs = 1000000000ull; // 1 s
+
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Whether an earlier wait of this schedule ran out (read by one thread, broadcast by the caller).
+__device__ __forceinline__ int schedule_aborted(const int *status)
+{
+    return *reinterpret_cast<const volatile int *>(status + ST_TIMEOUT);
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
@@ -641,20 +658,27 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
                  : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase)
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity)
 {
-    for (uint32_t i = 0; i < kSpinLimit; ++i)
-    {
-        uint32_t done;
-        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                     "selp.u32 %0, 1, 0, p;\n\t}"
-                     : "=r"(done)
-                     : "r"(smem_u32(bar)), "r"(phase)
-                     : "memory");
-        if (done)
-            return true;
-    }
-    return false;
+    uint32_t done;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(done)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return done != 0;
+}
+
+// Waits for the phase of the given parity to complete; false after kWaitLimitNs.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+{
+    if (mbar_try(bar, parity))
+        return true;
+    const uint64_t t0 = global_ns();
+    while (!mbar_try(bar, parity))
+        if (global_ns() - t0 > kWaitLimitNs)
+            return false;
+    return true;
 }
 
 // FP64 tensor-core MMA: d(8x8) += a(8x4) * b(4x8). Lane l holds a[l/4][l%4],
@@ -693,12 +717,19 @@ __global__ void __launch_bounds__(kUpd64Threads)
     double *gc = slab + S.blk_off[tgt];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    __shared__ int s_abort;
     if (tid == 0)
     {
-        mbar_init(bar, 1);
-        mbar_expect_tx(bar, 2 * 64 * 64 * 8);
+        s_abort = schedule_aborted(status);
+        if (!s_abort)
+        {
+            mbar_init(bar, 1);
+            mbar_expect_tx(bar, 2 * 64 * 64 * 8);
+        }
     }
     __syncthreads();
+    if (s_abort)
+        return;
     if (warp == 0)
     {
         // 64 rows of A and 64 rows of U, 512 bytes each, two per lane
@@ -724,6 +755,7 @@ __global__ void __launch_bounds__(kUpd64Threads)
     {
         if (lane == 0)
             atomicOr(status + ST_TIMEOUT, 1);
+        mbar_wait(bar, 0); // the copies in flight land before the CTA leaves, or a second limit passes
         return;
     }
 #pragma unroll 4
@@ -804,43 +836,59 @@ __device__ __forceinline__ void block_gemv(const T *__restrict__ blk, int m, int
     }
 }
 
-// Forward partials: unit u = one lower block (k, s) of a pivot in [p0, p1).
-template <typename T, typename V>
-__global__ void __launch_bounds__(kThreads)
-    k_fwd_partial(DevSym S, const T *__restrict__ slab, const V *__restrict__ y, V *__restrict__ scratch, int64_t p0,
-                  int64_t p1, int nrhs)
+// One launch per stage and direction. Every CTA of a pivot forms one partial product (a
+// block of the pivot's lower row, forward, or upper row, backward, against the vector),
+// publishes it and takes a ticket; the CTA that takes the pivot's last ticket finishes the
+// pivot -- sums the partials in ascending block order and, forward, applies D^{-1}. No CTA
+// waits for another, so nothing can stall; the ticket is reset for the next solve.
+// Returns true in the CTA that must finish pivot p.
+__device__ __forceinline__ bool last_ticket(int *tickets, int64_t p, int64_t nparts)
 {
-    const int64_t u = S.fwd_pref[p0] + blockIdx.x;
-    const int64_t p = find_owner(S.fwd_pref, p0, p1, u);
-    const int64_t k = S.piv[p];
-    const int64_t j = u - S.fwd_pref[p];
-    const int64_t blk = S.row_ptr[k] + j;
-    const int32_t s = S.cols[blk];
-    const int m = S.size[k];
-    const int64_t row = S.fwd_rows[p] - S.fwd_rows[p0] + j * m;
-    block_gemv(slab + S.blk_off[blk], m, S.size[s], y + S.dof_off[s] * nrhs, scratch + row * nrhs, nrhs);
+    __shared__ int s_last;
+    __threadfence(); // this CTA's partial is visible before its ticket is taken
+    __syncthreads();
+    if (threadIdx.x == 0)
+        s_last = atomicAdd(tickets + p, 1) == (int)(nparts - 1);
+    __syncthreads();
+    if (!s_last)
+        return false;
+    __threadfence();
+    if (threadIdx.x == 0)
+        tickets[p] = 0;
+    return true;
 }
 
-// Forward finish of pivot k: y_k <- D_k^{-1} (y_k - sum of its partials), partials summed
-// in ascending source order (block_system_apply_operations, src/blocks.c:729-769).
+// Forward stage: y_k <- D_k^{-1} (y_k - sum_s L(k,s) y_s) for the stage's pivots
+// (block_system_apply_operations, src/blocks.c:729-769). Units: fwdu_pref, one per lower
+// block of a pivot (at least one per pivot).
 template <typename T, typename V>
 __global__ void __launch_bounds__(kThreads)
-    k_fwd_final(DevSym S, const T *__restrict__ slab, V *__restrict__ y, const V *__restrict__ scratch, int64_t p0,
-                int nrhs, int stage_diag)
+    k_fwd_stage(DevSym S, const T *__restrict__ slab, V *__restrict__ y, V *__restrict__ scratch,
+                int *__restrict__ tickets, int64_t p0, int64_t p1, int nrhs, int stage_diag)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int64_t p = p0 + blockIdx.x;
+    const int64_t u = S.fwdu_pref[p0] + blockIdx.x;
+    const int64_t p = find_owner(S.fwdu_pref, p0, p1, u);
     const int64_t k = S.piv[p];
     const int m = S.size[k];
     const int64_t nparts = S.diag_pos[k] - S.row_ptr[k];
+    V *part = scratch + (S.fwd_rows[p] - S.fwd_rows[p0]) * nrhs;
+    if (nparts > 0)
+    {
+        const int64_t j = u - S.fwdu_pref[p];
+        const int64_t blk = S.row_ptr[k] + j;
+        const int32_t src = S.cols[blk];
+        block_gemv(slab + S.blk_off[blk], m, S.size[src], y + S.dof_off[src] * nrhs, part + j * m * nrhs, nrhs);
+        if (!last_ticket(tickets, p, nparts))
+            return;
+    }
     V *acc = reinterpret_cast<V *>(smem_raw); // m * nrhs
     V *yk = y + S.dof_off[k] * nrhs;
-    const V *part = scratch + (S.fwd_rows[p] - S.fwd_rows[p0]) * nrhs;
     for (int i = threadIdx.x; i < m * nrhs; i += blockDim.x)
     {
         V v = yk[i];
         for (int64_t j = 0; j < nparts; ++j)
-            v -= part[j * m * nrhs + i];
+            v -= __ldcg(part + j * m * nrhs + i);
         acc[i] = v;
     }
     // The diagonal block goes to shared memory with an odd row stride (column reads of the
@@ -886,40 +934,31 @@ __global__ void __launch_bounds__(kThreads)
         yk[i] = acc[i];
 }
 
-// Backward partials: unit u = one upper block (k, c).
+// Backward stage: y_k -= sum_c U(k,c) y_c over the upper blocks of the stage's pivots
+// (block_system_solve_u, src/blocks.c:771-800). Units: trsm_pref, one per upper block.
 template <typename T, typename V>
 __global__ void __launch_bounds__(kThreads)
-    k_bwd_partial(DevSym S, const T *__restrict__ slab, const V *__restrict__ y, V *__restrict__ scratch, int64_t p0,
-                  int64_t p1, int nrhs)
+    k_bwd_stage(DevSym S, const T *__restrict__ slab, V *__restrict__ y, V *__restrict__ scratch,
+                int *__restrict__ tickets, int64_t p0, int64_t p1, int nrhs)
 {
     const int64_t u = S.trsm_pref[p0] + blockIdx.x;
     const int64_t p = find_owner(S.trsm_pref, p0, p1, u);
     const int64_t k = S.piv[p];
+    const int m = S.size[k];
+    const int64_t nparts = S.row_ptr[k + 1] - S.diag_pos[k] - 1;
     const int64_t j = u - S.trsm_pref[p];
     const int64_t blk = S.diag_pos[k] + 1 + j;
     const int32_t c = S.cols[blk];
-    const int m = S.size[k];
-    const int64_t row = S.bwd_rows[p] - S.bwd_rows[p0] + j * m;
-    block_gemv(slab + S.blk_off[blk], m, S.size[c], y + S.dof_off[c] * nrhs, scratch + row * nrhs, nrhs);
-}
-
-// Backward finish: y_k -= sum of the partials of its upper blocks
-// (block_system_solve_u, src/blocks.c:771-800).
-template <typename V>
-__global__ void __launch_bounds__(kThreads)
-    k_bwd_final(DevSym S, V *__restrict__ y, const V *__restrict__ scratch, int64_t p0, int nrhs)
-{
-    const int64_t p = p0 + blockIdx.x;
-    const int64_t k = S.piv[p];
-    const int m = S.size[k];
-    const int64_t nparts = S.row_ptr[k + 1] - S.diag_pos[k] - 1;
+    V *part = scratch + (S.bwd_rows[p] - S.bwd_rows[p0]) * nrhs;
+    block_gemv(slab + S.blk_off[blk], m, S.size[c], y + S.dof_off[c] * nrhs, part + j * m * nrhs, nrhs);
+    if (!last_ticket(tickets, p, nparts))
+        return;
     V *yk = y + S.dof_off[k] * nrhs;
-    const V *part = scratch + (S.bwd_rows[p] - S.bwd_rows[p0]) * nrhs;
     for (int i = threadIdx.x; i < m * nrhs; i += blockDim.x)
     {
         V v = yk[i];
-        for (int64_t j = 0; j < nparts; ++j)
-            v -= part[j * m * nrhs + i];
+        for (int64_t q = 0; q < nparts; ++q)
+            v -= __ldcg(part + q * m * nrhs + i);
         yk[i] = v;
     }
 }

@@ -229,7 +229,10 @@ int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, co
     S.lu_pref.assign(n + 1, 0);
     S.upd_pref.assign(n + 1, 0);
     S.upd2_pref.assign(n + 1, 0);
+    S.split_pref.assign(n + 1, 0);
+    S.tc_pref.assign(n + 1, 0);
     S.fwd_pref.assign(n + 1, 0);
+    S.fwdu_pref.assign(n + 1, 0);
     S.fwd_rows.assign(n + 1, 0);
     S.bwd_rows.assign(n + 1, 0);
     double flops = 0;
@@ -245,7 +248,10 @@ int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, co
         S.lu_pref[p + 1] = S.lu_pref[p] + std::max<int64_t>(1, n_up);
         S.upd_pref[p + 1] = S.upd_pref[p] + n_lc * n_up;
         S.upd2_pref[p + 1] = S.upd2_pref[p] + (n_lc + 1) / 2 * n_up;
+        S.split_pref[p + 1] = S.split_pref[p] + n_lc + n_up;
+        S.tc_pref[p + 1] = S.tc_pref[p] + n_lc * ((n_up + 1) / 2);
         S.fwd_pref[p + 1] = S.fwd_pref[p] + n_lr;
+        S.fwdu_pref[p + 1] = S.fwdu_pref[p] + std::max<int64_t>(1, n_lr);
         S.fwd_rows[p + 1] = S.fwd_rows[p] + n_lr * S.size[k];
         S.bwd_rows[p + 1] = S.bwd_rows[p] + n_up * S.size[k];
         double up_cols = 0, lc_rows = 0;
@@ -308,6 +314,9 @@ int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, co
         sh.max_col = sh.max_up;
         sh.uniform64 = uniform;
         sh.piv64 = piv64;
+        if (uniform)
+            S.max_split_blocks =
+                std::max(S.max_split_blocks, S.split_pref[S.lvl_ptr[l + 1]] - S.split_pref[S.lvl_ptr[l]]);
         S.max_fwd_scratch_rows =
             std::max(S.max_fwd_scratch_rows, S.fwd_rows[S.lvl_ptr[l + 1]] - S.fwd_rows[S.lvl_ptr[l]]);
         S.max_bwd_scratch_rows =
@@ -381,6 +390,8 @@ int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, co
         sh.la_rest_units = (n_lc - (i0 >= 0)) * (n_up - (j0 >= 0));
         sh.la_rest_pairs = (n_lc - (i0 >= 0) + 1) / 2 * (n_up - (j0 >= 0));
         sh.la_prio_pairs = (i0 >= 0 ? n_up : 0) + (j0 >= 0 ? (n_lc - (i0 >= 0) + 1) / 2 : 0);
+        sh.la_prio_tiles = (i0 >= 0 ? (n_up + 1) / 2 : 0) + (j0 >= 0 ? n_lc - (i0 >= 0) : 0);
+        sh.la_rest_tiles = (n_lc - (i0 >= 0)) * ((n_up - (j0 >= 0) + 1) / 2);
     }
     return HYB_SUCCESS;
 }

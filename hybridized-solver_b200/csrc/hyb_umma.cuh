@@ -14,12 +14,10 @@
 namespace hyb
 {
 
-constexpr int kUmmaThreads = 128;
-// A (128 x 64) and B (64 x 64) as hi/lo BF16 tiles, each in the K-major 128-byte-swizzled
-// layout the MMA reads: 16 + 16 + 8 + 8 KB, then the mbarrier and the tensor-memory address.
-constexpr int kUmmaTileA = 128 * 64 * 2;
-constexpr int kUmmaTileB = 64 * 64 * 2;
-constexpr int kUmmaSmem = 2 * kUmmaTileA + 2 * kUmmaTileB + 64 + 1024; // + alignment slack
+// One 64x64 FP32 block as its BF16 split: hi (8 KB) then lo (8 KB), each a K-major tile of
+// 64 rows x 64 K in the 128-byte-swizzled layout the MMA reads.
+constexpr int kSplitBytes = 16384;
+constexpr int kSplitHalf = 8192;
 
 // Byte offset of element (row, k) of a K-major tile with 64 BF16 per row (one 128-byte
 // swizzle row): rows come in groups of 8 (1024 bytes), the 16-byte chunks of a row are
@@ -63,202 +61,403 @@ __device__ __forceinline__ void tmem_load32(uint32_t addr, uint32_t (&v)[32])
                  : "r"(addr));
 }
 
-// Splits 4 consecutive FP32 values into hi and lo BF16 and stores them at byte offset `off`
-// of the hi and lo tiles (the 4 values share one 16-byte chunk).
-__device__ __forceinline__ void split_store4(unsigned char *hi, unsigned char *lo, uint32_t off, float4 x)
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
 {
-    const float v[4] = {x.x, x.y, x.z, x.w};
-    __nv_bfloat16 h[4], l[4];
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Packs the BF16 split of 8 FP32 values into one 16-byte chunk of hi and one of lo.
+__device__ __forceinline__ void split8(const float (&x)[8], uint4 &hi, uint4 &lo)
+{
+    uint32_t h[4], l[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
     {
-        h[i] = __float2bfloat16_rn(v[i]);
-        l[i] = __float2bfloat16_rn(v[i] - __bfloat162float(h[i]));
+        const __nv_bfloat16 h0 = __float2bfloat16_rn(x[2 * i]), h1 = __float2bfloat16_rn(x[2 * i + 1]);
+        const __nv_bfloat16 l0 = __float2bfloat16_rn(x[2 * i] - __bfloat162float(h0));
+        const __nv_bfloat16 l1 = __float2bfloat16_rn(x[2 * i + 1] - __bfloat162float(h1));
+        h[i] = ((uint32_t)__bfloat16_as_ushort(h1) << 16) | __bfloat16_as_ushort(h0);
+        l[i] = ((uint32_t)__bfloat16_as_ushort(l1) << 16) | __bfloat16_as_ushort(l0);
     }
-    *reinterpret_cast<uint2 *>(hi + off) =
-        make_uint2(((uint32_t)__bfloat16_as_ushort(h[1]) << 16) | __bfloat16_as_ushort(h[0]),
-                   ((uint32_t)__bfloat16_as_ushort(h[3]) << 16) | __bfloat16_as_ushort(h[2]));
-    *reinterpret_cast<uint2 *>(lo + off) =
-        make_uint2(((uint32_t)__bfloat16_as_ushort(l[1]) << 16) | __bfloat16_as_ushort(l[0]),
-                   ((uint32_t)__bfloat16_as_ushort(l[3]) << 16) | __bfloat16_as_ushort(l[2]));
+    hi = make_uint4(h[0], h[1], h[2], h[3]);
+    lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
-// Uniform-64 FP32 update on the tensor cores. One CTA owns two target blocks of the same
-// column block c and consecutive rows t_a, t_b of the pivot's lower column (M = 128 rows,
-// N = 64): C(t,c) -= A(t,k) * U(k,c). Units: mode 0 enumerates row pairs of every pivot
-// of the level through upd2_pref; with one pivot and lookahead, mode 1 takes row i0
-// (one row per unit, every column) and then column j0 (row pairs of the other rows), and
-// mode 2 the row pairs and columns other than (i0, j0). Each target row's arithmetic is
-// the same whichever rows share its tile, so all modes give identical results.
-__global__ void __launch_bounds__(kUmmaThreads)
-    k_update64_umma(DevSym S, float *__restrict__ slab, int64_t p0, int64_t p1, int mode, int i0, int j0,
-                    int *status)
+// ----------------------------------------------------------------------------------
+// Operand staging of a tensor-core level: every lower-column block L(t,k) and upper-row
+// block U(k,c) of the level's pivots, split once into BF16 hi/lo in the layout the MMA
+// reads, so the update kernel only copies them into shared memory. Layout in `ops`: the
+// level's pivots in order, each with its n_lc lower blocks then its n_up upper blocks,
+// kSplitBytes apiece. L(t,k) is stored as it is (rows m, K = k contiguous); U(k,c) is
+// stored transposed (rows = its columns n, K = k contiguous).
+constexpr int kSplitThreads = 128;
+
+__global__ void __launch_bounds__(kSplitThreads)
+    k_split64(DevSym S, const float *__restrict__ slab, unsigned char *__restrict__ ops, int64_t p0, int64_t p1)
+{
+    __shared__ float tr[64 * 65];
+    const int64_t u = S.split_pref[p0] + blockIdx.x;
+    const int64_t p = find_owner(S.split_pref, p0, p1, u);
+    const int64_t k = S.piv[p];
+    const int64_t local = u - S.split_pref[p];
+    const int64_t n_lc = S.lcol_ptr[k + 1] - S.lcol_ptr[k];
+    unsigned char *dst = ops + (u - S.split_pref[p0]) * (int64_t)kSplitBytes;
+    const int tid = threadIdx.x;
+    if (local < n_lc)
+    {
+        const float *src = slab + S.blk_off[S.lcol_blk[S.lcol_ptr[k] + local]];
+        for (int ch = tid; ch < 512; ch += kSplitThreads)
+        {
+            const int row = ch >> 3, q = ch & 7;
+            const float4 a = *reinterpret_cast<const float4 *>(src + row * 64 + q * 8);
+            const float4 b = *reinterpret_cast<const float4 *>(src + row * 64 + q * 8 + 4);
+            const float x[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+            uint4 hi, lo;
+            split8(x, hi, lo);
+            const uint32_t off = sw128_offset(row, q * 8);
+            *reinterpret_cast<uint4 *>(dst + off) = hi;
+            *reinterpret_cast<uint4 *>(dst + kSplitHalf + off) = lo;
+        }
+        return;
+    }
+    const float *src = slab + S.blk_off[S.diag_pos[k] + 1 + (local - n_lc)];
+    for (int i = tid; i < 64 * 16; i += kSplitThreads)
+    {
+        const float4 v = *reinterpret_cast<const float4 *>(src + i * 4);
+        const int r = i >> 4, c = (i & 15) * 4;
+        tr[r * 65 + c] = v.x;
+        tr[r * 65 + c + 1] = v.y;
+        tr[r * 65 + c + 2] = v.z;
+        tr[r * 65 + c + 3] = v.w;
+    }
+    __syncthreads();
+    for (int ch = tid; ch < 512; ch += kSplitThreads)
+    {
+        const int n = ch >> 3, q = ch & 7;
+        float x[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            x[i] = tr[(q * 8 + i) * 65 + n];
+        uint4 hi, lo;
+        split8(x, hi, lo);
+        const uint32_t off = sw128_offset(n, q * 8);
+        *reinterpret_cast<uint4 *>(dst + off) = hi;
+        *reinterpret_cast<uint4 *>(dst + kSplitHalf + off) = lo;
+    }
+}
+
+// ----------------------------------------------------------------------------------
+// Uniform-64 FP32 Schur update on the tensor cores, C(t,c) -= L(t,k) U(k,c), computed
+// transposed: one tile is D = U(k, [c0 c1])^T L(t,k)^T (M = 128: the 2 x 64 columns of two
+// upper blocks, N = 64: the rows of one target row t, K = 64), so tensor-memory lane i holds
+// column i of the tile and a warp's 32 lanes read and write 32 consecutive floats of a row
+// of C. Each product takes three BF16 MMAs (hi*hi + hi*lo + lo*hi) accumulated in FP32.
+//
+// A persistent CTA walks a contiguous range of tiles ordered column pair major, so the
+// U pair stays in shared memory across its rows. Warp 4 (one lane) copies operands from
+// the staged splits with bulk copies into a 4-stage ring; warp 5 (one lane) issues the
+// MMAs into one of two tensor-memory accumulators; warps 0-3 drain an accumulator, read C,
+// subtract and write C while the next tile's MMAs run. Every wait has an iteration limit;
+// on expiry the CTA sets ST_TIMEOUT, drains its copies and MMAs and returns.
+//
+// Tiles: mode 0 enumerates every pivot of the level through tc_pref (n_lc x column pairs);
+// with one pivot and lookahead, mode 1 takes row i0 (column pairs) and then column j0 alone
+// for every other row, and mode 2 the other rows x column pairs of the other columns.
+// An element's value does not depend on which columns share its tile, so all modes give
+// identical results.
+constexpr int kTcThreads = 192;
+constexpr int kTcStages = 4;
+constexpr int kTcSmem = 2 * kSplitBytes + kTcStages * kSplitBytes + 256 + 1024; // + alignment slack
+
+struct TcTile
+{
+    int64_t p;   // pivot slot
+    int64_t row; // index in the pivot's lower column
+    int32_t ja;  // index in the pivot's upper row of the tile's first column block
+    int32_t jb;  // second column block, -1 if the tile has one
+};
+
+__device__ __forceinline__ TcTile tc_tile(const DevSym &S, int64_t p0, int64_t p1, int mode, int i0, int j0,
+                                          int64_t t)
+{
+    TcTile x;
+    int64_t p = p0, local = t;
+    if (mode == 0)
+    {
+        const int64_t u = S.tc_pref[p0] + t;
+        p = find_owner(S.tc_pref, p0, p1, u);
+        local = u - S.tc_pref[p];
+    }
+    const int64_t k = S.piv[p];
+    const int64_t n_lc = S.lcol_ptr[k + 1] - S.lcol_ptr[k];
+    const int32_t n_up = (int32_t)(S.row_ptr[k + 1] - S.diag_pos[k] - 1);
+    x.p = p;
+    if (mode == 0)
+    {
+        const int64_t cp = local / n_lc;
+        x.row = local - cp * n_lc;
+        x.ja = (int32_t)(2 * cp);
+        x.jb = x.ja + 1 < n_up ? x.ja + 1 : -1;
+    }
+    else if (mode == 1)
+    {
+        const int64_t ncp = i0 >= 0 ? (n_up + 1) / 2 : 0;
+        if (local < ncp)
+        {
+            x.row = i0;
+            x.ja = (int32_t)(2 * local);
+            x.jb = x.ja + 1 < n_up ? x.ja + 1 : -1;
+        }
+        else
+        {
+            const int64_t r = local - ncp;
+            x.row = r + (i0 >= 0 && r >= i0);
+            x.ja = j0;
+            x.jb = -1;
+        }
+    }
+    else
+    {
+        const int64_t nr = n_lc - (i0 >= 0);
+        const int32_t nc = n_up - (j0 >= 0);
+        const int64_t cp = local / nr;
+        const int64_t r = local - cp * nr;
+        x.row = r + (i0 >= 0 && r >= i0);
+        const int32_t a = (int32_t)(2 * cp), b = a + 1;
+        x.ja = a + (j0 >= 0 && a >= j0);
+        x.jb = b < nc ? b + (j0 >= 0 && b >= j0) : -1;
+    }
+    return x;
+}
+
+__global__ void __launch_bounds__(kTcThreads, 2)
+    k_update64_tc(DevSym S, float *__restrict__ slab, const unsigned char *__restrict__ ops, int64_t p0, int64_t p1,
+                  int mode, int i0, int j0, int64_t n_tiles, int *status)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
-    unsigned char *a_hi = base;
-    unsigned char *a_lo = a_hi + kUmmaTileA;
-    unsigned char *b_hi = a_lo + kUmmaTileA;
-    unsigned char *b_lo = b_hi + kUmmaTileB;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(b_lo + kUmmaTileB);
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar + 1);
-
-    // ---- work unit: pivot k, lower-column rows (ia, ib), upper column j
-    int64_t p = p0, local = blockIdx.x;
-    if (mode == 0)
-    {
-        const int64_t u = S.upd2_pref[p0] + blockIdx.x;
-        p = find_owner(S.upd2_pref, p0, p1, u);
-        local = u - S.upd2_pref[p];
-    }
-    const int64_t k = S.piv[p];
-    const int64_t n_lc = S.lcol_ptr[k + 1] - S.lcol_ptr[k];
-    const int64_t n_up = S.row_ptr[k + 1] - S.diag_pos[k] - 1;
-    int64_t ia, ib, jj;
-    bool has_b;
-    if (mode == 1 && i0 >= 0 && local < n_up)
-    {
-        ia = i0; // the next pivot's row, alone
-        ib = i0;
-        jj = local;
-        has_b = false;
-    }
-    else if (mode == 1)
-    {
-        // the next pivot's column: row pairs of every row except i0
-        const int64_t pr = local - (i0 >= 0 ? n_up : 0);
-        const int64_t rows = n_lc - (i0 >= 0 ? 1 : 0);
-        ia = 2 * pr;
-        ib = 2 * pr + 1;
-        has_b = ib < rows;
-        if (i0 >= 0)
-        {
-            ia += ia >= i0;
-            ib += ib >= i0;
-        }
-        jj = j0;
-    }
-    else
-    {
-        const int64_t rows = n_lc - (mode == 2 && i0 >= 0 ? 1 : 0);
-        const int64_t cols = n_up - (mode == 2 && j0 >= 0 ? 1 : 0);
-        const int64_t pr = local / cols;
-        jj = local % cols;
-        ia = 2 * pr;
-        ib = 2 * pr + 1;
-        has_b = ib < rows;
-        if (mode == 2)
-        {
-            if (i0 >= 0)
-            {
-                ia += ia >= i0;
-                ib += ib >= i0;
-            }
-            if (j0 >= 0)
-                jj += jj >= j0;
-        }
-    }
-    const int64_t la = S.lcol_ptr[k] + ia, lb = S.lcol_ptr[k] + ib;
-    const int64_t bu = S.diag_pos[k] + 1 + jj;
-    const int32_t c = S.cols[bu];
-    const float *ga = slab + S.blk_off[S.lcol_blk[la]];
-    const float *gb2 = has_b ? slab + S.blk_off[S.lcol_blk[lb]] : nullptr;
-    const float *gu = slab + S.blk_off[bu];
+    unsigned char *u_hi = base;                 // M = 128 rows: column block ja, then jb
+    unsigned char *u_lo = u_hi + kSplitBytes;   //
+    unsigned char *ring = u_lo + kSplitBytes;   // kTcStages x (hi 8 KB, lo 8 KB) of L(t,k)
+    uint64_t *bars = reinterpret_cast<uint64_t *>(ring + kTcStages * kSplitBytes);
+    uint64_t *full = bars;                      // [kTcStages] operand landed
+    uint64_t *empty = bars + kTcStages;         // [kTcStages] operand consumed by the MMAs
+    uint64_t *ufull = bars + 2 * kTcStages;     // U pair landed
+    uint64_t *uempty = ufull + 1;               // MMAs on the previous U pair done
+    uint64_t *tfull = ufull + 2;                // [2] accumulator ready
+    uint64_t *tempty = ufull + 4;               // [2] accumulator drained (4 warp arrivals)
+    uint64_t *done = ufull + 6;                 // all MMAs of the CTA done
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(ufull + 7);
+    __shared__ int s_fail;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t t0 = n_tiles * blockIdx.x / gridDim.x, t1 = n_tiles * (blockIdx.x + 1) / gridDim.x;
+    if (tid == 0)
+    {
+        for (int i = 0; i < kTcStages; ++i)
+        {
+            mbar_init(full + i, 1);
+            mbar_init(empty + i, 1);
+        }
+        mbar_init(ufull, 1);
+        mbar_init(uempty, 1);
+        mbar_init(tfull, 1);
+        mbar_init(tfull + 1, 1);
+        mbar_init(tempty, 4);
+        mbar_init(tempty + 1, 4);
+        mbar_init(done, 1);
+        s_fail = schedule_aborted(status);
+    }
     if (warp == 0)
     {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(64));
+                     "r"(128));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
-    if (tid == 0)
-        mbar_init(bar, 1);
-
-    // ---- operands: FP32 -> (hi, lo) BF16 in the swizzled K-major layouts
-    for (int i = tid; i < 128 * 16; i += kUmmaThreads)
-    {
-        const int r = i >> 4, q = (i & 15) * 4;
-        float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (r < 64)
-            x = *reinterpret_cast<const float4 *>(ga + r * 64 + q);
-        else if (has_b)
-            x = *reinterpret_cast<const float4 *>(gb2 + (r - 64) * 64 + q);
-        split_store4(a_hi, a_lo, sw128_offset(r, q), x);
-    }
-    for (int i = tid; i < 64 * 64; i += kUmmaThreads)
-    {
-        // U is row-major [k][n]; the MMA wants it K-major (rows = n, K contiguous)
-        const int kk = i >> 6, nn = i & 63;
-        const float x = gu[i];
-        const __nv_bfloat16 h = __float2bfloat16_rn(x);
-        const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
-        *reinterpret_cast<__nv_bfloat16 *>(b_hi + sw128_offset(nn, kk)) = h;
-        *reinterpret_cast<__nv_bfloat16 *>(b_lo + sw128_offset(nn, kk)) = l;
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
+    const int64_t lvl_base = S.split_pref[p0];
+    const bool run = s_fail == 0; // read by every thread before any role can change it
+    __syncthreads();
 
-    // ---- 4 K-steps of 16, three split products each, one issuing thread
-    if (tid == 0)
+    if (!run)
     {
-        constexpr uint32_t idesc = umma_idesc_bf16(128, 64);
-        const uint64_t dah = umma_smem_desc(smem_u32(a_hi)), dal = umma_smem_desc(smem_u32(a_lo));
-        const uint64_t dbh = umma_smem_desc(smem_u32(b_hi)), dbl = umma_smem_desc(smem_u32(b_lo));
-#pragma unroll
-        for (int s = 0; s < 4; ++s)
-        {
-            const uint64_t off = (uint64_t)((s * 32) >> 4); // 16 BF16 = 32 bytes along K
-            umma_bf16(tmem, dah + off, dbh + off, idesc, s > 0);
-            umma_bf16(tmem, dah + off, dbl + off, idesc, 1);
-            umma_bf16(tmem, dal + off, dbh + off, idesc, 1);
-        }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                         smem_u32(bar))
-                     : "memory");
     }
-    const bool ok = mbar_wait(bar, 0);
-    if (!ok && lane == 0)
-        atomicOr(status + ST_TIMEOUT, 1);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-
-    // ---- epilogue: row r of the product is tensor-memory lane r; C -= P in FP32
-    const int r = warp * 32 + lane;
-    float *gc = nullptr;
-    if (ok && (r < 64 || has_b))
+    else if (warp == 4)
     {
-        const int32_t t = S.lcol_row[r < 64 ? la : lb];
-        const int64_t tgt = find_col(S.cols, S.row_ptr[t], S.row_ptr[t + 1], c);
-        gc = slab + S.blk_off[tgt] + (r & 63) * 64;
-    }
-#pragma unroll
-    for (int h = 0; h < 2; ++h)
-    {
-        uint32_t v[32];
-        tmem_load32(tmem + ((uint32_t)(warp * 32) << 16) + h * 32, v);
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (gc != nullptr)
+        // ---- producer: U pair on change, one L(t,k) split per tile
+        if (lane == 0)
         {
-#pragma unroll
-            for (int q = 0; q < 8; ++q)
+            int64_t cur_p = -1;
+            int32_t cur_a = -2, cur_b = -2;
+            uint32_t uloads = 0;
+            int64_t i = 0;
+            for (int64_t t = t0; t < t1; ++t, ++i)
             {
-                float4 cv = *reinterpret_cast<float4 *>(gc + h * 32 + q * 4);
-                cv.x -= __uint_as_float(v[q * 4 + 0]);
-                cv.y -= __uint_as_float(v[q * 4 + 1]);
-                cv.z -= __uint_as_float(v[q * 4 + 2]);
-                cv.w -= __uint_as_float(v[q * 4 + 3]);
-                *reinterpret_cast<float4 *>(gc + h * 32 + q * 4) = cv;
+                const TcTile x = tc_tile(S, p0, p1, mode, i0, j0, t);
+                const int64_t k = S.piv[x.p];
+                const int64_t n_lc = S.lcol_ptr[k + 1] - S.lcol_ptr[k];
+                const unsigned char *pb = ops + (S.split_pref[x.p] - lvl_base) * (int64_t)kSplitBytes;
+                if (x.p != cur_p || x.ja != cur_a || x.jb != cur_b)
+                {
+                    if (uloads > 0 && !mbar_wait(uempty, (uloads - 1) & 1))
+                    {
+                        s_fail = 1;
+                        break;
+                    }
+                    mbar_expect_tx(ufull, x.jb >= 0 ? 2 * kSplitBytes : kSplitBytes);
+                    const unsigned char *sa = pb + (n_lc + x.ja) * (int64_t)kSplitBytes;
+                    bulk_g2s(u_hi, sa, kSplitHalf, ufull);
+                    bulk_g2s(u_lo, sa + kSplitHalf, kSplitHalf, ufull);
+                    if (x.jb >= 0)
+                    {
+                        const unsigned char *sb = pb + (n_lc + x.jb) * (int64_t)kSplitBytes;
+                        bulk_g2s(u_hi + kSplitHalf, sb, kSplitHalf, ufull);
+                        bulk_g2s(u_lo + kSplitHalf, sb + kSplitHalf, kSplitHalf, ufull);
+                    }
+                    ++uloads;
+                    cur_p = x.p;
+                    cur_a = x.ja;
+                    cur_b = x.jb;
+                }
+                const int s = (int)(i % kTcStages);
+                if (i >= kTcStages && !mbar_wait(empty + s, (uint32_t)((i / kTcStages - 1) & 1)))
+                {
+                    s_fail = 1;
+                    break;
+                }
+                mbar_expect_tx(full + s, kSplitBytes);
+                bulk_g2s(ring + s * kSplitBytes, pb + x.row * (int64_t)kSplitBytes, kSplitBytes, full + s);
+            }
+            // drain: every copy issued lands before the CTA can leave
+            const int64_t issued = i;
+            for (int64_t j = issued > kTcStages ? issued - kTcStages : 0; j < issued; ++j)
+                if (!mbar_wait(full + (j % kTcStages), (uint32_t)((j / kTcStages) & 1)))
+                    s_fail = 1;
+            if (uloads > 0 && !mbar_wait(ufull, (uloads - 1) & 1))
+                s_fail = 1;
+        }
+    }
+    else if (warp == 5)
+    {
+        // ---- MMA issuer
+        if (lane == 0)
+        {
+            constexpr uint32_t idesc = umma_idesc_bf16(128, 64);
+            const uint64_t duh = umma_smem_desc(smem_u32(u_hi)), dul = umma_smem_desc(smem_u32(u_lo));
+            int64_t cur_p = -1;
+            int32_t cur_a = -2, cur_b = -2;
+            uint32_t uloads = 0;
+            int64_t i = 0;
+            for (int64_t t = t0; t < t1; ++t, ++i)
+            {
+                const TcTile x = tc_tile(S, p0, p1, mode, i0, j0, t);
+                if (x.p != cur_p || x.ja != cur_a || x.jb != cur_b)
+                {
+                    if (uloads > 0)
+                        umma_commit(uempty);
+                    if (!mbar_wait(ufull, uloads & 1))
+                    {
+                        s_fail = 1;
+                        break;
+                    }
+                    ++uloads;
+                    cur_p = x.p;
+                    cur_a = x.ja;
+                    cur_b = x.jb;
+                }
+                const int s = (int)(i % kTcStages);
+                const int a = (int)(i & 1);
+                if (!mbar_wait(full + s, (uint32_t)((i / kTcStages) & 1)) ||
+                    (i >= 2 && !mbar_wait(tempty + a, (uint32_t)(((i >> 1) - 1) & 1))))
+                {
+                    s_fail = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t lh = smem_u32(ring + s * kSplitBytes);
+                const uint64_t dlh = umma_smem_desc(lh), dll = umma_smem_desc(lh + kSplitHalf);
+                const uint32_t acc = tmem + (uint32_t)(a * 64);
+#pragma unroll
+                for (int ks = 0; ks < 4; ++ks)
+                {
+                    const uint64_t off = (uint64_t)((ks * 32) >> 4); // 16 BF16 = 32 bytes along K
+                    umma_bf16(acc, duh + off, dlh + off, idesc, ks > 0);
+                    umma_bf16(acc, duh + off, dll + off, idesc, 1);
+                    umma_bf16(acc, dul + off, dlh + off, idesc, 1);
+                }
+                umma_commit(empty + s);
+                umma_commit(tfull + a);
+            }
+            umma_commit(done);
+            if (!mbar_wait(done, 0))
+                s_fail = 1;
+        }
+    }
+    else
+    {
+        // ---- epilogue warps 0-3: lane i of warp w is column (w & 1) * 32 + i of block
+        // (w < 2 ? ja : jb); registers hold the tile's 64 rows
+        int64_t i = 0;
+        for (int64_t t = t0; t < t1; ++t, ++i)
+        {
+            const TcTile x = tc_tile(S, p0, p1, mode, i0, j0, t);
+            const int64_t k = S.piv[x.p];
+            const int32_t j = warp < 2 ? x.ja : x.jb;
+            float *gc = nullptr;
+            float cv[64];
+            if (j >= 0)
+            {
+                const int32_t c = S.cols[S.diag_pos[k] + 1 + j];
+                const int32_t tr = S.lcol_row[S.lcol_ptr[k] + x.row];
+                const int64_t tgt = find_col(S.cols, S.row_ptr[tr], S.row_ptr[tr + 1], c);
+                gc = slab + S.blk_off[tgt] + (warp & 1) * 32 + lane;
+#pragma unroll
+                for (int r = 0; r < 64; ++r)
+                    cv[r] = gc[r * 64];
+            }
+            const int a = (int)(i & 1);
+            if (!mbar_wait(tfull + a, (uint32_t)((i >> 1) & 1)))
+            {
+                s_fail = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            uint32_t v0[32], v1[32];
+            const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(a * 64);
+            tmem_load32(ta, v0);
+            tmem_load32(ta + 32, v1);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+                mbar_arrive(tempty + a);
+            if (gc != nullptr)
+            {
+#pragma unroll
+                for (int r = 0; r < 32; ++r)
+                    gc[r * 64] = cv[r] - __uint_as_float(v0[r]);
+#pragma unroll
+                for (int r = 0; r < 32; ++r)
+                    gc[(r + 32) * 64] = cv[r + 32] - __uint_as_float(v1[r]);
             }
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
+    if (tid == 0 && s_fail)
+        atomicOr(status + ST_TIMEOUT, 1);
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128));
 }
 
 } // namespace hyb
