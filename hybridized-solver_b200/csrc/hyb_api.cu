@@ -57,10 +57,10 @@ int smem_optin()
     return g_smem_optin;
 }
 
-// Dynamic shared memory the forward solve stage may take (its static ticket flag aside).
+// Dynamic shared memory the forward solve stage may take (its static arrays aside).
 int solve_smem_cap()
 {
-    return smem_optin() - 1024;
+    return smem_optin() - 4096;
 }
 
 // Streaming multiprocessors of the current device.

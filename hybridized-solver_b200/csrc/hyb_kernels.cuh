@@ -858,6 +858,139 @@ __device__ __forceinline__ bool last_ticket(int *tickets, int64_t p, int64_t npa
     return true;
 }
 
+// Substitution with a factored diagonal block D (unit L below, U on and above the
+// diagonal; row stride ldd) for column r of acc (m x nrhs, shared memory), by one warp:
+// x <- U^{-1} L^{-1} x, as matrix_lu_solve (src/blocks.c:285-316) in right-looking order.
+// The vector stays in registers -- lane l holds rows l + 32 t, t < R -- and step i
+// broadcasts x_i with a shuffle, so a step costs one shuffle and R fused multiply-adds.
+template <int R, typename T, typename V>
+__device__ __forceinline__ void warp_lu_solve(const T *d, int ldd, int m, V *acc, int r, int nrhs)
+{
+    const int lane = threadIdx.x & 31;
+    V x[R], rcp[R];
+#pragma unroll
+    for (int t = 0; t < R; ++t)
+    {
+        const int row = lane + 32 * t, rr = min(row, m - 1);
+        x[t] = row < m ? acc[rr * nrhs + r] : V(0);
+        rcp[t] = V(1) / (V)d[(int64_t)rr * ldd + rr];
+    }
+#pragma unroll
+    for (int tb = 0; tb < R; ++tb)
+    {
+        const int n_i = min(32, m - 32 * tb);
+#pragma unroll 2
+        for (int il = 0; il < n_i; ++il)
+        {
+            const int i = 32 * tb + il;
+            const V xi = __shfl_sync(0xffffffffu, x[tb], il);
+#pragma unroll
+            for (int t = 0; t < R; ++t)
+            {
+                const int row = lane + 32 * t, rr = min(row, m - 1);
+                const V c = (V)d[(int64_t)rr * ldd + i];
+                x[t] -= (row > i && row < m ? c : V(0)) * xi;
+            }
+        }
+    }
+#pragma unroll
+    for (int tb = R - 1; tb >= 0; --tb)
+    {
+        const int n_i = min(32, m - 32 * tb);
+#pragma unroll 2
+        for (int il = n_i - 1; il >= 0; --il)
+        {
+            const int i = 32 * tb + il;
+            const V xi = __shfl_sync(0xffffffffu, x[tb] * rcp[tb], il);
+            if (lane == il)
+                x[tb] = xi;
+#pragma unroll
+            for (int t = 0; t < R; ++t)
+            {
+                const int row = lane + 32 * t, rr = min(row, m - 1);
+                const V c = (V)d[(int64_t)rr * ldd + i];
+                x[t] -= (row < i ? c : V(0)) * xi;
+            }
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < R; ++t)
+    {
+        const int row = lane + 32 * t;
+        if (row < m)
+            acc[row * nrhs + r] = x[t];
+    }
+}
+
+// The same for blocks of more than 128 rows, through shared memory.
+template <typename T, typename V>
+__device__ void warp_lu_solve_smem(const T *d, int ldd, int m, V *acc, int r, int nrhs)
+{
+    const int lane = threadIdx.x & 31;
+    for (int i = 0; i < m; ++i)
+    {
+        const V xi = acc[i * nrhs + r];
+        __syncwarp();
+        for (int q = i + 1 + lane; q < m; q += 32)
+            acc[q * nrhs + r] -= (V)d[(int64_t)q * ldd + i] * xi;
+        __syncwarp();
+    }
+    for (int i = m - 1; i >= 0; --i)
+    {
+        V xi = acc[i * nrhs + r] / (V)d[(int64_t)i * ldd + i];
+        __syncwarp();
+        if (lane == 0)
+            acc[i * nrhs + r] = xi;
+        for (int q = lane; q < i; q += 32)
+            acc[q * nrhs + r] -= (V)d[(int64_t)q * ldd + i] * xi;
+        __syncwarp();
+    }
+}
+
+// out[e] = y[e] - sum_j part[j][e] for e < E (E = rows x right-hand sides), with every
+// thread of the CTA busy: G = blockDim / E groups each sum every G-th partial, then the G
+// group sums are subtracted in group order (a fixed order, so results are reproducible).
+// `red` is shared scratch of blockDim values; `out` may alias `y`.
+template <typename V>
+__device__ void subtract_partials(const V *y, const V *__restrict__ part, int64_t nparts, int E, V *out, V *red)
+{
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int G = E < nt ? nt / E : 1;
+    if (G > 1)
+    {
+        const int g = tid / E, e = tid - g * E;
+        if (g < G)
+        {
+            V s0 = 0, s1 = 0;
+            int64_t j = g;
+            for (; j + G < nparts; j += 2 * G)
+            {
+                s0 += __ldcg(part + j * E + e);
+                s1 += __ldcg(part + (j + G) * E + e);
+            }
+            if (j < nparts)
+                s0 += __ldcg(part + j * E + e);
+            red[g * E + e] = s0 + s1;
+        }
+        __syncthreads();
+        for (int e2 = tid; e2 < E; e2 += nt)
+        {
+            V v = y[e2];
+            for (int q = 0; q < G; ++q)
+                v -= red[q * E + e2];
+            out[e2] = v;
+        }
+        return;
+    }
+    for (int e2 = tid; e2 < E; e2 += nt)
+    {
+        V v = y[e2];
+        for (int64_t j = 0; j < nparts; ++j)
+            v -= __ldcg(part + j * E + e2);
+        out[e2] = v;
+    }
+}
+
 // Forward stage: y_k <- D_k^{-1} (y_k - sum_s L(k,s) y_s) for the stage's pivots
 // (block_system_apply_operations, src/blocks.c:729-769). Units: fwdu_pref, one per lower
 // block of a pivot (at least one per pivot).
@@ -882,15 +1015,10 @@ __global__ void __launch_bounds__(kThreads)
         if (!last_ticket(tickets, p, nparts))
             return;
     }
+    __shared__ V red[kThreads];
     V *acc = reinterpret_cast<V *>(smem_raw); // m * nrhs
     V *yk = y + S.dof_off[k] * nrhs;
-    for (int i = threadIdx.x; i < m * nrhs; i += blockDim.x)
-    {
-        V v = yk[i];
-        for (int64_t j = 0; j < nparts; ++j)
-            v -= __ldcg(part + j * m * nrhs + i);
-        acc[i] = v;
-    }
+    subtract_partials(yk, part, nparts, m * nrhs, acc, red);
     // The diagonal block goes to shared memory with an odd row stride (column reads of the
     // substitution hit distinct banks) when it fits next to the accumulator.
     const T *gd = slab + S.blk_off[S.diag_pos[k]];
@@ -907,27 +1035,19 @@ __global__ void __launch_bounds__(kThreads)
     }
     __syncthreads();
     // unit lower, then upper; one warp per right-hand side
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int r = warp; r < nrhs; r += nw)
     {
-        for (int i = 0; i < m; ++i)
-        {
-            const V xi = acc[i * nrhs + r];
-            __syncwarp();
-            for (int q = i + 1 + lane; q < m; q += 32)
-                acc[q * nrhs + r] -= (V)d[(int64_t)q * ldd + i] * xi;
-            __syncwarp();
-        }
-        for (int i = m - 1; i >= 0; --i)
-        {
-            V xi = acc[i * nrhs + r] / (V)d[(int64_t)i * ldd + i];
-            __syncwarp();
-            if (lane == 0)
-                acc[i * nrhs + r] = xi;
-            for (int q = lane; q < i; q += 32)
-                acc[q * nrhs + r] -= (V)d[(int64_t)q * ldd + i] * xi;
-            __syncwarp();
-        }
+        if (m <= 32)
+            warp_lu_solve<1>(d, ldd, m, acc, r, nrhs);
+        else if (m <= 64)
+            warp_lu_solve<2>(d, ldd, m, acc, r, nrhs);
+        else if (m <= 96)
+            warp_lu_solve<3>(d, ldd, m, acc, r, nrhs);
+        else if (m <= 128)
+            warp_lu_solve<4>(d, ldd, m, acc, r, nrhs);
+        else
+            warp_lu_solve_smem(d, ldd, m, acc, r, nrhs);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < m * nrhs; i += blockDim.x)
@@ -953,14 +1073,9 @@ __global__ void __launch_bounds__(kThreads)
     block_gemv(slab + S.blk_off[blk], m, S.size[c], y + S.dof_off[c] * nrhs, part + j * m * nrhs, nrhs);
     if (!last_ticket(tickets, p, nparts))
         return;
+    __shared__ V red[kThreads];
     V *yk = y + S.dof_off[k] * nrhs;
-    for (int i = threadIdx.x; i < m * nrhs; i += blockDim.x)
-    {
-        V v = yk[i];
-        for (int64_t q = 0; q < nparts; ++q)
-            v -= __ldcg(part + q * m * nrhs + i);
-        yk[i] = v;
-    }
+    subtract_partials(yk, part, nparts, m * nrhs, yk, red);
 }
 
 // ----------------------------------------------------------------------------------
