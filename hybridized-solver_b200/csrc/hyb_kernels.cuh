@@ -97,6 +97,32 @@ __device__ __forceinline__ int64_t find_col(const int32_t *cols, int64_t b, int6
     return b;
 }
 
+// The same search by a whole warp (all lanes call it with the same arguments): each round
+// reads 256 entries with independent loads and finds c by ballot, so a row of up to 256
+// blocks costs one memory round trip instead of a chain of dependent ones.
+__device__ __forceinline__ int64_t warp_find_col(const int32_t *cols, int64_t b, int64_t e, int32_t c)
+{
+    const int lane = threadIdx.x & 31;
+    for (int64_t base = b; base < e; base += 256)
+    {
+        int32_t v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+        {
+            const int64_t idx = base + q * 32 + lane;
+            v[q] = idx < e ? cols[idx] : -1;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+        {
+            const unsigned hit = __ballot_sync(0xffffffffu, v[q] == c);
+            if (hit)
+                return base + q * 32 + __ffs(hit) - 1;
+        }
+    }
+    return b; // not reached: the filled pattern holds every target
+}
+
 template <typename T> __device__ __forceinline__ bool finite_val(T v)
 {
     return isfinite(v);
@@ -711,7 +737,7 @@ __global__ void __launch_bounds__(kUpd64Threads)
     const int64_t li = w.li, bu = w.bu;
     const int32_t t = S.lcol_row[li];
     const int32_t c = S.cols[bu];
-    const int64_t tgt = find_col(S.cols, S.row_ptr[t], S.row_ptr[t + 1], c);
+    const int64_t tgt = warp_find_col(S.cols, S.row_ptr[t], S.row_ptr[t + 1], c);
     const double *ga = slab + S.blk_off[S.lcol_blk[li]];
     const double *gb = slab + S.blk_off[bu];
     double *gc = slab + S.blk_off[tgt];

@@ -236,6 +236,21 @@ __device__ __forceinline__ TcTile tc_tile(const DevSym &S, int64_t p0, int64_t p
     return x;
 }
 
+// Slab offset of the target block of tile t for the column block the calling warp writes
+// (warps 0-1: ja, 2-3: jb), or -1 if the tile has no such block. Called by whole warps.
+__device__ __forceinline__ int64_t tc_target(const DevSym &S, int64_t p0, int64_t p1, int mode, int i0, int j0,
+                                             int64_t t, int warp)
+{
+    const TcTile x = tc_tile(S, p0, p1, mode, i0, j0, t);
+    const int32_t j = warp < 2 ? x.ja : x.jb;
+    if (j < 0)
+        return -1;
+    const int64_t k = S.piv[x.p];
+    const int32_t c = S.cols[S.diag_pos[k] + 1 + j];
+    const int32_t tr = S.lcol_row[S.lcol_ptr[k] + x.row];
+    return S.blk_off[warp_find_col(S.cols, S.row_ptr[tr], S.row_ptr[tr + 1], c)];
+}
+
 __global__ void __launch_bounds__(kTcThreads, 2)
     k_update64_tc(DevSym S, float *__restrict__ slab, const unsigned char *__restrict__ ops, int64_t p0, int64_t p1,
                   int mode, int i0, int j0, int64_t n_tiles, int *status)
@@ -406,27 +421,26 @@ __global__ void __launch_bounds__(kTcThreads, 2)
     else
     {
         // ---- epilogue warps 0-3: lane i of warp w is column (w & 1) * 32 + i of block
-        // (w < 2 ? ja : jb); registers hold the tile's 64 rows
+        // (w < 2 ? ja : jb); registers hold the tile's 64 rows. The next tile's target is
+        // looked up while this tile's C loads are in flight.
         int64_t i = 0;
+        int64_t next_off = t0 < t1 ? tc_target(S, p0, p1, mode, i0, j0, t0, warp) : -1;
         for (int64_t t = t0; t < t1; ++t, ++i)
         {
-            const TcTile x = tc_tile(S, p0, p1, mode, i0, j0, t);
-            const int64_t k = S.piv[x.p];
-            const int32_t j = warp < 2 ? x.ja : x.jb;
             float *gc = nullptr;
             float cv[64];
-            if (j >= 0)
+            if (next_off >= 0)
             {
-                const int32_t c = S.cols[S.diag_pos[k] + 1 + j];
-                const int32_t tr = S.lcol_row[S.lcol_ptr[k] + x.row];
-                const int64_t tgt = find_col(S.cols, S.row_ptr[tr], S.row_ptr[tr + 1], c);
-                gc = slab + S.blk_off[tgt] + (warp & 1) * 32 + lane;
+                gc = slab + next_off + (warp & 1) * 32 + lane;
 #pragma unroll
                 for (int r = 0; r < 64; ++r)
                     cv[r] = gc[r * 64];
             }
+            if (t + 1 < t1)
+                next_off = tc_target(S, p0, p1, mode, i0, j0, t + 1, warp);
             const int a = (int)(i & 1);
-            if (!mbar_wait(tfull + a, (uint32_t)((i >> 1) & 1)))
+            // warp-uniform outcome: the lookups above and below use full-warp ballots
+            if (!__all_sync(0xffffffffu, mbar_wait(tfull + a, (uint32_t)((i >> 1) & 1))))
             {
                 s_fail = 1;
                 break;
