@@ -136,6 +136,9 @@ struct hyb_system
     // BF16 operand splits of tensor-core levels, two level-parity halves of split_half bytes
     unsigned char *d_ops = nullptr;
     size_t split_half = 0;
+    // target-block offsets of tensor-core levels, two level-parity halves of tgt_half entries
+    int64_t *d_tgt = nullptr;
+    size_t tgt_half = 0;
     // solve buffers, sized for buf_nrhs right-hand sides
     int64_t buf_nrhs = 0;
     double *d_b = nullptr, *d_x = nullptr, *d_r = nullptr, *d_scr64 = nullptr, *d_part = nullptr, *d_norm = nullptr;
@@ -164,6 +167,7 @@ struct hyb_system
         cudaFree(d_f64);
         cudaFree(d_f32);
         cudaFree(d_ops);
+        cudaFree(d_tgt);
         free_solve_buffers();
         for (cudaEvent_t e : {ev_prio, ev_piv, ev_join})
             if (e)
@@ -197,11 +201,17 @@ struct hyb_system
 namespace
 {
 
+// The lookahead stream gets the highest priority, so the block scheduler places the next
+// pivot's CTAs ahead of the remaining update CTAs as soon as an SM has room; captured
+// kernels keep their stream's priority as a node attribute (see run_graph).
 cudaError_t create_streams(hyb_system *h)
 {
-    cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    int lo = 0, hi = 0;
+    cudaError_t e = cudaDeviceGetStreamPriorityRange(&lo, &hi);
     if (e == cudaSuccess)
-        e = cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking);
+        e = cudaStreamCreateWithPriority(&h->stream, cudaStreamNonBlocking, lo);
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithPriority(&h->stream2, cudaStreamNonBlocking, hi);
     for (cudaEvent_t *ev : {&h->ev_prio, &h->ev_piv, &h->ev_join})
         if (e == cudaSuccess)
             e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
@@ -293,12 +303,18 @@ template <typename T> int trsm_smem_bytes(int m)
 // Whether level l's Schur update runs on the tensor cores (mixed form, 64-blocks).
 template <typename T> bool tc_level(const hyb_system *h, int64_t l)
 {
-    return std::is_same_v<T, float> && h->umma && h->d_ops && !h->S.lvl_listed[l] && h->S.shape[l].uniform64;
+    return std::is_same_v<T, float> && h->umma && h->d_ops && h->d_tgt && !h->S.lvl_listed[l] &&
+           h->S.shape[l].uniform64;
 }
 
 unsigned char *level_ops(hyb_system *h, int64_t l)
 {
     return h->d_ops + (size_t)(l & 1) * h->split_half;
+}
+
+int64_t *level_tgt(hyb_system *h, int64_t l)
+{
+    return h->d_tgt + (size_t)(l & 1) * h->tgt_half;
 }
 
 // BF16 split of a tensor-core level's operands, once its pivots are factored.
@@ -313,7 +329,8 @@ template <typename T> int enqueue_split(hyb_system *h, T *slab, int64_t l, cudaS
         const int64_t blocks = S.split_pref[p1] - S.split_pref[p0];
         if (blocks > 0)
         {
-            hyb::k_split64<<<(unsigned)blocks, hyb::kSplitThreads, 0, st>>>(h->ds, slab, level_ops(h, l), p0, p1);
+            hyb::k_split64<<<(unsigned)blocks, hyb::kSplitThreads, 0, st>>>(h->ds, slab, level_ops(h, l),
+                                                                           level_tgt(h, l), p0, p1);
             ++launches;
             HYB_LAUNCHED("k_split64", l);
         }
@@ -398,7 +415,7 @@ template <typename T> int enqueue_update(hyb_system *h, T *slab, int64_t l, cuda
     }
     else
     {
-        // mixed form: split-BF16 products on the tensor cores, persistent CTAs (two per SM)
+        // mixed form: split-BF16 products on the tensor cores, one persistent CTA per SM
         if (tc_level<T>(h, l))
         {
             const int64_t tiles = mode == 0   ? S.tc_pref[p1] - S.tc_pref[p0]
@@ -406,9 +423,10 @@ template <typename T> int enqueue_update(hyb_system *h, T *slab, int64_t l, cuda
                                               : sh.la_rest_tiles;
             if (tiles > 0)
             {
-                const unsigned grid = (unsigned)std::min<int64_t>(tiles, 2 * (int64_t)sm_count());
+                const unsigned grid = (unsigned)std::min<int64_t>(tiles, (int64_t)sm_count());
                 hyb::k_update64_tc<<<grid, hyb::kTcThreads, hyb::kTcSmem, st>>>(
-                    ds, slab, level_ops(h, l), p0, p1, mode, sh.la_i0, sh.la_j0, tiles, h->d_status);
+                    ds, slab, level_ops(h, l), level_tgt(h, l), p0, p1, mode, sh.la_i0, sh.la_j0, tiles,
+                    h->d_status);
                 ++launches;
                 HYB_LAUNCHED("k_update64_tc", l);
             }
@@ -542,7 +560,7 @@ template <typename F> int run_graph(hyb_system *h, std::unique_ptr<GraphExec> &s
         }
         if (e != cudaSuccess)
             return cuda_fail(e, "cudaStreamEndCapture");
-        const cudaError_t ie = cudaGraphInstantiate(&g->exec, graph, 0);
+        const cudaError_t ie = cudaGraphInstantiate(&g->exec, graph, cudaGraphInstantiateFlagUseNodePriority);
         cudaGraphDestroy(graph);
         if (ie != cudaSuccess)
             return cuda_fail(ie, "cudaGraphInstantiate");
@@ -945,7 +963,9 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
         if (h->umma && !h->d_ops && S.max_split_blocks > 0)
         {
             h->split_half = (size_t)S.max_split_blocks * hyb::kSplitBytes;
+            h->tgt_half = (size_t)std::max<int64_t>(1, S.max_tc_targets);
             HYB_CUDA(cudaMalloc(&h->d_ops, 2 * h->split_half));
+            HYB_CUDA(cudaMalloc(&h->d_tgt, 2 * h->tgt_half * sizeof(int64_t)));
             h->g_factor[1].reset();
         }
         HYB_CUDA(cudaMemsetAsync(h->d_f32, 0, slab * sizeof(float), h->stream));

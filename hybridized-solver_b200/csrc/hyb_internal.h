@@ -99,6 +99,7 @@ struct Symbolic
     std::vector<LevelShape> shape;
 
     int64_t max_split_blocks = 0;     // max over uniform-64 levels of the split_pref span
+    int64_t max_tc_targets = 0;       // max over uniform-64 levels of the upd_pref span (target table)
     int64_t max_fwd_scratch_rows = 0; // max over levels of fwd_rows span
     int64_t max_bwd_scratch_rows = 0;
     double factor_flops = 0;          // exact algorithmic flops of the factorization

@@ -315,8 +315,11 @@ int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, co
         sh.uniform64 = uniform;
         sh.piv64 = piv64;
         if (uniform)
+        {
             S.max_split_blocks =
                 std::max(S.max_split_blocks, S.split_pref[S.lvl_ptr[l + 1]] - S.split_pref[S.lvl_ptr[l]]);
+            S.max_tc_targets = std::max(S.max_tc_targets, S.upd_pref[S.lvl_ptr[l + 1]] - S.upd_pref[S.lvl_ptr[l]]);
+        }
         S.max_fwd_scratch_rows =
             std::max(S.max_fwd_scratch_rows, S.fwd_rows[S.lvl_ptr[l + 1]] - S.fwd_rows[S.lvl_ptr[l]]);
         S.max_bwd_scratch_rows =

@@ -95,11 +95,15 @@ __device__ __forceinline__ void split8(const float (&x)[8], uint4 &hi, uint4 &lo
 // reads, so the update kernel only copies them into shared memory. Layout in `ops`: the
 // level's pivots in order, each with its n_lc lower blocks then its n_up upper blocks,
 // kSplitBytes apiece. L(t,k) is stored as it is (rows m, K = k contiguous); U(k,c) is
-// stored transposed (rows = its columns n, K = k contiguous).
+// stored transposed (rows = its columns n, K = k contiguous). The CTA of lower block i
+// also writes the slab offsets of the targets (t_i, c_j) of its row for every upper
+// column j into `tgt` (per pivot n_lc x n_up, at upd_pref[p] - upd_pref[p0]), so the
+// update kernel finds a tile's C blocks with one load.
 constexpr int kSplitThreads = 128;
 
 __global__ void __launch_bounds__(kSplitThreads)
-    k_split64(DevSym S, const float *__restrict__ slab, unsigned char *__restrict__ ops, int64_t p0, int64_t p1)
+    k_split64(DevSym S, const float *__restrict__ slab, unsigned char *__restrict__ ops, int64_t *__restrict__ tgt,
+              int64_t p0, int64_t p1)
 {
     __shared__ float tr[64 * 65];
     const int64_t u = S.split_pref[p0] + blockIdx.x;
@@ -123,6 +127,14 @@ __global__ void __launch_bounds__(kSplitThreads)
             const uint32_t off = sw128_offset(row, q * 8);
             *reinterpret_cast<uint4 *>(dst + off) = hi;
             *reinterpret_cast<uint4 *>(dst + kSplitHalf + off) = lo;
+        }
+        const int64_t n_up = S.row_ptr[k + 1] - S.diag_pos[k] - 1;
+        const int32_t t = S.lcol_row[S.lcol_ptr[k] + local];
+        int64_t *row_tgt = tgt + (S.upd_pref[p] - S.upd_pref[p0]) + local * n_up;
+        for (int64_t j = tid; j < n_up; j += kSplitThreads)
+        {
+            const int32_t c = S.cols[S.diag_pos[k] + 1 + j];
+            row_tgt[j] = S.blk_off[find_col(S.cols, S.row_ptr[t], S.row_ptr[t + 1], c)];
         }
         return;
     }
@@ -152,28 +164,42 @@ __global__ void __launch_bounds__(kSplitThreads)
     }
 }
 
+__device__ __forceinline__ void bulk_s2g(void *dst, const void *src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+                 "r"(bytes)
+                 : "memory");
+}
+
 // ----------------------------------------------------------------------------------
 // Uniform-64 FP32 Schur update on the tensor cores, C(t,c) -= L(t,k) U(k,c), computed
 // transposed: one tile is D = U(k, [c0 c1])^T L(t,k)^T (M = 128: the 2 x 64 columns of two
 // upper blocks, N = 64: the rows of one target row t, K = 64), so tensor-memory lane i holds
-// column i of the tile and a warp's 32 lanes read and write 32 consecutive floats of a row
-// of C. Each product takes three BF16 MMAs (hi*hi + hi*lo + lo*hi) accumulated in FP32.
+// column i of the tile. Each product takes three BF16 MMAs (hi*hi + hi*lo + lo*hi)
+// accumulated in FP32.
 //
-// A persistent CTA walks a contiguous range of tiles ordered column pair major, so the
-// U pair stays in shared memory across its rows. Warp 4 (one lane) copies operands from
-// the staged splits with bulk copies into a 4-stage ring; warp 5 (one lane) issues the
-// MMAs into one of two tensor-memory accumulators; warps 0-3 drain an accumulator, read C,
-// subtract and write C while the next tile's MMAs run. Every wait has an iteration limit;
-// on expiry the CTA sets ST_TIMEOUT, drains its copies and MMAs and returns.
+// One persistent CTA per SM walks a contiguous range of tiles ordered column pair major,
+// so the U pair stays in shared memory across its rows. All global traffic goes through
+// the bulk-copy engine: warp 8 (one lane) copies the U pair, the L(t,k) splits (2-stage
+// ring) and the tile's C blocks (3-slot ring, target offsets from the split kernel's
+// table); warp 9 (one lane) issues the MMAs into one of two tensor-memory accumulators;
+// warps 0-7 (warp w: lanes 32 (w & 3).., rows 32 (w >> 2)..) subtract the accumulator from
+// C in shared memory, and one of them bulk-stores the blocks back. At about 160 KB of
+// shared memory and few registers the CTA leaves room on its SM for the next pivot's
+// LU/solve CTA. Every wait is bounded in time; on expiry the CTA sets ST_TIMEOUT, drains its
+// copies and MMAs and returns.
 //
 // Tiles: mode 0 enumerates every pivot of the level through tc_pref (n_lc x column pairs);
 // with one pivot and lookahead, mode 1 takes row i0 (column pairs) and then column j0 alone
 // for every other row, and mode 2 the other rows x column pairs of the other columns.
 // An element's value does not depend on which columns share its tile, so all modes give
 // identical results.
-constexpr int kTcThreads = 192;
-constexpr int kTcStages = 4;
-constexpr int kTcSmem = 2 * kSplitBytes + kTcStages * kSplitBytes + 256 + 1024; // + alignment slack
+constexpr int kTcThreads = 320;
+constexpr int kTcEpiWarps = 8;
+constexpr int kTcStages = 2; // L(t,k) operand ring
+constexpr int kTcCSlots = 3; // C tile ring (two 16 KB blocks each)
+constexpr int kTcCBytes = 2 * 16384;
+constexpr int kTcSmem = 2 * kSplitBytes + kTcStages * kSplitBytes + kTcCSlots * kTcCBytes + 256 + 1024;
 
 struct TcTile
 {
@@ -236,40 +262,30 @@ __device__ __forceinline__ TcTile tc_tile(const DevSym &S, int64_t p0, int64_t p
     return x;
 }
 
-// Slab offset of the target block of tile t for the column block the calling warp writes
-// (warps 0-1: ja, 2-3: jb), or -1 if the tile has no such block. Called by whole warps.
-__device__ __forceinline__ int64_t tc_target(const DevSym &S, int64_t p0, int64_t p1, int mode, int i0, int j0,
-                                             int64_t t, int warp)
-{
-    const TcTile x = tc_tile(S, p0, p1, mode, i0, j0, t);
-    const int32_t j = warp < 2 ? x.ja : x.jb;
-    if (j < 0)
-        return -1;
-    const int64_t k = S.piv[x.p];
-    const int32_t c = S.cols[S.diag_pos[k] + 1 + j];
-    const int32_t tr = S.lcol_row[S.lcol_ptr[k] + x.row];
-    return S.blk_off[warp_find_col(S.cols, S.row_ptr[tr], S.row_ptr[tr + 1], c)];
-}
-
-__global__ void __launch_bounds__(kTcThreads, 2)
-    k_update64_tc(DevSym S, float *__restrict__ slab, const unsigned char *__restrict__ ops, int64_t p0, int64_t p1,
-                  int mode, int i0, int j0, int64_t n_tiles, int *status)
+__global__ void __launch_bounds__(kTcThreads, 1)
+    k_update64_tc(DevSym S, float *__restrict__ slab, const unsigned char *__restrict__ ops,
+                  const int64_t *__restrict__ tgt, int64_t p0, int64_t p1, int mode, int i0, int j0, int64_t n_tiles,
+                  int *status)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
-    unsigned char *u_hi = base;                 // M = 128 rows: column block ja, then jb
-    unsigned char *u_lo = u_hi + kSplitBytes;   //
-    unsigned char *ring = u_lo + kSplitBytes;   // kTcStages x (hi 8 KB, lo 8 KB) of L(t,k)
-    uint64_t *bars = reinterpret_cast<uint64_t *>(ring + kTcStages * kSplitBytes);
-    uint64_t *full = bars;                      // [kTcStages] operand landed
-    uint64_t *empty = bars + kTcStages;         // [kTcStages] operand consumed by the MMAs
-    uint64_t *ufull = bars + 2 * kTcStages;     // U pair landed
-    uint64_t *uempty = ufull + 1;               // MMAs on the previous U pair done
-    uint64_t *tfull = ufull + 2;                // [2] accumulator ready
-    uint64_t *tempty = ufull + 4;               // [2] accumulator drained (4 warp arrivals)
-    uint64_t *done = ufull + 6;                 // all MMAs of the CTA done
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(ufull + 7);
+    unsigned char *u_hi = base;                           // M = 128 rows: column block ja, then jb
+    unsigned char *u_lo = u_hi + kSplitBytes;             //
+    unsigned char *ring = u_lo + kSplitBytes;             // kTcStages x (hi 8 KB, lo 8 KB) of L(t,k)
+    unsigned char *cbuf = ring + kTcStages * kSplitBytes; // kTcCSlots x (C(t, c_ja), C(t, c_jb)) FP32
+    uint64_t *bars = reinterpret_cast<uint64_t *>(cbuf + kTcCSlots * kTcCBytes);
+    uint64_t *full = bars;                // [kTcStages] operand landed
+    uint64_t *empty = full + kTcStages;   // [kTcStages] operand consumed by the MMAs
+    uint64_t *cfull = empty + kTcStages;  // [kTcCSlots] C blocks landed
+    uint64_t *cempty = cfull + kTcCSlots; // [kTcCSlots] C blocks stored back (slot free)
+    uint64_t *ufull = cempty + kTcCSlots; // U pair landed
+    uint64_t *uempty = ufull + 1;         // MMAs on the previous U pair done
+    uint64_t *tfull = ufull + 2;          // [2] accumulator ready
+    uint64_t *tempty = ufull + 4;         // [2] accumulator drained (one arrival per epilogue warp)
+    uint64_t *done = ufull + 6;           // all MMAs of the CTA done
+    int64_t *coff = reinterpret_cast<int64_t *>(ufull + 7); // [kTcCSlots][2] target offsets of a slot
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(coff + 2 * kTcCSlots);
     __shared__ int s_fail;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -281,12 +297,17 @@ __global__ void __launch_bounds__(kTcThreads, 2)
             mbar_init(full + i, 1);
             mbar_init(empty + i, 1);
         }
+        for (int i = 0; i < kTcCSlots; ++i)
+        {
+            mbar_init(cfull + i, 1);
+            mbar_init(cempty + i, 1);
+        }
         mbar_init(ufull, 1);
         mbar_init(uempty, 1);
         mbar_init(tfull, 1);
         mbar_init(tfull + 1, 1);
-        mbar_init(tempty, 4);
-        mbar_init(tempty + 1, 4);
+        mbar_init(tempty, kTcEpiWarps);
+        mbar_init(tempty + 1, kTcEpiWarps);
         mbar_init(done, 1);
         s_fail = schedule_aborted(status);
     }
@@ -301,24 +322,46 @@ __global__ void __launch_bounds__(kTcThreads, 2)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
     const int64_t lvl_base = S.split_pref[p0];
+    const int64_t tgt_base = S.upd_pref[p0];
     const bool run = s_fail == 0; // read by every thread before any role can change it
     __syncthreads();
 
     if (!run)
     {
     }
-    else if (warp == 4)
+    else if (warp == kTcEpiWarps)
     {
-        // ---- producer: U pair on change, one L(t,k) split per tile
+        // ---- producer: U pair on change, one L(t,k) split and the C blocks per tile
         if (lane == 0)
         {
+            // target offsets of a tile (loads issued one tile ahead of their use)
+            auto targets = [&](const TcTile &x, int64_t &oa, int64_t &ob) {
+                const int64_t k = S.piv[x.p];
+                const int64_t n_up = S.row_ptr[k + 1] - S.diag_pos[k] - 1;
+                const int64_t *row_tgt = tgt + (S.upd_pref[x.p] - tgt_base) + x.row * n_up;
+                oa = row_tgt[x.ja];
+                ob = x.jb >= 0 ? row_tgt[x.jb] : -1;
+            };
             int64_t cur_p = -1;
             int32_t cur_a = -2, cur_b = -2;
             uint32_t uloads = 0;
+            TcTile xn{};
+            int64_t na = -1, nb = -1;
+            if (t0 < t1)
+            {
+                xn = tc_tile(S, p0, p1, mode, i0, j0, t0);
+                targets(xn, na, nb);
+            }
             int64_t i = 0;
             for (int64_t t = t0; t < t1; ++t, ++i)
             {
-                const TcTile x = tc_tile(S, p0, p1, mode, i0, j0, t);
+                const TcTile x = xn;
+                const int64_t off_a = na, off_b = nb;
+                if (t + 1 < t1)
+                {
+                    xn = tc_tile(S, p0, p1, mode, i0, j0, t + 1);
+                    targets(xn, na, nb);
+                }
                 const int64_t k = S.piv[x.p];
                 const int64_t n_lc = S.lcol_ptr[k + 1] - S.lcol_ptr[k];
                 const unsigned char *pb = ops + (S.split_pref[x.p] - lvl_base) * (int64_t)kSplitBytes;
@@ -352,17 +395,34 @@ __global__ void __launch_bounds__(kTcThreads, 2)
                 }
                 mbar_expect_tx(full + s, kSplitBytes);
                 bulk_g2s(ring + s * kSplitBytes, pb + x.row * (int64_t)kSplitBytes, kSplitBytes, full + s);
+                const int cs = (int)(i % kTcCSlots);
+                if (i >= kTcCSlots && !mbar_wait(cempty + cs, (uint32_t)((i / kTcCSlots - 1) & 1)))
+                {
+                    s_fail = 1;
+                    break;
+                }
+                coff[2 * cs] = off_a;
+                coff[2 * cs + 1] = off_b;
+                unsigned char *cb = cbuf + cs * kTcCBytes;
+                // the arrive releases coff to the epilogue together with the copies
+                mbar_expect_tx(cfull + cs, off_b >= 0 ? 2 * 16384 : 16384);
+                bulk_g2s(cb, slab + off_a, 16384, cfull + cs);
+                if (off_b >= 0)
+                    bulk_g2s(cb + 16384, slab + off_b, 16384, cfull + cs);
             }
             // drain: every copy issued lands before the CTA can leave
             const int64_t issued = i;
             for (int64_t j = issued > kTcStages ? issued - kTcStages : 0; j < issued; ++j)
                 if (!mbar_wait(full + (j % kTcStages), (uint32_t)((j / kTcStages) & 1)))
                     s_fail = 1;
+            for (int64_t j = issued > kTcCSlots ? issued - kTcCSlots : 0; j < issued; ++j)
+                if (!mbar_wait(cfull + (j % kTcCSlots), (uint32_t)((j / kTcCSlots) & 1)))
+                    s_fail = 1;
             if (uloads > 0 && !mbar_wait(ufull, (uloads - 1) & 1))
                 s_fail = 1;
         }
     }
-    else if (warp == 5)
+    else if (warp == kTcEpiWarps + 1)
     {
         // ---- MMA issuer
         if (lane == 0)
@@ -420,51 +480,60 @@ __global__ void __launch_bounds__(kTcThreads, 2)
     }
     else
     {
-        // ---- epilogue warps 0-3: lane i of warp w is column (w & 1) * 32 + i of block
-        // (w < 2 ? ja : jb); registers hold the tile's 64 rows. The next tile's target is
-        // looked up while this tile's C loads are in flight.
+        // ---- epilogue warps 0-7: lane i of warp w is column (w & 1) * 32 + i of block
+        // ((w & 3) < 2 ? ja : jb) and covers rows 32 (w >> 2) .. + 31 of the tile. Every
+        // epilogue warp runs all of the CTA's tiles -- after a failed wait without waiting or
+        // computing -- so the named barrier below always sees all eight warps.
+        const int q = warp & 3, h = warp >> 2;
+        const int cb_idx = q >> 1;
+        const int col = (q & 1) * 32 + lane;
+        bool failed = false; // warp-uniform
         int64_t i = 0;
-        int64_t next_off = t0 < t1 ? tc_target(S, p0, p1, mode, i0, j0, t0, warp) : -1;
         for (int64_t t = t0; t < t1; ++t, ++i)
         {
-            float *gc = nullptr;
-            float cv[64];
-            if (next_off >= 0)
-            {
-                gc = slab + next_off + (warp & 1) * 32 + lane;
-#pragma unroll
-                for (int r = 0; r < 64; ++r)
-                    cv[r] = gc[r * 64];
-            }
-            if (t + 1 < t1)
-                next_off = tc_target(S, p0, p1, mode, i0, j0, t + 1, warp);
             const int a = (int)(i & 1);
-            // warp-uniform outcome: the lookups above and below use full-warp ballots
-            if (!__all_sync(0xffffffffu, mbar_wait(tfull + a, (uint32_t)((i >> 1) & 1))))
+            const int cs = (int)(i % kTcCSlots);
+            if (!failed && !__all_sync(0xffffffffu, mbar_wait(tfull + a, (uint32_t)((i >> 1) & 1)) &&
+                                                        mbar_wait(cfull + cs, (uint32_t)((i / kTcCSlots) & 1))))
             {
                 s_fail = 1;
-                break;
+                failed = true;
             }
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            uint32_t v0[32], v1[32];
-            const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(a * 64);
-            tmem_load32(ta, v0);
-            tmem_load32(ta + 32, v1);
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            __syncwarp();
-            if (lane == 0)
-                mbar_arrive(tempty + a);
-            if (gc != nullptr)
+            if (!failed)
             {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                uint32_t v[32];
+                tmem_load32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * 64 + h * 32), v);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                __syncwarp();
+                if (lane == 0)
+                    mbar_arrive(tempty + a);
+                if (cb_idx == 0 || coff[2 * cs + 1] >= 0)
+                {
+                    float *c =
+                        reinterpret_cast<float *>(cbuf + cs * kTcCBytes + cb_idx * 16384) + h * 32 * 64 + col;
 #pragma unroll
-                for (int r = 0; r < 32; ++r)
-                    gc[r * 64] = cv[r] - __uint_as_float(v0[r]);
-#pragma unroll
-                for (int r = 0; r < 32; ++r)
-                    gc[(r + 32) * 64] = cv[r + 32] - __uint_as_float(v1[r]);
+                    for (int r = 0; r < 32; ++r)
+                        c[r * 64] -= __uint_as_float(v[r]);
+                }
+            }
+            // the bulk store reads what the generic stores wrote
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("bar.sync 1, %0;" ::"n"(kTcEpiWarps * 32) : "memory");
+            if (tid == 0 && !failed) // warp 0 saw this slot's C land, so its offsets are valid
+            {
+                const unsigned char *cb = cbuf + cs * kTcCBytes;
+                bulk_s2g(slab + coff[2 * cs], cb, 16384);
+                if (coff[2 * cs + 1] >= 0)
+                    bulk_s2g(slab + coff[2 * cs + 1], cb + 16384, 16384);
+                asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+                mbar_arrive(cempty + cs);
             }
         }
+        if (tid == 0)
+            asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); // stores complete before exit
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
