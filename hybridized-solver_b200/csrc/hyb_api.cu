@@ -60,7 +60,7 @@ int smem_optin()
 // Dynamic shared memory the forward solve stage may take (its static arrays aside).
 int solve_smem_cap()
 {
-    return smem_optin() - 4096;
+    return smem_optin() - 8192;
 }
 
 // Streaming multiprocessors of the current device.
@@ -125,11 +125,20 @@ struct hyb_system
     cudaEvent_t ev_prio = nullptr, ev_piv = nullptr, ev_join = nullptr;
     bool lookahead = true;
     bool umma = true; // mixed-form updates of 64-blocks on the tcgen05 tensor cores
+    bool flow = true; // dataflow substitution (enqueue_solve_flow) in hyb_solve
     void *arena = nullptr;
     DevSym ds{};
     double *d_a = nullptr; // original values (FP64, CSR order)
     int *d_status = nullptr;
     int *d_tickets = nullptr; // per pivot: partial products of the solve stage already published
+    // dataflow solve: per block row the tag of the last solve direction that finished it,
+    // the solve's status words, and the partial products of every pivot (flow_nrhs columns)
+    int *d_flags = nullptr;
+    int *d_solve_status = nullptr;
+    uint32_t solve_epoch = 0;
+    double *d_flow64 = nullptr;
+    float *d_flow32 = nullptr;
+    int64_t flow64_nrhs = 0, flow32_nrhs = 0;
     int factored = -1; // -1, HYB_PRECISION_FP64 or HYB_PRECISION_MIXED
     double *d_f64 = nullptr;
     float *d_f32 = nullptr;
@@ -164,6 +173,10 @@ struct hyb_system
         cudaFree(d_a);
         cudaFree(d_status);
         cudaFree(d_tickets);
+        cudaFree(d_flags);
+        cudaFree(d_solve_status);
+        cudaFree(d_flow64);
+        cudaFree(d_flow32);
         cudaFree(d_f64);
         cudaFree(d_f32);
         cudaFree(d_ops);
@@ -249,6 +262,9 @@ int upload_symbolic(hyb_system *h)
         {S.tc_pref.data(), S.tc_pref.size() * 8, (const void **)&d.tc_pref},
         {S.fwd_pref.data(), S.fwd_pref.size() * 8, (const void **)&d.fwd_pref},
         {S.fwdu_pref.data(), S.fwdu_pref.size() * 8, (const void **)&d.fwdu_pref},
+        {S.fwd_item_p.data(), S.fwd_item_p.size() * 4, (const void **)&d.fwd_item_p},
+        {S.bwd_item_p.data(), S.bwd_item_p.size() * 4, (const void **)&d.bwd_item_p},
+        {S.bwd_first.data(), S.bwd_first.size() * 8, (const void **)&d.bwd_first},
         {S.fwd_rows.data(), S.fwd_rows.size() * 8, (const void **)&d.fwd_rows},
         {S.bwd_rows.data(), S.bwd_rows.size() * 8, (const void **)&d.bwd_rows},
         {S.mt_tgt.data(), S.mt_tgt.size() * 4, (const void **)&d.mt_tgt},
@@ -541,6 +557,81 @@ template <typename T, typename V> int enqueue_solve(hyb_system *h, const T *slab
     return HYB_SUCCESS;
 }
 
+// Largest diagonal block of the system.
+int max_pivot(const Symbolic &S)
+{
+    int m = 0;
+    for (const Symbolic::LevelShape &sh : S.shape)
+        m = std::max(m, sh.max_piv);
+    return m;
+}
+
+template <typename V> V *&flow_scratch(hyb_system *h);
+template <> double *&flow_scratch<double>(hyb_system *h)
+{
+    return h->d_flow64;
+}
+template <> float *&flow_scratch<float>(hyb_system *h)
+{
+    return h->d_flow32;
+}
+
+// Dataflow substitution of y (dof x nrhs) with the factors in `slab`: one cooperative
+// launch per direction. Returns HYB_TOO_LARGE (before anything is enqueued) when the
+// device cannot keep a useful grid resident, in which case the caller uses the staged solve.
+template <typename T, typename V> int enqueue_solve_flow(hyb_system *h, const T *slab, V *y, int nrhs, uint64_t &launches)
+{
+    const Symbolic &S = h->S;
+    const int mp = max_pivot(S);
+    const int acc_bytes = (mp * nrhs * (int)sizeof(V) + 15) / 16 * 16;
+    const int diag_bytes = mp * (mp | 1) * (int)sizeof(T);
+    int stage = acc_bytes + diag_bytes <= solve_smem_cap() ? 1 : 0;
+    const int fwd_smem = acc_bytes + (stage ? diag_bytes : 0);
+    int per_sm_f = 0, per_sm_b = 0, coop = 0, dev = 0;
+    HYB_CUDA(cudaGetDevice(&dev));
+    HYB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    HYB_CUDA(cudaFuncSetAttribute(hyb::k_fwd_flow<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, fwd_smem));
+    HYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, hyb::k_fwd_flow<T, V>, hyb::kThreads, fwd_smem));
+    HYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_b, hyb::k_bwd_flow<T, V>, hyb::kThreads, 0));
+    if (!coop || per_sm_f < 1 || per_sm_b < 1)
+        return HYB_TOO_LARGE;
+    V *&scr = flow_scratch<V>(h);
+    int64_t &have = std::is_same_v<V, double> ? h->flow64_nrhs : h->flow32_nrhs;
+    if (have < nrhs)
+    {
+        cudaFree(scr);
+        scr = nullptr;
+        have = 0;
+        const int64_t rows = std::max<int64_t>(1, std::max(S.fwd_rows[S.n], S.bwd_rows[S.n]));
+        HYB_CUDA(cudaMalloc(&scr, rows * nrhs * sizeof(V)));
+        have = nrhs;
+    }
+    cudaStream_t st = h->stream;
+    HYB_CUDA(cudaMemsetAsync(h->d_tickets, 0, S.n * sizeof(int), st));
+    HYB_CUDA(cudaMemsetAsync(h->d_solve_status, 0, hyb::ST_WORDS * sizeof(int), st));
+    h->solve_epoch = (h->solve_epoch + 1) & 0x3fffffffu;
+    int tag_f = (int)(2 * h->solve_epoch + 1), tag_b = tag_f + 1;
+    DevSym ds = h->ds;
+    V *scratch = scr;
+    int *tickets = h->d_tickets, *flags = h->d_flags, *status = h->d_solve_status;
+    int64_t nf = (int64_t)S.fwd_item_p.size(), nb = (int64_t)S.bwd_item_p.size();
+    const int sms = sm_count();
+    {
+        const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nf, (int64_t)per_sm_f * sms));
+        void *args[] = {&ds, (void *)&slab, &y, &scratch, &tickets, &flags, &tag_f, &nf, &nrhs, &stage, &status};
+        HYB_CUDA(cudaLaunchCooperativeKernel((const void *)hyb::k_fwd_flow<T, V>, dim3(grid), dim3(hyb::kThreads),
+                                             args, fwd_smem, st));
+    }
+    {
+        const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nb, (int64_t)per_sm_b * sms));
+        void *args[] = {&ds, (void *)&slab, &y, &scratch, &tickets, &flags, &tag_b, &nb, &nrhs, &status};
+        HYB_CUDA(cudaLaunchCooperativeKernel((const void *)hyb::k_bwd_flow<T, V>, dim3(grid), dim3(hyb::kThreads),
+                                             args, 0, st));
+    }
+    launches += 2;
+    return HYB_SUCCESS;
+}
+
 // Runs `body` (which enqueues work and counts launches) through a cached CUDA graph.
 template <typename F> int run_graph(hyb_system *h, std::unique_ptr<GraphExec> &slot, F body)
 {
@@ -570,6 +661,22 @@ template <typename F> int run_graph(hyb_system *h, std::unique_ptr<GraphExec> &s
     HYB_CUDA(cudaGraphLaunch(slot->exec, h->stream));
     h->last_launches += slot->launches;
     return HYB_SUCCESS;
+}
+
+// One substitution of y with the factors in `slab`: the dataflow form when it is enabled
+// and the device can run it, else the staged form through the cached graph `slot`.
+template <typename T, typename V>
+int substitute(hyb_system *h, const T *slab, V *y, V *scratch, int nrhs, std::unique_ptr<GraphExec> &slot)
+{
+    if (h->flow)
+    {
+        uint64_t count = 0;
+        const int rc = enqueue_solve_flow<T, V>(h, slab, y, nrhs, count);
+        h->last_launches += count;
+        if (rc != HYB_TOO_LARGE)
+            return rc;
+    }
+    return run_graph(h, slot, [&](uint64_t &count) { return enqueue_solve<T, V>(h, slab, y, scratch, nrhs, count); });
 }
 
 int ensure_solve_buffers(hyb_system *h, int64_t nrhs)
@@ -772,6 +879,9 @@ HYB_API int hyb_system_create(uint64_t n, const uint64_t *block_sizes, const uin
     HYB_CUDA(cudaMemsetAsync(h->d_a, 0, std::max<int64_t>(1, h->S.a_val_off.back()) * sizeof(double), h->stream));
     HYB_CUDA(cudaMalloc(&h->d_status, hyb::ST_WORDS * sizeof(int)));
     HYB_CUDA(cudaMalloc(&h->d_tickets, h->S.n * sizeof(int)));
+    HYB_CUDA(cudaMalloc(&h->d_flags, h->S.n * sizeof(int)));
+    HYB_CUDA(cudaMemsetAsync(h->d_flags, 0, h->S.n * sizeof(int), h->stream));
+    HYB_CUDA(cudaMalloc(&h->d_solve_status, hyb::ST_WORDS * sizeof(int)));
     HYB_CUDA(cudaMemsetAsync(h->d_tickets, 0, h->S.n * sizeof(int), h->stream));
     HYB_CUDA(cudaStreamSynchronize(h->stream));
     *out = h.release();
@@ -805,6 +915,7 @@ HYB_API int hyb_system_copy(const hyb_system *src, hyb_system **out)
     h->device = src->device;
     h->lookahead = src->lookahead;
     h->umma = src->umma;
+    h->flow = src->flow;
     HYB_CUDA(create_streams(h.get()));
     int rc = upload_symbolic(h.get());
     if (rc != HYB_SUCCESS)
@@ -813,6 +924,9 @@ HYB_API int hyb_system_copy(const hyb_system *src, hyb_system **out)
     HYB_CUDA(cudaMalloc(&h->d_a, a_bytes));
     HYB_CUDA(cudaMalloc(&h->d_status, hyb::ST_WORDS * sizeof(int)));
     HYB_CUDA(cudaMalloc(&h->d_tickets, h->S.n * sizeof(int)));
+    HYB_CUDA(cudaMalloc(&h->d_flags, h->S.n * sizeof(int)));
+    HYB_CUDA(cudaMemsetAsync(h->d_flags, 0, h->S.n * sizeof(int), h->stream));
+    HYB_CUDA(cudaMalloc(&h->d_solve_status, hyb::ST_WORDS * sizeof(int)));
     HYB_CUDA(cudaMemsetAsync(h->d_tickets, 0, h->S.n * sizeof(int), h->stream));
     HYB_CUDA(cudaStreamSynchronize(src->stream));
     HYB_CUDA(cudaMemcpyAsync(h->d_a, src->d_a, a_bytes, cudaMemcpyDeviceToDevice, h->stream));
@@ -868,6 +982,9 @@ HYB_API int hyb_system_set_option(hyb_system *h, int option, int64_t value)
             h->umma = value != 0;
             h->g_factor[1].reset();
         }
+        return HYB_SUCCESS;
+    case HYB_OPTION_DATAFLOW_SOLVE:
+        h->flow = value != 0;
         return HYB_SUCCESS;
     default:
         return HYB_INVALID_ARGUMENT;
@@ -1047,6 +1164,7 @@ HYB_API int hyb_solve(hyb_system *h, const double *b, double *x, uint64_t nrhs, 
     if (tol <= 0)
         tol = 1e-12;
     HYB_CUDA(cudaMemcpyAsync(h->d_b, b, bytes, in, h->stream));
+    HYB_CUDA(cudaMemsetAsync(h->d_solve_status, 0, hyb::ST_WORDS * sizeof(int), h->stream));
     uint32_t iters = 0;
     double relres = -1;
     int status = HYB_SUCCESS;
@@ -1054,9 +1172,7 @@ HYB_API int hyb_solve(hyb_system *h, const double *b, double *x, uint64_t nrhs, 
     {
         HYB_CUDA(cudaMemcpyAsync(h->d_x, h->d_b, bytes, cudaMemcpyDeviceToDevice, h->stream));
         auto &slot = h->g_solve[{HYB_PRECISION_FP64, nr}];
-        rc = run_graph(h, slot, [&](uint64_t &count) {
-            return enqueue_solve<double, double>(h, h->d_f64, h->d_x, h->d_scr64, nr, count);
-        });
+        rc = substitute<double, double>(h, h->d_f64, h->d_x, h->d_scr64, nr, slot);
         if (rc != HYB_SUCCESS)
             return rc;
         if (want_residual)
@@ -1080,12 +1196,10 @@ HYB_API int hyb_solve(hyb_system *h, const double *b, double *x, uint64_t nrhs, 
         // Mixed: x0 = LU32^{-1} b, then x += LU32^{-1} (b - A x) with the FP64 residual.
         uint64_t cnt = 0;
         auto &slot = h->g_solve[{HYB_PRECISION_MIXED, nr}];
-        auto solve32 = [&](uint64_t &count) {
-            return enqueue_solve<float, float>(h, h->d_f32, h->d_yf, h->d_scr32, nr, count);
-        };
+        auto solve32 = [&]() { return substitute<float, float>(h, h->d_f32, h->d_yf, h->d_scr32, nr, slot); };
         hyb::k_convert<double, float><<<elementwise_grid(len), hyb::kThreads, 0, h->stream>>>(h->d_b, h->d_yf, len);
         ++cnt;
-        rc = run_graph(h, slot, solve32);
+        rc = solve32();
         if (rc != HYB_SUCCESS)
             return rc;
         hyb::k_convert<float, double><<<elementwise_grid(len), hyb::kThreads, 0, h->stream>>>(h->d_yf, h->d_x, len);
@@ -1112,7 +1226,7 @@ HYB_API int hyb_solve(hyb_system *h, const double *b, double *x, uint64_t nrhs, 
             hyb::k_convert<double, float><<<elementwise_grid(len), hyb::kThreads, 0, h->stream>>>(h->d_r, h->d_yf,
                                                                                                 len);
             ++cnt;
-            rc = run_graph(h, slot, solve32);
+            rc = solve32();
             if (rc != HYB_SUCCESS)
                 return rc;
             hyb::k_add_correction<float><<<elementwise_grid(len), hyb::kThreads, 0, h->stream>>>(h->d_x, h->d_yf,
@@ -1124,7 +1238,14 @@ HYB_API int hyb_solve(hyb_system *h, const double *b, double *x, uint64_t nrhs, 
     }
     HYB_CUDA(cudaGetLastError());
     HYB_CUDA(cudaMemcpyAsync(x, h->d_x, bytes, outk, h->stream));
+    int sst[hyb::ST_WORDS];
+    HYB_CUDA(cudaMemcpyAsync(sst, h->d_solve_status, sizeof(sst), cudaMemcpyDeviceToHost, h->stream));
     HYB_CUDA(cudaStreamSynchronize(h->stream));
+    if (sst[hyb::ST_TIMEOUT])
+    {
+        g_cuda_error = "a wait of the dataflow solve ran out of its time limit";
+        return HYB_CUDA_ERROR;
+    }
     h->launches += h->last_launches;
     if (info)
     {

@@ -54,8 +54,11 @@ struct Symbolic
     std::vector<int64_t> tc_pref;    // [n+1] prefix of n_lc * ceil(n_up / 2): tensor-core update tiles
     std::vector<int64_t> fwd_pref;  // [n+1] prefix of lower-row block counts
     std::vector<int64_t> fwdu_pref; // [n+1] prefix of max(1, lower-row block count): forward solve units
-    std::vector<int64_t> fwd_rows;  // [n+1] prefix of lower-row block count * pivot size (scratch rows)
-    std::vector<int64_t> bwd_rows;  // [n+1] prefix of upper-row block count * pivot size
+    std::vector<int32_t> fwd_item_p; // [fwdu_pref[n]] pivot slot of each forward dataflow item
+    std::vector<int32_t> bwd_item_p; // backward dataflow items (levels descending, max(1, n_up) per pivot)
+    std::vector<int64_t> bwd_first;  // [n] first backward item of each pivot slot
+    std::vector<int64_t> fwd_rows;  // [n+1] prefix of lower-row block count * pivot size, padded to 4 (scratch rows)
+    std::vector<int64_t> bwd_rows;  // [n+1] prefix of upper-row block count * pivot size, padded to 4
 
     // Levels whose pivots share target rows get explicit target lists, each target's
     // sources in ascending pivot order (a fixed order, no atomics).

@@ -14,6 +14,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 namespace hyb
@@ -40,6 +41,9 @@ struct DevSym
     const int64_t *tc_pref;
     const int64_t *fwd_pref;
     const int64_t *fwdu_pref;
+    const int32_t *fwd_item_p; // dataflow forward solve: pivot slot of item j (fwdu_pref order)
+    const int32_t *bwd_item_p; // dataflow backward solve: pivot slot of item j (levels descending)
+    const int64_t *bwd_first;  // [n] first backward item of pivot slot p
     const int64_t *fwd_rows;
     const int64_t *bwd_rows;
     const int32_t *mt_tgt;
@@ -974,29 +978,74 @@ __device__ void warp_lu_solve_smem(const T *d, int ldd, int m, V *acc, int r, in
 }
 
 // out[e] = y[e] - sum_j part[j][e] for e < E (E = rows x right-hand sides), with every
-// thread of the CTA busy: G = blockDim / E groups each sum every G-th partial, then the G
-// group sums are subtracted in group order (a fixed order, so results are reproducible).
-// `red` is shared scratch of blockDim values; `out` may alias `y`.
+// thread of the CTA busy: the E values are read as 16-byte vectors when aligned, G =
+// blockDim / (vectors per partial) groups each sum every G-th partial with eight loads in
+// flight, then the group sums are subtracted in group order (a fixed order, so results are
+// reproducible). `red` is shared scratch of blockDim x 16 bytes; `out` may alias `y`.
+__device__ __forceinline__ void vadd(double &a, double b) { a += b; }
+__device__ __forceinline__ void vadd(float &a, float b) { a += b; }
+__device__ __forceinline__ void vadd(double2 &a, double2 b)
+{
+    a.x += b.x;
+    a.y += b.y;
+}
+__device__ __forceinline__ void vadd(float4 &a, float4 b)
+{
+    a.x += b.x;
+    a.y += b.y;
+    a.z += b.z;
+    a.w += b.w;
+}
+
+// Sum over j = g, g + G, ... < nparts of part[j * EU + e] (U: scalar or 16-byte vector).
+template <typename U>
+__device__ __forceinline__ U sum_strided(const U *__restrict__ part, int64_t nparts, int EU, int G, int g, int e)
+{
+    U s[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+        s[q] = U{};
+    int64_t j = g;
+    for (; j + 7 * (int64_t)G < nparts; j += 8 * (int64_t)G)
+    {
+        U v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            v[q] = __ldcg(part + (j + q * G) * EU + e);
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            vadd(s[q], v[q]);
+    }
+    // at most seven left
+#pragma unroll
+    for (int q = 0; q < 7; ++q)
+        if (j + q * (int64_t)G < nparts)
+            vadd(s[q], __ldcg(part + (j + q * G) * EU + e));
+#pragma unroll
+    for (int q = 1; q < 8; ++q)
+        vadd(s[0], s[q]);
+    return s[0];
+}
+
 template <typename V>
 __device__ void subtract_partials(const V *y, const V *__restrict__ part, int64_t nparts, int E, V *out, V *red)
 {
+    using Vec = typename std::conditional<sizeof(V) == 8, double2, float4>::type;
+    constexpr int W = 16 / sizeof(V);
     const int tid = threadIdx.x, nt = blockDim.x;
-    const int G = E < nt ? nt / E : 1;
+    const bool vec = E % W == 0 && (reinterpret_cast<uintptr_t>(part) & 15) == 0;
+    const int EU = vec ? E / W : E;
+    const int G = EU < nt ? nt / EU : 1;
     if (G > 1)
     {
-        const int g = tid / E, e = tid - g * E;
+        const int g = tid / EU, e = tid - g * EU;
         if (g < G)
         {
-            V s0 = 0, s1 = 0;
-            int64_t j = g;
-            for (; j + G < nparts; j += 2 * G)
-            {
-                s0 += __ldcg(part + j * E + e);
-                s1 += __ldcg(part + (j + G) * E + e);
-            }
-            if (j < nparts)
-                s0 += __ldcg(part + j * E + e);
-            red[g * E + e] = s0 + s1;
+            if (vec)
+                reinterpret_cast<Vec *>(red)[g * EU + e] =
+                    sum_strided(reinterpret_cast<const Vec *>(part), nparts, EU, G, g, e);
+            else
+                red[g * EU + e] = sum_strided(part, nparts, EU, G, g, e);
         }
         __syncthreads();
         for (int e2 = tid; e2 < E; e2 += nt)
@@ -1009,39 +1058,17 @@ __device__ void subtract_partials(const V *y, const V *__restrict__ part, int64_
         return;
     }
     for (int e2 = tid; e2 < E; e2 += nt)
-    {
-        V v = y[e2];
-        for (int64_t j = 0; j < nparts; ++j)
-            v -= __ldcg(part + j * E + e2);
-        out[e2] = v;
-    }
+        out[e2] = y[e2] - sum_strided(part, nparts, E, 1, 0, e2);
 }
 
-// Forward stage: y_k <- D_k^{-1} (y_k - sum_s L(k,s) y_s) for the stage's pivots
-// (block_system_apply_operations, src/blocks.c:729-769). Units: fwdu_pref, one per lower
-// block of a pivot (at least one per pivot).
+// Finishes pivot k of a forward stage: y_k <- D_k^{-1} (y_k - sum of its nparts partial
+// products), in ascending block order, D_k staged in shared memory when it fits.
 template <typename T, typename V>
-__global__ void __launch_bounds__(kThreads)
-    k_fwd_stage(DevSym S, const T *__restrict__ slab, V *__restrict__ y, V *__restrict__ scratch,
-                int *__restrict__ tickets, int64_t p0, int64_t p1, int nrhs, int stage_diag)
+__device__ void fwd_finish(const DevSym &S, const T *__restrict__ slab, V *__restrict__ y, const V *part,
+                           int64_t nparts, int64_t k, int nrhs, int stage_diag, unsigned char *smem_raw)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int64_t u = S.fwdu_pref[p0] + blockIdx.x;
-    const int64_t p = find_owner(S.fwdu_pref, p0, p1, u);
-    const int64_t k = S.piv[p];
     const int m = S.size[k];
-    const int64_t nparts = S.diag_pos[k] - S.row_ptr[k];
-    V *part = scratch + (S.fwd_rows[p] - S.fwd_rows[p0]) * nrhs;
-    if (nparts > 0)
-    {
-        const int64_t j = u - S.fwdu_pref[p];
-        const int64_t blk = S.row_ptr[k] + j;
-        const int32_t src = S.cols[blk];
-        block_gemv(slab + S.blk_off[blk], m, S.size[src], y + S.dof_off[src] * nrhs, part + j * m * nrhs, nrhs);
-        if (!last_ticket(tickets, p, nparts))
-            return;
-    }
-    __shared__ V red[kThreads];
+    __shared__ __align__(16) V red[kThreads * 16 / sizeof(V)];
     V *acc = reinterpret_cast<V *>(smem_raw); // m * nrhs
     V *yk = y + S.dof_off[k] * nrhs;
     subtract_partials(yk, part, nparts, m * nrhs, acc, red);
@@ -1080,6 +1107,33 @@ __global__ void __launch_bounds__(kThreads)
         yk[i] = acc[i];
 }
 
+// Forward stage: y_k <- D_k^{-1} (y_k - sum_s L(k,s) y_s) for the stage's pivots
+// (block_system_apply_operations, src/blocks.c:729-769). Units: fwdu_pref, one per lower
+// block of a pivot (at least one per pivot).
+template <typename T, typename V>
+__global__ void __launch_bounds__(kThreads)
+    k_fwd_stage(DevSym S, const T *__restrict__ slab, V *__restrict__ y, V *__restrict__ scratch,
+                int *__restrict__ tickets, int64_t p0, int64_t p1, int nrhs, int stage_diag)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int64_t u = S.fwdu_pref[p0] + blockIdx.x;
+    const int64_t p = find_owner(S.fwdu_pref, p0, p1, u);
+    const int64_t k = S.piv[p];
+    const int m = S.size[k];
+    const int64_t nparts = S.diag_pos[k] - S.row_ptr[k];
+    V *part = scratch + (S.fwd_rows[p] - S.fwd_rows[p0]) * nrhs;
+    if (nparts > 0)
+    {
+        const int64_t j = u - S.fwdu_pref[p];
+        const int64_t blk = S.row_ptr[k] + j;
+        const int32_t src = S.cols[blk];
+        block_gemv(slab + S.blk_off[blk], m, S.size[src], y + S.dof_off[src] * nrhs, part + j * m * nrhs, nrhs);
+        if (!last_ticket(tickets, p, nparts))
+            return;
+    }
+    fwd_finish(S, slab, y, part, nparts, k, nrhs, stage_diag, smem_raw);
+}
+
 // Backward stage: y_k -= sum_c U(k,c) y_c over the upper blocks of the stage's pivots
 // (block_system_solve_u, src/blocks.c:771-800). Units: trsm_pref, one per upper block.
 template <typename T, typename V>
@@ -1099,9 +1153,159 @@ __global__ void __launch_bounds__(kThreads)
     block_gemv(slab + S.blk_off[blk], m, S.size[c], y + S.dof_off[c] * nrhs, part + j * m * nrhs, nrhs);
     if (!last_ticket(tickets, p, nparts))
         return;
-    __shared__ V red[kThreads];
+    __shared__ __align__(16) V red[kThreads * 16 / sizeof(V)];
     V *yk = y + S.dof_off[k] * nrhs;
     subtract_partials(yk, part, nparts, m * nrhs, yk, red);
+}
+
+// ----------------------------------------------------------------------------------
+// Dataflow substitution: one cooperative launch per direction instead of one launch per
+// level. A work item is one partial product -- block (k, s) of a pivot's lower row
+// (forward) or (k, c) of its upper row (backward) against the source's final vector --
+// and pivots without such blocks get one empty item. Items are ordered by level (forward
+// ascending, backward descending) and CTA b takes items b, b + G, ... in order. Before its
+// product an item waits until the source block row's flag carries this solve's tag; the
+// CTA that takes a pivot's last ticket finishes it and sets the pivot's flag. Every wait
+// depends only on items earlier in the order and all CTAs are resident (cooperative
+// launch), so the waits end; each is also bounded in time (ST_TIMEOUT in `status`, after
+// which every wait returns at once). Source vectors are read from L2 (__ldcg): another
+// SM may have written them after this SM cached a neighbouring line.
+__device__ __forceinline__ int ld_acquire(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release(int *p, int v)
+{
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Waits (thread 0, bounded) until *flag == tag; CTA-uniform result.
+__device__ __forceinline__ bool wait_flag(const int *flag, int tag, int *status)
+{
+    __shared__ int s_ok;
+    if (threadIdx.x == 0)
+    {
+        int ok = 1;
+        if (ld_acquire(flag) != tag)
+        {
+            const uint64_t t0 = global_ns();
+            while (ld_acquire(flag) != tag)
+            {
+                if (schedule_aborted(status) || global_ns() - t0 > kWaitLimitNs)
+                {
+                    atomicOr(status + ST_TIMEOUT, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    const bool ok = s_ok != 0;
+    __syncthreads(); // s_ok is reused by the next wait
+    return ok;
+}
+
+// Marks block row k final for this solve (after every thread's writes of y_k).
+__device__ __forceinline__ void publish_flag(int *flag, int tag)
+{
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        __threadfence();
+        st_release(flag, tag);
+    }
+}
+
+// out = B y_src for one block (m x K), y read from L2.
+template <typename T, typename V>
+__device__ __forceinline__ void block_gemv_l2(const T *__restrict__ blk, int m, int K, const V *y, V *__restrict__ out,
+                                              int nrhs)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int i = warp; i < m; i += nw)
+    {
+        for (int r = 0; r < nrhs; ++r)
+        {
+            V s = 0;
+            for (int q = lane; q < K; q += 32)
+                s += (V)blk[(int64_t)i * K + q] * __ldcg(y + (int64_t)q * nrhs + r);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+                s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0)
+                out[(int64_t)i * nrhs + r] = s;
+        }
+    }
+}
+
+// Forward direction; partials of pivot slot p at scratch + fwd_rows[p] * nrhs.
+template <typename T, typename V>
+__global__ void __launch_bounds__(kThreads, 2)
+    k_fwd_flow(DevSym S, const T *__restrict__ slab, V *__restrict__ y, V *__restrict__ scratch,
+               int *__restrict__ tickets, int *__restrict__ flags, int tag, int64_t n_items, int nrhs, int stage_diag,
+               int *status)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    for (int64_t j = blockIdx.x; j < n_items; j += gridDim.x)
+    {
+        const int64_t p = S.fwd_item_p[j];
+        const int64_t k = S.piv[p];
+        const int m = S.size[k];
+        const int64_t nparts = S.diag_pos[k] - S.row_ptr[k];
+        V *part = scratch + S.fwd_rows[p] * nrhs;
+        if (nparts > 0)
+        {
+            const int64_t local = j - S.fwdu_pref[p];
+            const int64_t blk = S.row_ptr[k] + local;
+            const int32_t src = S.cols[blk];
+            if (!wait_flag(flags + src, tag, status))
+                return;
+            block_gemv_l2(slab + S.blk_off[blk], m, S.size[src], y + S.dof_off[src] * nrhs, part + local * m * nrhs,
+                          nrhs);
+            if (!last_ticket(tickets, p, nparts))
+                continue;
+        }
+        fwd_finish(S, slab, y, part, nparts, k, nrhs, stage_diag, smem_raw);
+        publish_flag(flags + k, tag);
+    }
+}
+
+// Backward direction; partials of pivot slot p at scratch + bwd_rows[p] * nrhs.
+template <typename T, typename V>
+__global__ void __launch_bounds__(kThreads)
+    k_bwd_flow(DevSym S, const T *__restrict__ slab, V *__restrict__ y, V *__restrict__ scratch,
+               int *__restrict__ tickets, int *__restrict__ flags, int tag, int64_t n_items, int nrhs, int *status)
+{
+    for (int64_t j = blockIdx.x; j < n_items; j += gridDim.x)
+    {
+        const int64_t p = S.bwd_item_p[j];
+        const int64_t k = S.piv[p];
+        const int m = S.size[k];
+        const int64_t nparts = S.row_ptr[k + 1] - S.diag_pos[k] - 1;
+        if (nparts > 0)
+        {
+            const int64_t local = j - S.bwd_first[p];
+            const int64_t blk = S.diag_pos[k] + 1 + local;
+            const int32_t c = S.cols[blk];
+            V *part = scratch + S.bwd_rows[p] * nrhs;
+            if (!wait_flag(flags + c, tag, status))
+                return;
+            block_gemv_l2(slab + S.blk_off[blk], m, S.size[c], y + S.dof_off[c] * nrhs, part + local * m * nrhs,
+                          nrhs);
+            if (!last_ticket(tickets, p, nparts))
+                continue;
+            __shared__ __align__(16) V red[kThreads * 16 / sizeof(V)];
+            V *yk = y + S.dof_off[k] * nrhs;
+            subtract_partials(yk, part, nparts, m * nrhs, yk, red);
+        }
+        publish_flag(flags + k, tag);
+    }
 }
 
 // ----------------------------------------------------------------------------------

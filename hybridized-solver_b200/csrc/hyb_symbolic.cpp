@@ -252,8 +252,10 @@ int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, co
         S.tc_pref[p + 1] = S.tc_pref[p] + n_lc * ((n_up + 1) / 2);
         S.fwd_pref[p + 1] = S.fwd_pref[p] + n_lr;
         S.fwdu_pref[p + 1] = S.fwdu_pref[p] + std::max<int64_t>(1, n_lr);
-        S.fwd_rows[p + 1] = S.fwd_rows[p] + n_lr * S.size[k];
-        S.bwd_rows[p + 1] = S.bwd_rows[p] + n_up * S.size[k];
+        // partial-product spans padded to 4 values, so every pivot's partials start on a
+        // 16-byte boundary in the staged (per-stage) and the dataflow (global) layouts alike
+        S.fwd_rows[p + 1] = S.fwd_rows[p] + (n_lr * S.size[k] + 3) / 4 * 4;
+        S.bwd_rows[p + 1] = S.bwd_rows[p] + (n_up * S.size[k] + 3) / 4 * 4;
         double up_cols = 0, lc_rows = 0;
         for (int64_t j = S.diag_pos[k] + 1; j < S.row_ptr[k + 1]; ++j)
             up_cols += S.size[S.cols[j]];
@@ -265,6 +267,24 @@ int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, co
         piv_upd_ab[p] = m * (lc_rows + up_cols);
     }
     S.factor_flops = flops;
+
+    // ---- Dataflow solve items: forward in pivot order, backward by levels descending.
+    S.fwd_item_p.resize(S.fwdu_pref[n]);
+    for (int64_t p = 0; p < n; ++p)
+        for (int64_t j = S.fwdu_pref[p]; j < S.fwdu_pref[p + 1]; ++j)
+            S.fwd_item_p[j] = (int32_t)p;
+    S.bwd_item_p.clear();
+    S.bwd_item_p.reserve(S.trsm_pref[n] + n);
+    S.bwd_first.assign(n, 0);
+    for (int64_t l = S.n_levels - 1; l >= 0; --l)
+        for (int64_t p = S.lvl_ptr[l]; p < S.lvl_ptr[l + 1]; ++p)
+        {
+            const int64_t k = S.piv[p];
+            const int64_t n_up = S.row_ptr[k + 1] - S.diag_pos[k] - 1;
+            S.bwd_first[p] = (int64_t)S.bwd_item_p.size();
+            for (int64_t j = 0; j < std::max<int64_t>(1, n_up); ++j)
+                S.bwd_item_p.push_back((int32_t)p);
+        }
 
     // ---- Level shapes, scratch spans and listed (conflicting) update levels.
     S.shape.assign(S.n_levels, {});

@@ -277,6 +277,10 @@ class NativeSystem:
     def set_tensor_core_mixed(self, enable: bool):
         _check(lib().hyb_system_set_option(self._h, 1, 1 if enable else 0), "hyb_system_set_option")
 
+    def set_dataflow_solve(self, enable: bool):
+        """Dataflow substitution (one cooperative launch per direction) or one launch per stage."""
+        _check(lib().hyb_system_set_option(self._h, 2, 1 if enable else 0), "hyb_system_set_option")
+
     @property
     def stream(self) -> int:
         return int(lib().hyb_system_stream(self._h) or 0)

@@ -155,7 +155,11 @@ typedef enum
     HYB_OPTION_LOOKAHEAD = 0,
     /* 1 (default): in the mixed form, the 64x64 Schur updates run on the tcgen05 tensor
      * cores as three BF16 products of a hi/lo split; 0: FP32 CUDA-core updates. */
-    HYB_OPTION_TENSOR_CORE_MIXED = 1
+    HYB_OPTION_TENSOR_CORE_MIXED = 1,
+    /* 1 (default): hyb_solve substitutes in one cooperative launch per direction, each
+     * pivot proceeding as soon as its sources are final; 0: one launch per elimination
+     * stage. Both give the same solution. */
+    HYB_OPTION_DATAFLOW_SOLVE = 2
 } hyb_option;
 
 /* Sets a schedule option of the handle (takes effect at the next decomposition). */

@@ -297,3 +297,27 @@ def test_dense_single_block_kernels(gpu):
         assert rel_err(lu, ref) < 1e-12
         b = rng.standard_normal((m, 70))
         assert rel_err(gpu.block_lu_solve(lu, b), O.lu_solve(ref, b)) < 1e-12
+
+
+@pytest.mark.parametrize(("n", "p", "nrhs"), [(12, 8, 1), (6, "rand", 3), (16, 4, 2)])
+@pytest.mark.parametrize("prec", [0, 1])
+def test_dataflow_solve_matches_staged(gpu, n, p, nrhs, prec):
+    """The dataflow substitution (one cooperative launch per direction, pivots released by
+    flags) forms the same partial products in the same order as the staged one, so the
+    solutions agree bit for bit; both match the oracle."""
+    from hybsol.b200 import meshgen
+
+    pp = meshgen.random_orders(n, 2, 10, seed=5) if p == "rand" else p
+    mat, b = _mesh(n, pp, seed=21, nrhs=nrhs)
+    order, pm, ns = _native_from(gpu, mat)
+    bn = reorder_rhs(mat.sizes, order, b)
+    ns.decompose(prec)
+    x_flow, info_f = ns.solve(bn)
+    x_flow2, _ = ns.solve(bn)  # flags and tickets carry over between solves
+    ns.set_dataflow_solve(False)
+    x_staged, info_s = ns.solve(bn)
+    assert np.array_equal(x_flow, x_staged) and np.array_equal(x_flow, x_flow2)
+    assert info_f["iterations"] == info_s["iterations"]
+    osys = O.OracleSystem.from_csr(pm.sizes, pm.row_ptr, pm.cols, pm.vals)
+    osys.decompose()
+    assert rel_err(x_flow, osys.solve(bn)) < (TOL_X if prec == 0 else TOL_X_MIXED)
