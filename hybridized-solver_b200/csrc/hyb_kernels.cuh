@@ -845,22 +845,35 @@ __global__ void __launch_bounds__(kThreads) k_update_listed(DevSym S, T *__restr
 //
 // Partial products of one block against the vector: out[i][r] = sum_q blk[i][q] * y[q][r]
 // for an m x K block; one warp per output row.
-template <typename T, typename V>
-__device__ __forceinline__ void block_gemv(const T *__restrict__ blk, int m, int K, const V *__restrict__ y,
-                                           V *__restrict__ out, int nrhs)
+// out = B y for one m x K block B (row-major) of the factors: every row is split over a
+// group of tpr consecutive threads (the largest power of two, at most 32, with 2 tpr m >
+// blockDim), each summing every tpr-th column, so all of the CTA's loads are in flight at
+// once; the group's sums are combined by an xor butterfly. With kL2, y is read from L2.
+template <bool kL2 = false, typename T, typename V>
+__device__ __forceinline__ void block_gemv(const T *__restrict__ blk, int m, int K, const V *y, V *__restrict__ out,
+                                           int nrhs)
 {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int i = warp; i < m; i += nw)
+    const int nt = blockDim.x;
+    int tpr = 1;
+    while (tpr < 32 && 2 * tpr * m <= nt)
+        tpr *= 2;
+    const int q = threadIdx.x & (tpr - 1), rl = threadIdx.x / tpr, rows = nt / tpr;
+    for (int r0 = 0; r0 < m; r0 += rows)
     {
+        const int i = r0 + rl;
         for (int r = 0; r < nrhs; ++r)
         {
             V s = 0;
-            for (int q = lane; q < K; q += 32)
-                s += (V)blk[(int64_t)i * K + q] * y[(int64_t)q * nrhs + r];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
+            if (i < m)
+            {
+                const T *row = blk + (int64_t)i * K;
+#pragma unroll 8
+                for (int c = q; c < K; c += tpr)
+                    s += (V)row[c] * (kL2 ? __ldcg(y + (int64_t)c * nrhs + r) : y[(int64_t)c * nrhs + r]);
+            }
+            for (int o = tpr >> 1; o > 0; o >>= 1)
                 s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0)
+            if (q == 0 && i < m)
                 out[(int64_t)i * nrhs + r] = s;
         }
     }
@@ -1111,7 +1124,7 @@ __device__ void fwd_finish(const DevSym &S, const T *__restrict__ slab, V *__res
 // (block_system_apply_operations, src/blocks.c:729-769). Units: fwdu_pref, one per lower
 // block of a pivot (at least one per pivot).
 template <typename T, typename V>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
     k_fwd_stage(DevSym S, const T *__restrict__ slab, V *__restrict__ y, V *__restrict__ scratch,
                 int *__restrict__ tickets, int64_t p0, int64_t p1, int nrhs, int stage_diag)
 {
@@ -1137,7 +1150,7 @@ __global__ void __launch_bounds__(kThreads)
 // Backward stage: y_k -= sum_c U(k,c) y_c over the upper blocks of the stage's pivots
 // (block_system_solve_u, src/blocks.c:771-800). Units: trsm_pref, one per upper block.
 template <typename T, typename V>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
     k_bwd_stage(DevSym S, const T *__restrict__ slab, V *__restrict__ y, V *__restrict__ scratch,
                 int *__restrict__ tickets, int64_t p0, int64_t p1, int nrhs)
 {
@@ -1222,27 +1235,6 @@ __device__ __forceinline__ void publish_flag(int *flag, int tag)
     }
 }
 
-// out = B y_src for one block (m x K), y read from L2.
-template <typename T, typename V>
-__device__ __forceinline__ void block_gemv_l2(const T *__restrict__ blk, int m, int K, const V *y, V *__restrict__ out,
-                                              int nrhs)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int i = warp; i < m; i += nw)
-    {
-        for (int r = 0; r < nrhs; ++r)
-        {
-            V s = 0;
-            for (int q = lane; q < K; q += 32)
-                s += (V)blk[(int64_t)i * K + q] * __ldcg(y + (int64_t)q * nrhs + r);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
-                s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0)
-                out[(int64_t)i * nrhs + r] = s;
-        }
-    }
-}
 
 // Forward direction; partials of pivot slot p at scratch + fwd_rows[p] * nrhs.
 template <typename T, typename V>
@@ -1266,7 +1258,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             const int32_t src = S.cols[blk];
             if (!wait_flag(flags + src, tag, status))
                 return;
-            block_gemv_l2(slab + S.blk_off[blk], m, S.size[src], y + S.dof_off[src] * nrhs, part + local * m * nrhs,
+            block_gemv<true>(slab + S.blk_off[blk], m, S.size[src], y + S.dof_off[src] * nrhs, part + local * m * nrhs,
                           nrhs);
             if (!last_ticket(tickets, p, nparts))
                 continue;
@@ -1278,7 +1270,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 
 // Backward direction; partials of pivot slot p at scratch + bwd_rows[p] * nrhs.
 template <typename T, typename V>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
     k_bwd_flow(DevSym S, const T *__restrict__ slab, V *__restrict__ y, V *__restrict__ scratch,
                int *__restrict__ tickets, int *__restrict__ flags, int tag, int64_t n_items, int nrhs, int *status)
 {
@@ -1296,7 +1288,7 @@ __global__ void __launch_bounds__(kThreads)
             V *part = scratch + S.bwd_rows[p] * nrhs;
             if (!wait_flag(flags + c, tag, status))
                 return;
-            block_gemv_l2(slab + S.blk_off[blk], m, S.size[c], y + S.dof_off[c] * nrhs, part + local * m * nrhs,
+            block_gemv<true>(slab + S.blk_off[blk], m, S.size[c], y + S.dof_off[c] * nrhs, part + local * m * nrhs,
                           nrhs);
             if (!last_ticket(tickets, p, nparts))
                 continue;
