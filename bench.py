@@ -63,6 +63,7 @@ def parse_args():
         action="store_true",
         help="one decompose + solve per form and nothing else (the command ncu captures run)",
     )
+    ap.add_argument("--form", choices=["both", "fp64", "mixed"], default="both", help="forms --single runs")
     return ap.parse_args()
 
 
@@ -74,7 +75,8 @@ def run_single(args):
 
     pm, bn = build_workload(args.mesh, args.p)
     ns = native.NativeSystem.from_matrix(pm)
-    for prec in (native.FP64, native.MIXED):
+    forms = {"both": (native.FP64, native.MIXED), "fp64": (native.FP64,), "mixed": (native.MIXED,)}[args.form]
+    for prec in forms:
         ns.set_values(pm.vals)
         ns.decompose(prec)
         x, info = ns.solve(bn)
@@ -448,16 +450,19 @@ def run_ours(args):
     barrier()
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps)
 
-    def roofline(prof, bound, peak, unit, elem_bytes, peak_note, step_ms):
+    def roofline(prof, bound, peak, unit, elem_bytes, peak_note, step_ms, kernel):
+        """One level's Schur update (both lookahead launches, timed with events on the
+        handle's stream) against its bound; algorithmic work per level from the pattern:
+        2 m k n flops per target block, and the FP32/FP64 bytes of reading and writing every
+        target once plus reading the lower-column and upper-row operands once."""
         if prof is None:
             return None
         avg_ms = prof.total_ms / prof.launches
-        if bound == "tensor":
-            per_launch = prof.flops / prof.launches
-            achieved = per_launch / (avg_ms * 1e-3) / 1e12
-        else:
-            per_launch = elem_bytes * (2 * prof.c_elems + prof.ab_elems) / prof.launches
-            achieved = per_launch / (avg_ms * 1e-3) / 1e9
+        flops_per = prof.flops / prof.launches
+        bytes_per = elem_bytes * (2 * prof.c_elems + prof.ab_elems) / prof.launches
+        tflops = flops_per / (avg_ms * 1e-3) / 1e12
+        gbs = bytes_per / (avg_ms * 1e-3) / 1e9
+        achieved, per_launch = (tflops, flops_per) if bound == "tensor" else (gbs, bytes_per)
         return {
             "bound": bound,
             "achieved": achieved,
@@ -465,18 +470,32 @@ def run_ours(args):
             "unit": unit,
             "frac": achieved / peak,
             "traffic": None,
-            "kernel": "Schur-complement update (k_update64_f64 / k_update)",
+            "kernel": kernel,
             "launches": prof.launches,
             "avg_launch_ms": avg_ms,
             "share_of_step": prof.total_ms / step_ms,
             "peak_source": peak_note,
             "algorithmic_per_launch": per_launch,
+            "algorithmic_unit": "flop" if bound == "tensor" else "byte",
+            "tflops_fp_equivalent": tflops,
+            "gbs_algorithmic": gbs,
         }
 
-    rf64 = roofline(fp64_prof, "tensor", fp64_peak, "TFLOP/s", 8, "cuBLAS DGEMM 8192^3 measured in this run", fp64_ms)
-    rmix = roofline(
-        mixed_prof, "tensor", fp32_peak, "TFLOP/s", 4, "cuBLAS SGEMM 8192^3 measured in this run", mixed_ms
+    rf64 = roofline(
+        fp64_prof, "tensor", fp64_peak, "TFLOP/s", 8, "cuBLAS DGEMM 8192^3 measured in this run (FP64 DMMA)",
+        fp64_ms, "k_update64_f64 (FP64 DMMA m8n8k4, bulk-copy staged operands)",
     )
+    hbm = float(peaks.get("hbm_gbs") or 6650.0)
+    rmix = roofline(
+        mixed_prof, "hbm", hbm, "GB/s", 4,
+        f"MEASURED_PEAKS.json hbm_gbs ({peak_src})", mixed_ms,
+        "k_update64_tc (tcgen05 split-BF16, persistent, bulk-copy C ring)",
+    )
+    if rmix is not None:
+        # three BF16 MMAs per FP32 product on the tensor cores, against the sustained peak
+        bf16 = float(peaks.get("bf16_tflops_sustained") or 1390.5)
+        rmix["tensor_bf16_tflops"] = 3 * rmix["tflops_fp_equivalent"]
+        rmix["tensor_bf16_frac_of_sustained"] = 3 * rmix["tflops_fp_equivalent"] / bf16
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
