@@ -88,6 +88,12 @@ template <typename K> cudaError_t allow_smem(K kernel, int bytes)
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  std::min<int>(bytes, smem_optin() - (int)fa.sharedSizeBytes));
+    // The SM's L1/shared split is fixed while a CTA is resident: with every kernel of the
+    // factorization preferring the largest shared carveout, the next pivot's CTAs fit
+    // beside a running update CTA instead of waiting for it to finish.
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
     cudaGetLastError();
     return e;
 }
@@ -1027,6 +1033,9 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
             allow_smem(hyb::k_lu_trsm64<double>, hyb::lu_trsm64_smem<double>()),
             allow_smem(hyb::k_lu_trsm64<float>, hyb::lu_trsm64_smem<float>()),
             allow_smem(hyb::k_update64_tc, hyb::kTcSmem),
+            allow_smem(hyb::k_split64, 0),
+            allow_smem(hyb::k_update<double>, 0),
+            allow_smem(hyb::k_update<float>, 0),
         };
         for (cudaError_t e : errs)
             if (e != cudaSuccess)
