@@ -1084,10 +1084,24 @@ __device__ void fwd_finish(const DevSym &S, const T *__restrict__ slab, V *__res
     __shared__ __align__(16) V red[kThreads * 16 / sizeof(V)];
     V *acc = reinterpret_cast<V *>(smem_raw); // m * nrhs
     V *yk = y + S.dof_off[k] * nrhs;
-    subtract_partials(yk, part, nparts, m * nrhs, acc, red);
     // The diagonal block goes to shared memory with an odd row stride (column reads of the
-    // substitution hit distinct banks) when it fits next to the accumulator.
+    // substitution hit distinct banks) when it fits next to the accumulator. Its first
+    // kStageRegs x blockDim values are loaded into registers before the partial products
+    // are summed, so the two memory latencies overlap.
+    constexpr int kStageRegs = 16;
     const T *gd = slab + S.blk_off[S.diag_pos[k]];
+    const int mm = m * m, nt = blockDim.x, tid = threadIdx.x;
+    T dv[kStageRegs];
+    if (stage_diag)
+    {
+#pragma unroll
+        for (int q = 0; q < kStageRegs; ++q)
+        {
+            const int i = q * nt + tid;
+            dv[q] = i < mm ? gd[i] : T(0);
+        }
+    }
+    subtract_partials(yk, part, nparts, m * nrhs, acc, red);
     const T *d = gd;
     int ldd = m;
     const size_t acc_bytes = ((size_t)m * nrhs * sizeof(V) + 15) / 16 * 16;
@@ -1095,7 +1109,14 @@ __device__ void fwd_finish(const DevSym &S, const T *__restrict__ slab, V *__res
     {
         T *sd = reinterpret_cast<T *>(smem_raw + acc_bytes);
         ldd = m | 1;
-        for (int i = threadIdx.x; i < m * m; i += blockDim.x)
+#pragma unroll
+        for (int q = 0; q < kStageRegs; ++q)
+        {
+            const int i = q * nt + tid;
+            if (i < mm)
+                sd[(i / m) * ldd + i % m] = dv[q];
+        }
+        for (int i = kStageRegs * nt + tid; i < mm; i += nt)
             sd[(i / m) * ldd + i % m] = gd[i];
         d = sd;
     }
@@ -1236,9 +1257,78 @@ __device__ __forceinline__ void publish_flag(int *flag, int tag)
 }
 
 
+// A block's share of the row-group product (block_gemv's mapping) held in registers, so
+// it can be loaded before the wait for the vector it multiplies. Used when one pass covers
+// the block and a thread's share fits (kGemvRegs values); otherwise `ok` is false.
+constexpr int kGemvRegs = 16;
+template <typename T> struct GemvRegs
+{
+    T v[kGemvRegs];
+    bool ok;
+};
+
+template <typename T> __device__ __forceinline__ int gemv_tpr(int m)
+{
+    int tpr = 1;
+    while (tpr < 32 && 2 * tpr * m <= (int)blockDim.x)
+        tpr *= 2;
+    return tpr;
+}
+
+template <typename T> __device__ __forceinline__ void gemv_load(GemvRegs<T> &g, const T *__restrict__ blk, int m, int K)
+{
+    const int tpr = gemv_tpr<T>(m), rows = blockDim.x / tpr;
+    const int q = threadIdx.x & (tpr - 1), i = threadIdx.x / tpr;
+    g.ok = rows >= m && (K + tpr - 1) / tpr <= kGemvRegs;
+    if (!g.ok)
+        return;
+#pragma unroll
+    for (int c = 0; c < kGemvRegs; ++c)
+    {
+        const int col = q + c * tpr;
+        g.v[c] = (i < m && col < K) ? blk[(int64_t)i * K + col] : T(0);
+    }
+}
+
+// out = B y with B's share in registers; the same products and order as block_gemv<true>.
+template <typename T, typename V>
+__device__ __forceinline__ void gemv_finish(const GemvRegs<T> &g, int m, int K, const V *y, V *__restrict__ out,
+                                            int nrhs)
+{
+    const int tpr = gemv_tpr<T>(m);
+    const int q = threadIdx.x & (tpr - 1), i = threadIdx.x / tpr;
+    for (int r = 0; r < nrhs; ++r)
+    {
+        V s = 0;
+        if (i < m)
+        {
+#pragma unroll
+            for (int c = 0; c < kGemvRegs; ++c)
+            {
+                const int col = q + c * tpr;
+                if (col < K)
+                    s += (V)g.v[c] * __ldcg(y + (int64_t)col * nrhs + r);
+            }
+        }
+        for (int o = tpr >> 1; o > 0; o >>= 1)
+            s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (q == 0 && i < m)
+            out[(int64_t)i * nrhs + r] = s;
+    }
+}
+
+// Pulls a block into L2 ahead of its use (one 128-byte line per thread and step).
+template <typename T> __device__ __forceinline__ void prefetch_l2(const T *p, int64_t elems)
+{
+    const char *c = reinterpret_cast<const char *>(p);
+    const int64_t bytes = elems * (int64_t)sizeof(T);
+    for (int64_t off = (int64_t)threadIdx.x * 128; off < bytes; off += (int64_t)blockDim.x * 128)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(c + off));
+}
+
 // Forward direction; partials of pivot slot p at scratch + fwd_rows[p] * nrhs.
 template <typename T, typename V>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 8 ? 1 : 2)
     k_fwd_flow(DevSym S, const T *__restrict__ slab, V *__restrict__ y, V *__restrict__ scratch,
                int *__restrict__ tickets, int *__restrict__ flags, int tag, int64_t n_items, int nrhs, int stage_diag,
                int *status)
@@ -1256,10 +1346,18 @@ __global__ void __launch_bounds__(kThreads, 2)
             const int64_t local = j - S.fwdu_pref[p];
             const int64_t blk = S.row_ptr[k] + local;
             const int32_t src = S.cols[blk];
+            const int K = S.size[src];
+            if (local == 0 && stage_diag) // the finisher will stage D_k: bring it into L2 now
+                prefetch_l2(slab + S.blk_off[S.diag_pos[k]], (int64_t)m * m);
+            GemvRegs<T> g;
+            gemv_load(g, slab + S.blk_off[blk], m, K);
             if (!wait_flag(flags + src, tag, status))
                 return;
-            block_gemv<true>(slab + S.blk_off[blk], m, S.size[src], y + S.dof_off[src] * nrhs, part + local * m * nrhs,
-                          nrhs);
+            if (g.ok)
+                gemv_finish(g, m, K, y + S.dof_off[src] * nrhs, part + local * m * nrhs, nrhs);
+            else
+                block_gemv<true>(slab + S.blk_off[blk], m, K, y + S.dof_off[src] * nrhs, part + local * m * nrhs,
+                                 nrhs);
             if (!last_ticket(tickets, p, nparts))
                 continue;
         }
@@ -1285,11 +1383,16 @@ __global__ void __launch_bounds__(kThreads, 2)
             const int64_t local = j - S.bwd_first[p];
             const int64_t blk = S.diag_pos[k] + 1 + local;
             const int32_t c = S.cols[blk];
+            const int K = S.size[c];
             V *part = scratch + S.bwd_rows[p] * nrhs;
+            GemvRegs<T> g;
+            gemv_load(g, slab + S.blk_off[blk], m, K);
             if (!wait_flag(flags + c, tag, status))
                 return;
-            block_gemv<true>(slab + S.blk_off[blk], m, S.size[c], y + S.dof_off[c] * nrhs, part + local * m * nrhs,
-                          nrhs);
+            if (g.ok)
+                gemv_finish(g, m, K, y + S.dof_off[c] * nrhs, part + local * m * nrhs, nrhs);
+            else
+                block_gemv<true>(slab + S.blk_off[blk], m, K, y + S.dof_off[c] * nrhs, part + local * m * nrhs, nrhs);
             if (!last_ticket(tickets, p, nparts))
                 continue;
             __shared__ __align__(16) V red[kThreads * 16 / sizeof(V)];
