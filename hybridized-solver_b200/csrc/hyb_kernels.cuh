@@ -904,10 +904,158 @@ __device__ __forceinline__ bool last_ticket(int *tickets, int64_t p, int64_t npa
 // Substitution with a factored diagonal block D (unit L below, U on and above the
 // diagonal; row stride ldd) for column r of acc (m x nrhs, shared memory), by one warp:
 // x <- U^{-1} L^{-1} x, as matrix_lu_solve (src/blocks.c:285-316) in right-looking order.
-// The vector stays in registers -- lane l holds rows l + 32 t, t < R -- and step i
-// broadcasts x_i with a shuffle, so a step costs one shuffle and R fused multiply-adds.
+// The vector stays in registers -- lane l holds rows l + 32 t, t < R. Pivots are taken
+// four per round: their four current values are shuffled at once, every lane finishes the
+// 4x4 triangle with broadcast coefficients, then applies the four updates to the rows it
+// holds, so a round costs one shuffle latency for four pivots. Each row sees the same
+// fused multiply-adds in the same order as with one pivot per round, and registers wholly
+// before (after) the round's 32-row group take no (unmasked) updates.
 template <int R, typename T, typename V>
 __device__ __forceinline__ void warp_lu_solve(const T *d, int ldd, int m, V *acc, int r, int nrhs)
+{
+    const int lane = threadIdx.x & 31;
+    V x[R], rcp[R];
+    int rr[R];
+#pragma unroll
+    for (int t = 0; t < R; ++t)
+    {
+        const int row = lane + 32 * t;
+        rr[t] = min(row, m - 1);
+        x[t] = row < m ? acc[rr[t] * nrhs + r] : V(0);
+        rcp[t] = V(1) / (V)d[(int64_t)rr[t] * ldd + rr[t]];
+    }
+    // ---- forward, unit lower
+#pragma unroll
+    for (int tb = 0; tb < R; ++tb)
+    {
+        const int n_i = min(32, m - 32 * tb);
+        int il = 0;
+        for (; il + 4 <= n_i; il += 4)
+        {
+            const int i = 32 * tb + il;
+            V c[R][4];
+#pragma unroll
+            for (int t = 0; t < R; ++t)
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    c[t][q] = t >= tb ? (V)d[(int64_t)rr[t] * ldd + i + q] : V(0);
+            const V l10 = (V)d[(int64_t)(i + 1) * ldd + i], l20 = (V)d[(int64_t)(i + 2) * ldd + i];
+            const V l21 = (V)d[(int64_t)(i + 2) * ldd + i + 1], l30 = (V)d[(int64_t)(i + 3) * ldd + i];
+            const V l31 = (V)d[(int64_t)(i + 3) * ldd + i + 1], l32 = (V)d[(int64_t)(i + 3) * ldd + i + 2];
+            V a0 = __shfl_sync(0xffffffffu, x[tb], il), a1 = __shfl_sync(0xffffffffu, x[tb], il + 1);
+            V a2 = __shfl_sync(0xffffffffu, x[tb], il + 2), a3 = __shfl_sync(0xffffffffu, x[tb], il + 3);
+            a1 -= l10 * a0;
+            a2 -= l20 * a0;
+            a2 -= l21 * a1;
+            a3 -= l30 * a0;
+            a3 -= l31 * a1;
+            a3 -= l32 * a2;
+            const V av[4] = {a0, a1, a2, a3};
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int t = 0; t < R; ++t)
+                {
+                    if (t < tb)
+                        continue;
+                    if (t == tb)
+                        x[t] -= (lane > il + q ? c[t][q] : V(0)) * av[q];
+                    else
+                        x[t] -= (lane + 32 * t < m ? c[t][q] : V(0)) * av[q];
+                }
+        }
+        for (; il < n_i; ++il)
+        {
+            const int i = 32 * tb + il;
+            const V xi = __shfl_sync(0xffffffffu, x[tb], il);
+#pragma unroll
+            for (int t = 0; t < R; ++t)
+            {
+                const int row = lane + 32 * t;
+                const V c = (V)d[(int64_t)rr[t] * ldd + i];
+                x[t] -= (row > i && row < m ? c : V(0)) * xi;
+            }
+        }
+    }
+    // ---- backward, upper with the diagonal
+#pragma unroll
+    for (int tb = R - 1; tb >= 0; --tb)
+    {
+        const int n_i = min(32, m - 32 * tb);
+        int il = n_i - 1;
+        for (; il >= 3; il -= 4)
+        {
+            const int i = 32 * tb + il;
+            V c[R][4];
+#pragma unroll
+            for (int t = 0; t < R; ++t)
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    c[t][q] = t <= tb ? (V)d[(int64_t)rr[t] * ldd + i - q] : V(0);
+            const V u10 = (V)d[(int64_t)(i - 1) * ldd + i], u20 = (V)d[(int64_t)(i - 2) * ldd + i];
+            const V u21 = (V)d[(int64_t)(i - 2) * ldd + i - 1], u30 = (V)d[(int64_t)(i - 3) * ldd + i];
+            const V u31 = (V)d[(int64_t)(i - 3) * ldd + i - 1], u32 = (V)d[(int64_t)(i - 3) * ldd + i - 2];
+            const V r0 = __shfl_sync(0xffffffffu, rcp[tb], il), r1 = __shfl_sync(0xffffffffu, rcp[tb], il - 1);
+            const V r2 = __shfl_sync(0xffffffffu, rcp[tb], il - 2), r3 = __shfl_sync(0xffffffffu, rcp[tb], il - 3);
+            V a0 = __shfl_sync(0xffffffffu, x[tb], il), a1 = __shfl_sync(0xffffffffu, x[tb], il - 1);
+            V a2 = __shfl_sync(0xffffffffu, x[tb], il - 2), a3 = __shfl_sync(0xffffffffu, x[tb], il - 3);
+            const V f0 = a0 * r0;
+            a1 -= u10 * f0;
+            const V f1 = a1 * r1;
+            a2 -= u20 * f0;
+            a2 -= u21 * f1;
+            const V f2 = a2 * r2;
+            a3 -= u30 * f0;
+            a3 -= u31 * f1;
+            a3 -= u32 * f2;
+            const V f3 = a3 * r3;
+            const V fv[4] = {f0, f1, f2, f3};
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int t = 0; t < R; ++t)
+                {
+                    if (t > tb)
+                        continue;
+                    if (t == tb)
+                        x[t] -= (lane < il - q ? c[t][q] : V(0)) * fv[q];
+                    else
+                        x[t] -= c[t][q] * fv[q];
+                }
+            x[tb] = lane == il ? f0 : x[tb];
+            x[tb] = lane == il - 1 ? f1 : x[tb];
+            x[tb] = lane == il - 2 ? f2 : x[tb];
+            x[tb] = lane == il - 3 ? f3 : x[tb];
+        }
+        for (; il >= 0; --il)
+        {
+            const int i = 32 * tb + il;
+            const V xi = __shfl_sync(0xffffffffu, x[tb] * rcp[tb], il);
+            if (lane == il)
+                x[tb] = xi;
+#pragma unroll
+            for (int t = 0; t < R; ++t)
+            {
+                const int row = lane + 32 * t;
+                const V c = (V)d[(int64_t)rr[t] * ldd + i];
+                x[t] -= (row < i ? c : V(0)) * xi;
+            }
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < R; ++t)
+    {
+        const int row = lane + 32 * t;
+        if (row < m)
+            acc[row * nrhs + r] = x[t];
+    }
+}
+
+// One pivot per round (blocks of 65 to 128 rows, where four-pivot rounds would need more
+// registers than the kernels have): step i broadcasts x_i, each step's coefficients are
+// loaded one step ahead.
+template <int R, typename T, typename V>
+__device__ __forceinline__ void warp_lu_solve1(const T *d, int ldd, int m, V *acc, int r, int nrhs)
 {
     const int lane = threadIdx.x & 31;
     V x[R], rcp[R];
@@ -1109,12 +1257,26 @@ __device__ void fwd_finish(const DevSym &S, const T *__restrict__ slab, V *__res
     {
         T *sd = reinterpret_cast<T *>(smem_raw + acc_bytes);
         ldd = m | 1;
-#pragma unroll
-        for (int q = 0; q < kStageRegs; ++q)
+        if ((m & (m - 1)) == 0)
         {
-            const int i = q * nt + tid;
-            if (i < mm)
-                sd[(i / m) * ldd + i % m] = dv[q];
+            const int sh = __ffs(m) - 1;
+#pragma unroll
+            for (int q = 0; q < kStageRegs; ++q)
+            {
+                const int i = q * nt + tid;
+                if (i < mm)
+                    sd[(i >> sh) * ldd + (i & (m - 1))] = dv[q];
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int q = 0; q < kStageRegs; ++q)
+            {
+                const int i = q * nt + tid;
+                if (i < mm)
+                    sd[(i / m) * ldd + i % m] = dv[q];
+            }
         }
         for (int i = kStageRegs * nt + tid; i < mm; i += nt)
             sd[(i / m) * ldd + i % m] = gd[i];
@@ -1130,9 +1292,9 @@ __device__ void fwd_finish(const DevSym &S, const T *__restrict__ slab, V *__res
         else if (m <= 64)
             warp_lu_solve<2>(d, ldd, m, acc, r, nrhs);
         else if (m <= 96)
-            warp_lu_solve<3>(d, ldd, m, acc, r, nrhs);
+            warp_lu_solve1<3>(d, ldd, m, acc, r, nrhs);
         else if (m <= 128)
-            warp_lu_solve<4>(d, ldd, m, acc, r, nrhs);
+            warp_lu_solve1<4>(d, ldd, m, acc, r, nrhs);
         else
             warp_lu_solve_smem(d, ldd, m, acc, r, nrhs);
     }
@@ -1145,7 +1307,7 @@ __device__ void fwd_finish(const DevSym &S, const T *__restrict__ slab, V *__res
 // (block_system_apply_operations, src/blocks.c:729-769). Units: fwdu_pref, one per lower
 // block of a pivot (at least one per pivot).
 template <typename T, typename V>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, 1)
     k_fwd_stage(DevSym S, const T *__restrict__ slab, V *__restrict__ y, V *__restrict__ scratch,
                 int *__restrict__ tickets, int64_t p0, int64_t p1, int nrhs, int stage_diag)
 {
@@ -1328,7 +1490,7 @@ template <typename T> __device__ __forceinline__ void prefetch_l2(const T *p, in
 
 // Forward direction; partials of pivot slot p at scratch + fwd_rows[p] * nrhs.
 template <typename T, typename V>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 8 ? 1 : 2)
+__global__ void __launch_bounds__(kThreads, 1)
     k_fwd_flow(DevSym S, const T *__restrict__ slab, V *__restrict__ y, V *__restrict__ scratch,
                int *__restrict__ tickets, int *__restrict__ flags, int tag, int64_t n_items, int nrhs, int stage_diag,
                int *status)
