@@ -140,6 +140,7 @@ struct hyb_system
     // dataflow solve: per block row the tag of the last solve direction that finished it,
     // the solve's status words, and the partial products of every pivot (flow_nrhs columns)
     int *d_flags = nullptr;
+    int *d_pflags = nullptr; // per pivot: tag of the solve direction whose early partials are summed
     int *d_solve_status = nullptr;
     uint32_t solve_epoch = 0;
     double *d_flow64 = nullptr;
@@ -180,6 +181,7 @@ struct hyb_system
         cudaFree(d_status);
         cudaFree(d_tickets);
         cudaFree(d_flags);
+        cudaFree(d_pflags);
         cudaFree(d_solve_status);
         cudaFree(d_flow64);
         cudaFree(d_flow32);
@@ -598,7 +600,8 @@ template <typename T, typename V> int enqueue_solve_flow(hyb_system *h, const T 
     HYB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
     HYB_CUDA(cudaFuncSetAttribute(hyb::k_fwd_flow<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, fwd_smem));
     HYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, hyb::k_fwd_flow<T, V>, hyb::kThreads, fwd_smem));
-    HYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_b, hyb::k_bwd_flow<T, V>, hyb::kThreads, 0));
+    HYB_CUDA(cudaFuncSetAttribute(hyb::k_bwd_flow<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, acc_bytes));
+    HYB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_b, hyb::k_bwd_flow<T, V>, hyb::kThreads, acc_bytes));
     if (!coop || per_sm_f < 1 || per_sm_b < 1)
         return HYB_TOO_LARGE;
     V *&scr = flow_scratch<V>(h);
@@ -619,20 +622,20 @@ template <typename T, typename V> int enqueue_solve_flow(hyb_system *h, const T 
     int tag_f = (int)(2 * h->solve_epoch + 1), tag_b = tag_f + 1;
     DevSym ds = h->ds;
     V *scratch = scr;
-    int *tickets = h->d_tickets, *flags = h->d_flags, *status = h->d_solve_status;
+    int *tickets = h->d_tickets, *flags = h->d_flags, *pflags = h->d_pflags, *status = h->d_solve_status;
     int64_t nf = (int64_t)S.fwd_item_p.size(), nb = (int64_t)S.bwd_item_p.size();
     const int sms = sm_count();
     {
         const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nf, (int64_t)per_sm_f * sms));
-        void *args[] = {&ds, (void *)&slab, &y, &scratch, &tickets, &flags, &tag_f, &nf, &nrhs, &stage, &status};
+        void *args[] = {&ds, (void *)&slab, &y, &scratch, &tickets, &flags, &pflags, &tag_f, &nf, &nrhs, &stage, &status};
         HYB_CUDA(cudaLaunchCooperativeKernel((const void *)hyb::k_fwd_flow<T, V>, dim3(grid), dim3(hyb::kThreads),
                                              args, fwd_smem, st));
     }
     {
         const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nb, (int64_t)per_sm_b * sms));
-        void *args[] = {&ds, (void *)&slab, &y, &scratch, &tickets, &flags, &tag_b, &nb, &nrhs, &status};
+        void *args[] = {&ds, (void *)&slab, &y, &scratch, &tickets, &flags, &pflags, &tag_b, &nb, &nrhs, &status};
         HYB_CUDA(cudaLaunchCooperativeKernel((const void *)hyb::k_bwd_flow<T, V>, dim3(grid), dim3(hyb::kThreads),
-                                             args, 0, st));
+                                             args, acc_bytes, st));
     }
     launches += 2;
     return HYB_SUCCESS;
@@ -887,6 +890,8 @@ HYB_API int hyb_system_create(uint64_t n, const uint64_t *block_sizes, const uin
     HYB_CUDA(cudaMalloc(&h->d_tickets, h->S.n * sizeof(int)));
     HYB_CUDA(cudaMalloc(&h->d_flags, h->S.n * sizeof(int)));
     HYB_CUDA(cudaMemsetAsync(h->d_flags, 0, h->S.n * sizeof(int), h->stream));
+    HYB_CUDA(cudaMalloc(&h->d_pflags, h->S.n * sizeof(int)));
+    HYB_CUDA(cudaMemsetAsync(h->d_pflags, 0, h->S.n * sizeof(int), h->stream));
     HYB_CUDA(cudaMalloc(&h->d_solve_status, hyb::ST_WORDS * sizeof(int)));
     HYB_CUDA(cudaMemsetAsync(h->d_tickets, 0, h->S.n * sizeof(int), h->stream));
     HYB_CUDA(cudaStreamSynchronize(h->stream));
@@ -932,6 +937,8 @@ HYB_API int hyb_system_copy(const hyb_system *src, hyb_system **out)
     HYB_CUDA(cudaMalloc(&h->d_tickets, h->S.n * sizeof(int)));
     HYB_CUDA(cudaMalloc(&h->d_flags, h->S.n * sizeof(int)));
     HYB_CUDA(cudaMemsetAsync(h->d_flags, 0, h->S.n * sizeof(int), h->stream));
+    HYB_CUDA(cudaMalloc(&h->d_pflags, h->S.n * sizeof(int)));
+    HYB_CUDA(cudaMemsetAsync(h->d_pflags, 0, h->S.n * sizeof(int), h->stream));
     HYB_CUDA(cudaMalloc(&h->d_solve_status, hyb::ST_WORDS * sizeof(int)));
     HYB_CUDA(cudaMemsetAsync(h->d_tickets, 0, h->S.n * sizeof(int), h->stream));
     HYB_CUDA(cudaStreamSynchronize(src->stream));

@@ -1138,11 +1138,10 @@ __device__ void warp_lu_solve_smem(const T *d, int ldd, int m, V *acc, int r, in
     }
 }
 
-// out[e] = y[e] - sum_j part[j][e] for e < E (E = rows x right-hand sides), with every
-// thread of the CTA busy: the E values are read as 16-byte vectors when aligned, G =
-// blockDim / (vectors per partial) groups each sum every G-th partial with eight loads in
-// flight, then the group sums are subtracted in group order (a fixed order, so results are
-// reproducible). `red` is shared scratch of blockDim x 16 bytes; `out` may alias `y`.
+// Sums of partial products with every thread of the CTA busy: the E values of a partial
+// (E = rows x right-hand sides) are read as 16-byte vectors when aligned, G = blockDim /
+// (vectors per partial) groups each sum every G-th partial with eight loads in flight, and
+// the group sums are added in group order (a fixed order, so results are reproducible).
 __device__ __forceinline__ void vadd(double &a, double b) { a += b; }
 __device__ __forceinline__ void vadd(float &a, float b) { a += b; }
 __device__ __forceinline__ void vadd(double2 &a, double2 b)
@@ -1188,8 +1187,9 @@ __device__ __forceinline__ U sum_strided(const U *__restrict__ part, int64_t npa
     return s[0];
 }
 
-template <typename V>
-__device__ void subtract_partials(const V *y, const V *__restrict__ part, int64_t nparts, int E, V *out, V *red)
+// out[e] = sum_j part[j][e] (j < nparts); `red` is shared scratch of blockDim x 16 bytes;
+// out may be part's first slot (every value is read before any is written).
+template <typename V> __device__ void sum_partials(const V *part, int64_t nparts, int E, V *out, V *red)
 {
     using Vec = typename std::conditional<sizeof(V) == 8, double2, float4>::type;
     constexpr int W = 16 / sizeof(V);
@@ -1211,45 +1211,66 @@ __device__ void subtract_partials(const V *y, const V *__restrict__ part, int64_
         __syncthreads();
         for (int e2 = tid; e2 < E; e2 += nt)
         {
-            V v = y[e2];
-            for (int q = 0; q < G; ++q)
-                v -= red[q * E + e2];
+            V v = red[e2];
+            for (int q = 1; q < G; ++q)
+                v += red[q * E + e2];
             out[e2] = v;
         }
         return;
     }
     for (int e2 = tid; e2 < E; e2 += nt)
-        out[e2] = y[e2] - sum_strided(part, nparts, E, 1, 0, e2);
+    {
+        const V v = sum_strided(part, nparts, E, 1, 0, e2);
+        out[e2] = v;
+    }
 }
 
-// Finishes pivot k of a forward stage: y_k <- D_k^{-1} (y_k - sum of its nparts partial
-// products), in ascending block order, D_k staged in shared memory when it fits.
+// out[e] = (y[e] - early[e]) - late[e], either term absent when null; early is read from
+// L2, late from L2 when late_l2 (written by another CTA) and directly otherwise.
+template <typename V>
+__device__ __forceinline__ void combine_partials(V *out, const V *y, const V *early, const V *late, bool late_l2,
+                                                 int E)
+{
+    for (int e = threadIdx.x; e < E; e += blockDim.x)
+    {
+        V v = y[e];
+        if (early)
+            v -= __ldcg(early + e);
+        if (late)
+            v -= late_l2 ? __ldcg(late + e) : late[e];
+        out[e] = v;
+    }
+}
+
+
+// The first kStageRegs x blockDim values of a diagonal block, loaded into registers
+// early so their latency overlaps other work before they go to shared memory.
+constexpr int kStageRegs = 16;
+template <typename T> struct DiagRegs
+{
+    T v[kStageRegs];
+};
+
+template <typename T> __device__ __forceinline__ void diag_load(DiagRegs<T> &dv, const T *gd, int mm)
+{
+#pragma unroll
+    for (int q = 0; q < kStageRegs; ++q)
+    {
+        const int i = q * (int)blockDim.x + (int)threadIdx.x;
+        dv.v[q] = i < mm ? gd[i] : T(0);
+    }
+}
+
+// y_k <- D_k^{-1} acc for pivot k (acc: m x nrhs in shared memory), D_k staged in shared
+// memory with an odd row stride (column reads of the substitution hit distinct banks) when
+// stage_diag, from the registers `dv` filled by diag_load.
 template <typename T, typename V>
-__device__ void fwd_finish(const DevSym &S, const T *__restrict__ slab, V *__restrict__ y, const V *part,
-                           int64_t nparts, int64_t k, int nrhs, int stage_diag, unsigned char *smem_raw)
+__device__ void fwd_solve_store(const DevSym &S, const T *__restrict__ slab, V *__restrict__ yk, int64_t k, int nrhs,
+                                int stage_diag, unsigned char *smem_raw, V *acc, const DiagRegs<T> &dv)
 {
     const int m = S.size[k];
-    __shared__ __align__(16) V red[kThreads * 16 / sizeof(V)];
-    V *acc = reinterpret_cast<V *>(smem_raw); // m * nrhs
-    V *yk = y + S.dof_off[k] * nrhs;
-    // The diagonal block goes to shared memory with an odd row stride (column reads of the
-    // substitution hit distinct banks) when it fits next to the accumulator. Its first
-    // kStageRegs x blockDim values are loaded into registers before the partial products
-    // are summed, so the two memory latencies overlap.
-    constexpr int kStageRegs = 16;
     const T *gd = slab + S.blk_off[S.diag_pos[k]];
     const int mm = m * m, nt = blockDim.x, tid = threadIdx.x;
-    T dv[kStageRegs];
-    if (stage_diag)
-    {
-#pragma unroll
-        for (int q = 0; q < kStageRegs; ++q)
-        {
-            const int i = q * nt + tid;
-            dv[q] = i < mm ? gd[i] : T(0);
-        }
-    }
-    subtract_partials(yk, part, nparts, m * nrhs, acc, red);
     const T *d = gd;
     int ldd = m;
     const size_t acc_bytes = ((size_t)m * nrhs * sizeof(V) + 15) / 16 * 16;
@@ -1265,7 +1286,7 @@ __device__ void fwd_finish(const DevSym &S, const T *__restrict__ slab, V *__res
             {
                 const int i = q * nt + tid;
                 if (i < mm)
-                    sd[(i >> sh) * ldd + (i & (m - 1))] = dv[q];
+                    sd[(i >> sh) * ldd + (i & (m - 1))] = dv.v[q];
             }
         }
         else
@@ -1275,7 +1296,7 @@ __device__ void fwd_finish(const DevSym &S, const T *__restrict__ slab, V *__res
             {
                 const int i = q * nt + tid;
                 if (i < mm)
-                    sd[(i / m) * ldd + i % m] = dv[q];
+                    sd[(i / m) * ldd + i % m] = dv.v[q];
             }
         }
         for (int i = kStageRegs * nt + tid; i < mm; i += nt)
@@ -1303,6 +1324,10 @@ __device__ void fwd_finish(const DevSym &S, const T *__restrict__ slab, V *__res
         yk[i] = acc[i];
 }
 
+// Partials of a pivot with n blocks: the "late" block -- the one whose source is final last,
+// the last lower block (forward) or the first upper block (backward) -- and the n - 1 early
+// ones, contiguous. Both substitution forms compute y - (sum of the early partials, in
+// sum_partials' order) - late partial, so they agree bit for bit.
 // Forward stage: y_k <- D_k^{-1} (y_k - sum_s L(k,s) y_s) for the stage's pivots
 // (block_system_apply_operations, src/blocks.c:729-769). Units: fwdu_pref, one per lower
 // block of a pivot (at least one per pivot).
@@ -1318,16 +1343,29 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int m = S.size[k];
     const int64_t nparts = S.diag_pos[k] - S.row_ptr[k];
     V *part = scratch + (S.fwd_rows[p] - S.fwd_rows[p0]) * nrhs;
+    const int E = m * nrhs;
     if (nparts > 0)
     {
         const int64_t j = u - S.fwdu_pref[p];
         const int64_t blk = S.row_ptr[k] + j;
         const int32_t src = S.cols[blk];
-        block_gemv(slab + S.blk_off[blk], m, S.size[src], y + S.dof_off[src] * nrhs, part + j * m * nrhs, nrhs);
+        block_gemv(slab + S.blk_off[blk], m, S.size[src], y + S.dof_off[src] * nrhs, part + j * E, nrhs);
         if (!last_ticket(tickets, p, nparts))
             return;
     }
-    fwd_finish(S, slab, y, part, nparts, k, nrhs, stage_diag, smem_raw);
+    __shared__ __align__(16) V red[kThreads * 16 / sizeof(V)];
+    DiagRegs<T> dv;
+    if (stage_diag)
+        diag_load(dv, slab + S.blk_off[S.diag_pos[k]], m * m);
+    if (nparts > 1)
+    {
+        sum_partials(part, nparts - 1, E, part, red);
+        __syncthreads();
+    }
+    V *acc = reinterpret_cast<V *>(smem_raw);
+    V *yk = y + S.dof_off[k] * nrhs;
+    combine_partials(acc, yk, nparts > 1 ? part : nullptr, nparts > 0 ? part + (nparts - 1) * E : nullptr, true, E);
+    fwd_solve_store(S, slab, yk, k, nrhs, stage_diag, smem_raw, acc, dv);
 }
 
 // Backward stage: y_k -= sum_c U(k,c) y_c over the upper blocks of the stage's pivots
@@ -1346,12 +1384,18 @@ __global__ void __launch_bounds__(kThreads, 2)
     const int64_t blk = S.diag_pos[k] + 1 + j;
     const int32_t c = S.cols[blk];
     V *part = scratch + (S.bwd_rows[p] - S.bwd_rows[p0]) * nrhs;
-    block_gemv(slab + S.blk_off[blk], m, S.size[c], y + S.dof_off[c] * nrhs, part + j * m * nrhs, nrhs);
+    const int E = m * nrhs;
+    block_gemv(slab + S.blk_off[blk], m, S.size[c], y + S.dof_off[c] * nrhs, part + j * E, nrhs);
     if (!last_ticket(tickets, p, nparts))
         return;
     __shared__ __align__(16) V red[kThreads * 16 / sizeof(V)];
+    if (nparts > 1)
+    {
+        sum_partials(part + E, nparts - 1, E, part + E, red);
+        __syncthreads();
+    }
     V *yk = y + S.dof_off[k] * nrhs;
-    subtract_partials(yk, part, nparts, m * nrhs, yk, red);
+    combine_partials(yk, yk, nparts > 1 ? part + E : nullptr, part, true, E);
 }
 
 // ----------------------------------------------------------------------------------
@@ -1488,79 +1532,128 @@ template <typename T> __device__ __forceinline__ void prefetch_l2(const T *p, in
         asm volatile("prefetch.global.L2 [%0];" ::"l"(c + off));
 }
 
-// Forward direction; partials of pivot slot p at scratch + fwd_rows[p] * nrhs.
+// Forward direction; partials of pivot slot p at scratch + fwd_rows[p] * nrhs. The late
+// item (the pivot's last lower block, whose source is the most recent pivot) finishes the
+// pivot: it loads its diagonal block before waiting, keeps its own partial in shared
+// memory, and waits only for the pre-sum of the early partials, which the CTA taking the
+// last early ticket forms and flags in pflags.
 template <typename T, typename V>
 __global__ void __launch_bounds__(kThreads, 1)
     k_fwd_flow(DevSym S, const T *__restrict__ slab, V *__restrict__ y, V *__restrict__ scratch,
-               int *__restrict__ tickets, int *__restrict__ flags, int tag, int64_t n_items, int nrhs, int stage_diag,
-               int *status)
+               int *__restrict__ tickets, int *__restrict__ flags, int *__restrict__ pflags, int tag, int64_t n_items,
+               int nrhs, int stage_diag, int *status)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(16) V red[kThreads * 16 / sizeof(V)];
+    V *acc = reinterpret_cast<V *>(smem_raw); // m * nrhs
     for (int64_t j = blockIdx.x; j < n_items; j += gridDim.x)
     {
         const int64_t p = S.fwd_item_p[j];
         const int64_t k = S.piv[p];
         const int m = S.size[k];
+        const int E = m * nrhs;
         const int64_t nparts = S.diag_pos[k] - S.row_ptr[k];
         V *part = scratch + S.fwd_rows[p] * nrhs;
-        if (nparts > 0)
+        V *yk = y + S.dof_off[k] * nrhs;
+        const T *gd = slab + S.blk_off[S.diag_pos[k]];
+        DiagRegs<T> dv;
+        if (nparts == 0)
         {
-            const int64_t local = j - S.fwdu_pref[p];
-            const int64_t blk = S.row_ptr[k] + local;
-            const int32_t src = S.cols[blk];
-            const int K = S.size[src];
-            if (local == 0 && stage_diag) // the finisher will stage D_k: bring it into L2 now
-                prefetch_l2(slab + S.blk_off[S.diag_pos[k]], (int64_t)m * m);
-            GemvRegs<T> g;
-            gemv_load(g, slab + S.blk_off[blk], m, K);
-            if (!wait_flag(flags + src, tag, status))
-                return;
-            if (g.ok)
-                gemv_finish(g, m, K, y + S.dof_off[src] * nrhs, part + local * m * nrhs, nrhs);
-            else
-                block_gemv<true>(slab + S.blk_off[blk], m, K, y + S.dof_off[src] * nrhs, part + local * m * nrhs,
-                                 nrhs);
-            if (!last_ticket(tickets, p, nparts))
-                continue;
+            if (stage_diag)
+                diag_load(dv, gd, m * m);
+            combine_partials(acc, yk, (const V *)nullptr, (const V *)nullptr, false, E);
+            fwd_solve_store(S, slab, yk, k, nrhs, stage_diag, smem_raw, acc, dv);
+            publish_flag(flags + k, tag);
+            continue;
         }
-        fwd_finish(S, slab, y, part, nparts, k, nrhs, stage_diag, smem_raw);
+        const int64_t local = j - S.fwdu_pref[p];
+        const bool late = local == nparts - 1;
+        const int64_t blk = S.row_ptr[k] + local;
+        const int32_t src = S.cols[blk];
+        const int K = S.size[src];
+        if (local == 0 && !late && stage_diag) // the finisher will stage D_k: bring it into L2 now
+            prefetch_l2(gd, (int64_t)m * m);
+        if (late && stage_diag)
+            diag_load(dv, gd, m * m);
+        GemvRegs<T> g;
+        gemv_load(g, slab + S.blk_off[blk], m, K);
+        if (!wait_flag(flags + src, tag, status))
+            return;
+        V *dst = late ? acc : part + local * E;
+        if (g.ok)
+            gemv_finish(g, m, K, y + S.dof_off[src] * nrhs, dst, nrhs);
+        else
+            block_gemv<true>(slab + S.blk_off[blk], m, K, y + S.dof_off[src] * nrhs, dst, nrhs);
+        if (!late)
+        {
+            if (!last_ticket(tickets, p, nparts - 1))
+                continue;
+            sum_partials(part, nparts - 1, E, part, red);
+            publish_flag(pflags + p, tag);
+            continue;
+        }
+        if (nparts > 1 && !wait_flag(pflags + p, tag, status))
+            return;
+        __syncthreads(); // the late partial is in acc
+        combine_partials(acc, yk, nparts > 1 ? (const V *)part : nullptr, (const V *)acc, false, E);
+        fwd_solve_store(S, slab, yk, k, nrhs, stage_diag, smem_raw, acc, dv);
         publish_flag(flags + k, tag);
     }
 }
 
-// Backward direction; partials of pivot slot p at scratch + bwd_rows[p] * nrhs.
+// Backward direction; partials of pivot slot p at scratch + bwd_rows[p] * nrhs. Item q of a
+// pivot with n upper blocks takes block (q + 1) mod n, so the late block 0 (its source is
+// the most recently finished pivot) comes last and finishes the pivot as in k_fwd_flow.
 template <typename T, typename V>
 __global__ void __launch_bounds__(kThreads, 2)
     k_bwd_flow(DevSym S, const T *__restrict__ slab, V *__restrict__ y, V *__restrict__ scratch,
-               int *__restrict__ tickets, int *__restrict__ flags, int tag, int64_t n_items, int nrhs, int *status)
+               int *__restrict__ tickets, int *__restrict__ flags, int *__restrict__ pflags, int tag, int64_t n_items,
+               int nrhs, int *status)
 {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(16) V red[kThreads * 16 / sizeof(V)];
+    V *acc = reinterpret_cast<V *>(smem_raw); // m * nrhs
     for (int64_t j = blockIdx.x; j < n_items; j += gridDim.x)
     {
         const int64_t p = S.bwd_item_p[j];
         const int64_t k = S.piv[p];
         const int m = S.size[k];
+        const int E = m * nrhs;
         const int64_t nparts = S.row_ptr[k + 1] - S.diag_pos[k] - 1;
-        if (nparts > 0)
+        if (nparts == 0)
         {
-            const int64_t local = j - S.bwd_first[p];
-            const int64_t blk = S.diag_pos[k] + 1 + local;
-            const int32_t c = S.cols[blk];
-            const int K = S.size[c];
-            V *part = scratch + S.bwd_rows[p] * nrhs;
-            GemvRegs<T> g;
-            gemv_load(g, slab + S.blk_off[blk], m, K);
-            if (!wait_flag(flags + c, tag, status))
-                return;
-            if (g.ok)
-                gemv_finish(g, m, K, y + S.dof_off[c] * nrhs, part + local * m * nrhs, nrhs);
-            else
-                block_gemv<true>(slab + S.blk_off[blk], m, K, y + S.dof_off[c] * nrhs, part + local * m * nrhs, nrhs);
-            if (!last_ticket(tickets, p, nparts))
-                continue;
-            __shared__ __align__(16) V red[kThreads * 16 / sizeof(V)];
-            V *yk = y + S.dof_off[k] * nrhs;
-            subtract_partials(yk, part, nparts, m * nrhs, yk, red);
+            publish_flag(flags + k, tag);
+            continue;
         }
+        const int64_t q = j - S.bwd_first[p];
+        const int64_t b = (q + 1) % nparts;
+        const bool late = b == 0;
+        const int64_t blk = S.diag_pos[k] + 1 + b;
+        const int32_t c = S.cols[blk];
+        const int K = S.size[c];
+        V *part = scratch + S.bwd_rows[p] * nrhs;
+        GemvRegs<T> g;
+        gemv_load(g, slab + S.blk_off[blk], m, K);
+        if (!wait_flag(flags + c, tag, status))
+            return;
+        V *dst = late ? acc : part + b * E;
+        if (g.ok)
+            gemv_finish(g, m, K, y + S.dof_off[c] * nrhs, dst, nrhs);
+        else
+            block_gemv<true>(slab + S.blk_off[blk], m, K, y + S.dof_off[c] * nrhs, dst, nrhs);
+        if (!late)
+        {
+            if (!last_ticket(tickets, p, nparts - 1))
+                continue;
+            sum_partials(part + E, nparts - 1, E, part + E, red);
+            publish_flag(pflags + p, tag);
+            continue;
+        }
+        if (nparts > 1 && !wait_flag(pflags + p, tag, status))
+            return;
+        __syncthreads(); // the late partial is in acc
+        V *yk = y + S.dof_off[k] * nrhs;
+        combine_partials(yk, yk, nparts > 1 ? (const V *)(part + E) : nullptr, (const V *)acc, false, E);
         publish_flag(flags + k, tag);
     }
 }
