@@ -45,6 +45,10 @@ METRIC = "decompose+solve ms: FP32+refine vs plain FP64 on one B200 at 1e-12 res
 TOL = 1e-12
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 CPU_SAMPLE_MESH = 20  # reference CPU sample: 20x20 elements at the same p
+# DRAM bytes (read + write) per 64x64 FP32 target block of a tensor-core update stage,
+# measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum, one pass) on a 96x96
+# p=8 stage, whose targets exceed L2: 245.3 MB for ~9,000 target blocks.
+TC_DRAM_BYTES_PER_TARGET_BLOCK = 245.3e6 / 9000
 
 
 def parse_args():
@@ -450,7 +454,7 @@ def run_ours(args):
     barrier()
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps)
 
-    def roofline(prof, bound, peak, unit, elem_bytes, peak_note, step_ms, kernel):
+    def roofline(prof, bound, peak, unit, elem_bytes, peak_note, step_ms, kernel, traffic_per_block=None):
         """One level's Schur update (both lookahead launches, timed with events on the
         handle's stream) against its bound; algorithmic work per level from the pattern:
         2 m k n flops per target block, and the FP32/FP64 bytes of reading and writing every
@@ -463,13 +467,16 @@ def run_ours(args):
         tflops = flops_per / (avg_ms * 1e-3) / 1e12
         gbs = bytes_per / (avg_ms * 1e-3) / 1e9
         achieved, per_launch = (tflops, flops_per) if bound == "tensor" else (gbs, bytes_per)
+        traffic = None
+        if traffic_per_block is not None:
+            traffic = traffic_per_block * prof.c_elems / prof.launches / 4096.0
         return {
             "bound": bound,
             "achieved": achieved,
             "peak": peak,
             "unit": unit,
             "frac": achieved / peak,
-            "traffic": None,
+            "traffic": traffic,
             "kernel": kernel,
             "launches": prof.launches,
             "avg_launch_ms": avg_ms,
@@ -490,7 +497,13 @@ def run_ours(args):
         mixed_prof, "hbm", hbm, "GB/s", 4,
         f"MEASURED_PEAKS.json hbm_gbs ({peak_src})", mixed_ms,
         "k_update64_tc (tcgen05 split-BF16, persistent, bulk-copy C ring)",
+        traffic_per_block=TC_DRAM_BYTES_PER_TARGET_BLOCK,
     )
+    if rmix is not None:
+        rmix["traffic_note"] = (
+            "dram__bytes_read.sum + dram__bytes_write.sum of one stage (both launches) from a 1-pass ncu capture "
+            "at 96x96 p=8, 27.2 KB per 64x64 target block, scaled to this stage's target blocks"
+        )
     if rmix is not None:
         # three BF16 MMAs per FP32 product on the tensor cores, against the sustained peak
         bf16 = float(peaks.get("bf16_tflops_sustained") or 1390.5)
