@@ -58,7 +58,11 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--mesh", type=int, default=128)
-    ap.add_argument("--p", type=int, default=8)
+    ap.add_argument(
+        "--p",
+        default="8",
+        help="element order: an integer, or 'rand' for a per-element order drawn uniformly from 2..10 (seed 0)",
+    )
     ap.add_argument("--cpu-sample-mesh", type=int, default=CPU_SAMPLE_MESH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-profile", action="store_true", help="do not time the dominant kernel with events")
@@ -90,9 +94,13 @@ def run_single(args):
 
 
 def workload_config(n, p, extra=None):
+    if str(p) == "rand":
+        blocks = "per-element p uniform in 2..10 (element blocks 4x4 to 100x100, edge blocks the larger neighbour's p)"
+    else:
+        p = int(p)
+        blocks = f"p={p} (element blocks {p * p}x{p * p}, edge blocks {p}x{p})"
     cfg = {
-        "workload": f"hybridized quad mesh {n}x{n} elements, p={p} (element blocks {p * p}x{p * p}, edge blocks "
-        f"{p}x{p}), 1 RHS, seed 0, reference first-fit coloring order",
+        "workload": f"hybridized quad mesh {n}x{n} elements, {blocks}, 1 RHS, seed 0, reference first-fit coloring order",
         "mesh": f"{n}x{n}",
         "p": p,
         "nrhs": 1,
@@ -108,12 +116,22 @@ def workload_config(n, p, extra=None):
 # workload
 
 
+def element_orders(n, p):
+    """The mesh generator's order argument: one order for every element, or per-element
+    orders uniform in 2..10 (seed 0) for p == 'rand'."""
+    from hybsol.b200 import meshgen
+
+    if str(p) == "rand":
+        return meshgen.random_orders(n, 2, 10, seed=0)
+    return int(p)
+
+
 def build_workload(n, p):
     import numpy as np
 
     from hybsol.b200 import meshgen, native
 
-    mat, b = meshgen.mesh_system(n, p, seed=0)
+    mat, b = meshgen.mesh_system(n, element_orders(n, p), seed=0)
     order = native.compute_ordering(mat.row_ptr, mat.cols, "first")
     pm = mat.permuted(order)
     off_o = np.concatenate([[0], np.cumsum(mat.sizes)])
@@ -203,7 +221,7 @@ def reference_sample(n, p, steps, warmup, threads):
     from oracle import oracle as O
 
     ref = O.load_reference()
-    mat, b = meshgen.mesh_system(n, p, seed=0)
+    mat, b = meshgen.mesh_system(n, element_orders(n, p), seed=0)
     times = []
     for it in range(warmup + steps):
         s = ref.BlockSystem(*[int(x) for x in mat.sizes])

@@ -141,6 +141,7 @@ struct hyb_system
     // the solve's status words, and the partial products of every pivot (flow_nrhs columns)
     int *d_flags = nullptr;
     int *d_pflags = nullptr; // per pivot: tag of the solve direction whose early partials are summed
+    int *d_lu_tickets = nullptr; // per pivot: CTAs of k_lu_trsm64 that have read the diagonal block
     int *d_solve_status = nullptr;
     uint32_t solve_epoch = 0;
     double *d_flow64 = nullptr;
@@ -182,6 +183,7 @@ struct hyb_system
         cudaFree(d_tickets);
         cudaFree(d_flags);
         cudaFree(d_pflags);
+        cudaFree(d_lu_tickets);
         cudaFree(d_solve_status);
         cudaFree(d_flow64);
         cudaFree(d_flow32);
@@ -369,12 +371,18 @@ template <typename T> int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cuda
     const int optin = smem_optin();
     const int64_t p0 = S.lvl_ptr[l], p1 = S.lvl_ptr[l + 1];
     const Symbolic::LevelShape &sh = S.shape[l];
-    if (sh.piv64)
+    if (sh.max_piv > 32 && sh.max_piv <= 64 && sh.max_up <= 128)
     {
-        // fused: 64x64 diagonal LU and the solves of the pivot rows' upper blocks
+        // fused: diagonal LU (padded to 64x64) and the solves of the pivot rows' upper blocks;
+        // pivots of up to 32 rows stay on the generic kernels, whose serial steps are short
         const int64_t units = S.lu_pref[p1] - S.lu_pref[p0];
-        hyb::k_lu_trsm64<T><<<(unsigned)units, hyb::kThreads, hyb::lu_trsm64_smem<T>(), st>>>(ds, slab, p0, p1,
-                                                                                              ds.lu_pref, h->d_status);
+        const dim3 grid((unsigned)units, sh.max_up > 64 ? 2u : 1u);
+        if (sh.piv64) // every pivot and upper block exactly 64: no padding
+            hyb::k_lu_trsm64<T, false><<<grid, hyb::kThreads, hyb::lu_trsm64_smem<T>(), st>>>(
+                ds, slab, p0, p1, ds.lu_pref, h->d_lu_tickets, h->d_status);
+        else
+            hyb::k_lu_trsm64<T, true><<<grid, hyb::kThreads, hyb::lu_trsm64_smem<T>(), st>>>(
+                ds, slab, p0, p1, ds.lu_pref, h->d_lu_tickets, h->d_status);
         ++launches;
         HYB_LAUNCHED("k_lu_trsm64", l);
         return enqueue_split<T>(h, slab, l, st, launches);
@@ -457,8 +465,8 @@ template <typename T> int enqueue_update(hyb_system *h, T *slab, int64_t l, cuda
             return HYB_SUCCESS;
         }
     }
-    hyb::k_update<T><<<dim3((unsigned)nu, tiles), hyb::kThreads, 0, st>>>(ds, slab, p0, p1, mode, sh.la_i0,
-                                                                         sh.la_j0);
+    // one CTA per target block, looping over its 64x64 tiles
+    hyb::k_update<T><<<(unsigned)nu, hyb::kThreads, 0, st>>>(ds, slab, p0, p1, mode, sh.la_i0, sh.la_j0);
     ++launches;
     HYB_LAUNCHED("k_update", l);
     return HYB_SUCCESS;
@@ -475,6 +483,7 @@ template <typename T> int enqueue_factor(hyb_system *h, T *slab, uint64_t &launc
     HYB_CUDA(cudaGetLastError()); // nothing earlier may be blamed on this schedule
     k_status_init<<<1, 32, 0, st>>>(h->d_status);
     ++launches;
+    HYB_CUDA(cudaMemsetAsync(h->d_lu_tickets, 0, S.n * sizeof(int), st)); // an aborted run may leave tickets
     int rc = HYB_SUCCESS;
     bool next_pivots_issued = false, forked = false;
     for (int64_t l = 0; l < S.n_levels; ++l)
@@ -892,6 +901,8 @@ HYB_API int hyb_system_create(uint64_t n, const uint64_t *block_sizes, const uin
     HYB_CUDA(cudaMemsetAsync(h->d_flags, 0, h->S.n * sizeof(int), h->stream));
     HYB_CUDA(cudaMalloc(&h->d_pflags, h->S.n * sizeof(int)));
     HYB_CUDA(cudaMemsetAsync(h->d_pflags, 0, h->S.n * sizeof(int), h->stream));
+    HYB_CUDA(cudaMalloc(&h->d_lu_tickets, h->S.n * sizeof(int)));
+    HYB_CUDA(cudaMemsetAsync(h->d_lu_tickets, 0, h->S.n * sizeof(int), h->stream));
     HYB_CUDA(cudaMalloc(&h->d_solve_status, hyb::ST_WORDS * sizeof(int)));
     HYB_CUDA(cudaMemsetAsync(h->d_tickets, 0, h->S.n * sizeof(int), h->stream));
     HYB_CUDA(cudaStreamSynchronize(h->stream));
@@ -939,6 +950,8 @@ HYB_API int hyb_system_copy(const hyb_system *src, hyb_system **out)
     HYB_CUDA(cudaMemsetAsync(h->d_flags, 0, h->S.n * sizeof(int), h->stream));
     HYB_CUDA(cudaMalloc(&h->d_pflags, h->S.n * sizeof(int)));
     HYB_CUDA(cudaMemsetAsync(h->d_pflags, 0, h->S.n * sizeof(int), h->stream));
+    HYB_CUDA(cudaMalloc(&h->d_lu_tickets, h->S.n * sizeof(int)));
+    HYB_CUDA(cudaMemsetAsync(h->d_lu_tickets, 0, h->S.n * sizeof(int), h->stream));
     HYB_CUDA(cudaMalloc(&h->d_solve_status, hyb::ST_WORDS * sizeof(int)));
     HYB_CUDA(cudaMemsetAsync(h->d_tickets, 0, h->S.n * sizeof(int), h->stream));
     HYB_CUDA(cudaStreamSynchronize(src->stream));
@@ -1037,8 +1050,10 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
             allow_smem(hyb::k_fwd_stage<double, double>, optin),
             allow_smem(hyb::k_fwd_stage<float, float>, optin),
             allow_smem(hyb::k_update64_f64, hyb::kUpd64Smem),
-            allow_smem(hyb::k_lu_trsm64<double>, hyb::lu_trsm64_smem<double>()),
-            allow_smem(hyb::k_lu_trsm64<float>, hyb::lu_trsm64_smem<float>()),
+            allow_smem(hyb::k_lu_trsm64<double, false>, hyb::lu_trsm64_smem<double>()),
+            allow_smem(hyb::k_lu_trsm64<float, false>, hyb::lu_trsm64_smem<float>()),
+            allow_smem(hyb::k_lu_trsm64<double, true>, hyb::lu_trsm64_smem<double>()),
+            allow_smem(hyb::k_lu_trsm64<float, true>, hyb::lu_trsm64_smem<float>()),
             allow_smem(hyb::k_update64_tc, hyb::kTcSmem),
             allow_smem(hyb::k_split64, 0),
             allow_smem(hyb::k_update<double>, 0),

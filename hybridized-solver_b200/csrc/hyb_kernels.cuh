@@ -70,7 +70,6 @@ enum
 
 constexpr int kThreads = 256;
 constexpr int kTile = 64;  // output tile edge of the generic update kernel
-constexpr int kTileK = 16; // K chunk staged through shared memory
 
 // Largest p with pref[p] <= u in [lo, hi) (pref is non-decreasing); work units are
 // assigned to pivots through these prefix arrays.
@@ -399,14 +398,19 @@ __device__ __forceinline__ int dt_idx(int c, int r)
 // pivots in diag. Four lanes share a column; lane q of a column holds rows 16q .. 16q+15
 // in registers, so a substitution step is one shuffle, eight 16-byte shared loads and 16
 // FMAs, with no barrier and no per-row test.
-template <typename T> __device__ void trsm64_columns(const T *dtl, const T *dtu, const T *diag, T *gb)
+// With kPad, gb is `rows` x `cols` (at most 64 each) of a row-major block with row stride
+// ldb, and the rest of the 64x64 system reads as zero and is not written; without, gb is a
+// full 64x64 block.
+template <typename T, bool kPad = false>
+__device__ void trsm64_columns(const T *dtl, const T *dtu, const T *diag, T *gb, int ldb = 64, int rows = 64,
+                               int cols = 64)
 {
     const int tid = threadIdx.x, lane = tid & 31;
     const int col = tid >> 2, q = tid & 3, base = lane & ~3;
     T x[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j)
-        x[j] = gb[(16 * q + j) * 64 + col];
+        x[j] = (!kPad || (16 * q + j < rows && col < cols)) ? gb[(16 * q + j) * ldb + col] : T(0);
 #pragma unroll
     for (int i = 0; i < 63; ++i)
     {
@@ -436,7 +440,8 @@ template <typename T> __device__ void trsm64_columns(const T *dtl, const T *dtu,
     }
 #pragma unroll
     for (int j = 0; j < 16; ++j)
-        gb[(16 * q + j) * 64 + col] = x[j];
+        if (!kPad || (16 * q + j < rows && col < cols))
+            gb[(16 * q + j) * ldb + col] = x[j];
 }
 
 template <typename T> constexpr int lu_trsm64_smem()
@@ -444,14 +449,15 @@ template <typename T> constexpr int lu_trsm64_smem()
     return (64 * kLd65 + 2 * 64 * kLdT + 64 + 256) * (int)sizeof(T);
 }
 
-// One CTA per upper block of the level's (64-row) pivots; every CTA factors its pivot's
-// diagonal block in shared memory (the first CTA of each pivot writes it back) and then
-// solves its block. A pivot without upper blocks gets one CTA for the LU alone: the grid
-// is the level's work units with empty pivots counted once (see enqueue_factor).
-template <typename T>
+// One CTA per upper block (grid.y: its 64-column strips) of the level's pivots of at most
+// 64 rows; every CTA factors its pivot's diagonal block in shared memory (the last of them
+// to read it writes it back) and then solves its strip. A pivot without upper blocks gets
+// one CTA for the LU alone: the grid is the level's work units with empty pivots counted
+// once (lu_pref).
+template <typename T, bool kPad>
 __global__ void __launch_bounds__(kThreads, 1)
     k_lu_trsm64(DevSym S, T *__restrict__ slab, int64_t p0, int64_t p1, const int64_t *__restrict__ unit_pref,
-                int *status)
+                int *__restrict__ lu_tickets, int *status)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *d = reinterpret_cast<T *>(smem_raw);
@@ -464,16 +470,39 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int64_t p = find_owner(unit_pref, p0, p1, u);
     const int64_t k = S.piv[p];
     const int64_t j = u - unit_pref[p];
+    const int m = kPad ? S.size[k] : 64;
+    const bool owner = j == 0 && blockIdx.y == 0; // reports zero and non-finite pivots
     T *gd = slab + S.blk_off[S.diag_pos[k]];
+    __shared__ int s_writer;
+    // an m x m diagonal block (m <= 64) is factored as [D 0; 0 I]: the padding only meets
+    // zeros, so D's factors are exactly those of D alone
     for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
-        d[(i >> 6) * kLd65 + (i & 63)] = gd[i];
+    {
+        const int r = i >> 6, c = i & 63;
+        d[r * kLd65 + c] = (!kPad || (r < m && c < m)) ? gd[r * m + c] : T(r == c);
+    }
     __syncthreads();
-    lu64_shared(d, rowbuf, colbuf, j == 0 ? status : nullptr, (int)k);
-    if (j == 0)
-        for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
-            gd[i] = d[(i >> 6) * kLd65 + (i & 63)];
+    // Every CTA of the pivot reads the unfactored block; the one that takes the pivot's last
+    // ticket -- after all the others have read it -- writes the factors back.
+    if (threadIdx.x == 0)
+    {
+        const int total = (int)(unit_pref[p + 1] - unit_pref[p]) * (int)gridDim.y;
+        s_writer = atomicAdd(lu_tickets + p, 1) == total - 1;
+    }
+    lu64_shared(d, rowbuf, colbuf, owner ? status : nullptr, (int)k);
+    if (s_writer)
+    {
+        for (int i = threadIdx.x; i < m * m; i += blockDim.x)
+            gd[i] = kPad ? d[(i / m) * kLd65 + i % m] : d[(i >> 6) * kLd65 + (i & 63)];
+        if (threadIdx.x == 0)
+            lu_tickets[p] = 0; // ready for the next factorization
+    }
     const int64_t blk = S.diag_pos[k] + 1 + j;
     if (blk >= S.row_ptr[k + 1])
+        return;
+    const int cc = kPad ? S.size[S.cols[blk]] : 64;
+    const int col0 = 64 * (int)blockIdx.y; // 64-column strip of the upper block
+    if (col0 >= cc)
         return;
     for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
     {
@@ -485,7 +514,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             diag[c] = v;
     }
     __syncthreads();
-    trsm64_columns(dtl, dtu, diag, slab + S.blk_off[blk]);
+    trsm64_columns<T, kPad>(dtl, dtu, diag, slab + S.blk_off[blk] + col0, cc, m, min(64, cc - col0));
 }
 
 // ----------------------------------------------------------------------------------
@@ -525,29 +554,52 @@ __device__ __forceinline__ void tile_store(const TileAcc<T> &acc, T *c, int ldc,
         }
 }
 
+// acc -= A B for one 64x64 output tile (A: M x K, row stride lda; B: K x N, row stride ldb;
+// rows/columns beyond M, N and K read as zero). K goes in chunks of kTileKC: a chunk is
+// staged in shared memory -- A transposed with a padded stride, so the staging stores hit
+// distinct banks -- while the next chunk is already loaded into registers. 256 threads,
+// 4x4 outputs each. sa: kTileKC x kLdA, sb: kTileKC x kTile.
+constexpr int kTileKC = 32;
+constexpr int kLdA = kTile + 1;
 template <typename T>
 __device__ __forceinline__ void tile_sub_ab(TileAcc<T> &acc, const T *__restrict__ a, int lda,
                                             const T *__restrict__ b, int ldb, int M, int N, int K, T *sa, T *sb)
 {
+    constexpr int kPer = kTile * kTileKC / kThreads; // chunk values per thread, each of A and B
     const int tid = threadIdx.x;
     const int ty = tid / 16, tx = tid % 16;
-    for (int k0 = 0; k0 < K; k0 += kTileK)
-    {
-        for (int idx = tid; idx < kTile * kTileK; idx += kThreads)
+    T ra[kPer], rb[kPer];
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int q = 0; q < kPer; ++q)
         {
-            const int r = idx / kTileK, kk = idx % kTileK;
-            sa[kk * kTile + r] = (r < M && k0 + kk < K) ? a[r * lda + k0 + kk] : T(0);
-            const int kr = idx / kTile, cc = idx % kTile;
-            sb[kr * kTile + cc] = (cc < N && k0 + kr < K) ? b[(k0 + kr) * ldb + cc] : T(0);
+            const int idx = q * kThreads + tid;
+            const int r = idx / kTileKC, kk = idx % kTileKC; // A: rows of kTileKC along K
+            ra[q] = (r < M && k0 + kk < K) ? a[(int64_t)r * lda + k0 + kk] : T(0);
+            const int kr = idx / kTile, cc = idx % kTile; // B: rows of 64 along N
+            rb[q] = (cc < N && k0 + kr < K) ? b[(int64_t)(k0 + kr) * ldb + cc] : T(0);
+        }
+    };
+    load(0);
+    for (int k0 = 0; k0 < K; k0 += kTileKC)
+    {
+#pragma unroll
+        for (int q = 0; q < kPer; ++q)
+        {
+            const int idx = q * kThreads + tid;
+            sa[(idx % kTileKC) * kLdA + idx / kTileKC] = ra[q];
+            sb[idx] = rb[q];
         }
         __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < kTileK; ++kk)
+        if (k0 + kTileKC < K)
+            load(k0 + kTileKC);
+#pragma unroll 8
+        for (int kk = 0; kk < kTileKC; ++kk)
         {
             T av[4], bv[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
-                av[i] = sa[kk * kTile + ty * 4 + i];
+                av[i] = sa[kk * kLdA + ty * 4 + i];
 #pragma unroll
             for (int j = 0; j < 4; ++j)
                 bv[j] = sb[kk * kTile + tx * 4 + j];
@@ -614,11 +666,11 @@ __device__ __forceinline__ UpdUnit update_unit(const DevSym &S, int64_t p0, int6
 // Update of a level whose pivots touch disjoint target rows; grid.x: work units (see
 // update_unit), grid.y: the 64x64 tiles of a target block.
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
     k_update(DevSym S, T *__restrict__ slab, int64_t p0, int64_t p1, int mode, int i0, int j0)
 {
-    __shared__ __align__(16) T sa[kTile * kTileK];
-    __shared__ __align__(16) T sb[kTile * kTileK];
+    __shared__ __align__(16) T sa[kTileKC * kLdA];
+    __shared__ __align__(16) T sb[kTileKC * kTile];
     const UpdUnit w = update_unit(S, p0, p1, mode, i0, j0);
     const int64_t k = w.k, li = w.li, bu = w.bu;
     const int32_t t = S.lcol_row[li];
@@ -626,17 +678,18 @@ __global__ void __launch_bounds__(kThreads)
     const int M = S.size[t], N = S.size[c], K = S.size[k];
     const int tn = (N + kTile - 1) / kTile;
     const int tm = (M + kTile - 1) / kTile;
-    if ((int)blockIdx.y >= tm * tn)
-        return;
-    const int r0 = (blockIdx.y / tn) * kTile, c0 = (blockIdx.y % tn) * kTile;
-    const int64_t tgt = find_col(S.cols, S.row_ptr[t], S.row_ptr[t + 1], c);
-    T *cb = slab + S.blk_off[tgt] + (int64_t)r0 * N + c0;
-    const T *ab = slab + S.blk_off[S.lcol_blk[li]] + (int64_t)r0 * K;
-    const T *bb = slab + S.blk_off[bu] + c0;
-    TileAcc<T> acc;
-    tile_load(acc, cb, N, M - r0, N - c0);
-    tile_sub_ab(acc, ab, K, bb, N, M - r0, N - c0, K, sa, sb);
-    tile_store(acc, cb, N, M - r0, N - c0);
+    const int64_t tgt = warp_find_col(S.cols, S.row_ptr[t], S.row_ptr[t + 1], c);
+    for (int tile = 0; tile < tm * tn; ++tile)
+    {
+        const int r0 = (tile / tn) * kTile, c0 = (tile % tn) * kTile;
+        T *cb = slab + S.blk_off[tgt] + (int64_t)r0 * N + c0;
+        const T *ab = slab + S.blk_off[S.lcol_blk[li]] + (int64_t)r0 * K;
+        const T *bb = slab + S.blk_off[bu] + c0;
+        TileAcc<T> acc;
+        tile_load(acc, cb, N, M - r0, N - c0);
+        tile_sub_ab(acc, ab, K, bb, N, M - r0, N - c0, K, sa, sb);
+        tile_store(acc, cb, N, M - r0, N - c0);
+    }
 }
 
 // ----------------------------------------------------------------------------------
@@ -817,8 +870,8 @@ __global__ void __launch_bounds__(kUpd64Threads)
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_update_listed(DevSym S, T *__restrict__ slab, int64_t q0)
 {
-    __shared__ __align__(16) T sa[kTile * kTileK];
-    __shared__ __align__(16) T sb[kTile * kTileK];
+    __shared__ __align__(16) T sa[kTileKC * kLdA];
+    __shared__ __align__(16) T sb[kTileKC * kTile];
     const int64_t q = q0 + blockIdx.x;
     const int32_t t = S.mt_row[q], c = S.mt_col[q];
     const int M = S.size[t], N = S.size[c];
@@ -1773,8 +1826,8 @@ __global__ void k_dense_lu_global(double *a, int m, int *status)
 __global__ void __launch_bounds__(kThreads) k_dense_gemm(const double *a, const double *b, double *c, int m, int k,
                                                          int n, int subtract)
 {
-    __shared__ __align__(16) double sa[kTile * kTileK];
-    __shared__ __align__(16) double sb[kTile * kTileK];
+    __shared__ __align__(16) double sa[kTileKC * kLdA];
+    __shared__ __align__(16) double sb[kTileKC * kTile];
     const int r0 = blockIdx.y * kTile, c0 = blockIdx.x * kTile;
     TileAcc<double> acc;
     if (subtract)

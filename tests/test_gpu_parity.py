@@ -321,3 +321,19 @@ def test_dataflow_solve_matches_staged(gpu, n, p, nrhs, prec):
     osys = O.OracleSystem.from_csr(pm.sizes, pm.row_ptr, pm.cols, pm.vals)
     osys.decompose()
     assert rel_err(x_flow, osys.solve(bn)) < (TOL_X if prec == 0 else TOL_X_MIXED)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_uneven_orders_large_pivot_grids(gpu, prec):
+    """64x64 mesh with per-element orders 2..10: pivots of 33-64 rows take the padded fused
+    LU + row-solve kernel with more CTAs than fit at once (and 128-wide upper blocks in two
+    strips); every CTA must factor the unfactored block. The FP64 residual pins it."""
+    from hybsol.b200 import meshgen
+
+    n = 64
+    mat, b = _mesh(n, meshgen.random_orders(n, 2, 10, seed=0), seed=0)
+    order, pm, ns = _native_from(gpu, mat)
+    bn = reorder_rhs(mat.sizes, order, b)
+    ns.decompose(prec)
+    x, info = ns.solve(bn)
+    assert info["relative_residual"] < (1e-13 if prec == 0 else 1e-12)
