@@ -534,7 +534,7 @@ __device__ __forceinline__ void tile_load(TileAcc<T> &acc, const T *c, int ldc, 
 #pragma unroll
         for (int j = 0; j < 4; ++j)
         {
-            const int r = ty * 4 + i, cc = tx * 4 + j;
+            const int r = ty * 4 + i, cc = tx + 16 * j;
             acc.v[i][j] = (r < M && cc < N) ? c[r * ldc + cc] : T(0);
         }
 }
@@ -548,7 +548,7 @@ __device__ __forceinline__ void tile_store(const TileAcc<T> &acc, T *c, int ldc,
 #pragma unroll
         for (int j = 0; j < 4; ++j)
         {
-            const int r = ty * 4 + i, cc = tx * 4 + j;
+            const int r = ty * 4 + i, cc = tx + 16 * j;
             if (r < M && cc < N)
                 c[r * ldc + cc] = acc.v[i][j];
         }
@@ -558,7 +558,7 @@ __device__ __forceinline__ void tile_store(const TileAcc<T> &acc, T *c, int ldc,
 // rows/columns beyond M, N and K read as zero). K goes in chunks of kTileKC: a chunk is
 // staged in shared memory -- A transposed with a padded stride, so the staging stores hit
 // distinct banks -- while the next chunk is already loaded into registers. 256 threads,
-// 4x4 outputs each. sa: kTileKC x kLdA, sb: kTileKC x kTile.
+// 4x4 outputs each (rows 4 ty + i, columns tx + 16 j). sa: kTileKC x kLdA, sb: kTileKC x kTile.
 constexpr int kTileKC = 32;
 constexpr int kLdA = kTile + 1;
 template <typename T>
@@ -602,7 +602,7 @@ __device__ __forceinline__ void tile_sub_ab(TileAcc<T> &acc, const T *__restrict
                 av[i] = sa[kk * kLdA + ty * 4 + i];
 #pragma unroll
             for (int j = 0; j < 4; ++j)
-                bv[j] = sb[kk * kTile + tx * 4 + j];
+                bv[j] = sb[kk * kTile + tx + 16 * j]; // consecutive across lanes: no bank conflicts
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
