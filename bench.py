@@ -67,6 +67,12 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-profile", action="store_true", help="do not time the dominant kernel with events")
     ap.add_argument(
+        "--profile-stride",
+        type=int,
+        default=32,
+        help="time the Schur update of every n-th level with events (each event pair costs a few us of its stage)",
+    )
+    ap.add_argument(
         "--single",
         action="store_true",
         help="one decompose + solve per form and nothing else (the command ncu captures run)",
@@ -403,7 +409,7 @@ def run_ours(args):
     d_b = torch.from_numpy(bn).to("cuda")
     d_x = torch.empty_like(d_b)
     if not args.no_profile:
-        lib.hyb_profile_enable(ns._h, 1)
+        lib.hyb_profile_enable(ns._h, max(1, args.profile_stride))
 
     def device_step(prec):
         """One step with inputs resident in HBM; returns (launches, solve info)."""
@@ -474,9 +480,11 @@ def run_ours(args):
 
     def roofline(prof, bound, peak, unit, elem_bytes, peak_note, step_ms, kernel, traffic_per_block=None):
         """One level's Schur update (both lookahead launches, timed with events on the
-        handle's stream) against its bound; algorithmic work per level from the pattern:
-        2 m k n flops per target block, and the FP32/FP64 bytes of reading and writing every
-        target once plus reading the lower-column and upper-row operands once."""
+        handle's stream, every profile-stride-th level of the timed steps) against its bound;
+        algorithmic work per level from the pattern: 2 m k n flops per target block, and the
+        FP32/FP64 bytes of reading and writing every target once plus reading the
+        lower-column and upper-row operands once. The share of the step scales the sampled
+        mean to every level with an update."""
         if prof is None:
             return None
         avg_ms = prof.total_ms / prof.launches
@@ -496,9 +504,10 @@ def run_ours(args):
             "frac": achieved / peak,
             "traffic": traffic,
             "kernel": kernel,
-            "launches": prof.launches,
             "avg_launch_ms": avg_ms,
-            "share_of_step": prof.total_ms / step_ms,
+            "share_of_step": avg_ms * prof.levels / step_ms,
+            "levels_timed": prof.launches,
+            "levels_with_update": prof.levels,
             "peak_source": peak_note,
             "algorithmic_per_launch": per_launch,
             "algorithmic_unit": "flop" if bound == "tensor" else "byte",

@@ -165,10 +165,12 @@ struct hyb_system
     std::map<std::pair<int, int>, std::unique_ptr<GraphExec>> g_solve; // (precision, nrhs)
     uint64_t launches = 0;
     uint64_t last_launches = 0;
-    // profiling: one event pair per level around the Schur-update kernel
-    bool profile = false;
+    // profiling: one event pair around the Schur-update kernels of every profile-th level
+    // that has an update (0: off)
+    int profile = 0;
     std::vector<cudaEvent_t> prof_ev;
     std::vector<int64_t> prof_levels; // level of each event pair
+    int64_t prof_update_levels = 0;   // levels with an update in the captured schedule
     int prof_precision = -1;
 
     ~hyb_system()
@@ -207,6 +209,7 @@ struct hyb_system
             cudaEventDestroy(e);
         prof_ev.clear();
         prof_levels.clear();
+        prof_update_levels = 0;
     }
 
     void free_solve_buffers()
@@ -495,8 +498,10 @@ template <typename T> int enqueue_factor(hyb_system *h, T *slab, uint64_t &launc
         else if ((rc = enqueue_pivots<T>(h, slab, l, st, launches)) != HYB_SUCCESS)
             return rc;
         next_pivots_issued = false;
-        const bool timed = h->profile && (S.lvl_listed[l] ? S.mt_lvl_ptr[l + 1] > S.mt_lvl_ptr[l]
-                                                          : S.upd_pref[p1] > S.upd_pref[p0]);
+        const bool has_update =
+            S.lvl_listed[l] ? S.mt_lvl_ptr[l + 1] > S.mt_lvl_ptr[l] : S.upd_pref[p1] > S.upd_pref[p0];
+        const bool timed = h->profile > 0 && has_update && h->prof_update_levels % h->profile == 0;
+        h->prof_update_levels += has_update ? 1 : 0;
         if (timed)
         {
             cudaEvent_t e0, e1;
@@ -1376,13 +1381,13 @@ HYB_API uint64_t hyb_last_launch_count(const hyb_system *h)
     return h ? h->last_launches : 0;
 }
 
-HYB_API int hyb_profile_enable(hyb_system *h, int enable)
+HYB_API int hyb_profile_enable(hyb_system *h, int stride)
 {
-    if (check_handle(h))
+    if (check_handle(h) || stride < 0)
         return HYB_INVALID_ARGUMENT;
-    if (h->profile != (enable != 0))
+    if (h->profile != stride)
     {
-        h->profile = enable != 0;
+        h->profile = stride;
         // the factorization graphs are recaptured with (or without) the event nodes
         h->g_factor[0].reset();
         h->g_factor[1].reset();
@@ -1414,6 +1419,7 @@ HYB_API int hyb_profile_read(const hyb_system *h, hyb_kernel_profile *out)
         out->c_elems += sh.upd_c_elems;
         out->ab_elems += sh.upd_ab_elems;
     }
+    out->levels = (uint64_t)h->prof_update_levels;
     return HYB_SUCCESS;
 }
 

@@ -71,6 +71,7 @@ class KernelProfile(ctypes.Structure):
         ("flops", ctypes.c_double),
         ("c_elems", ctypes.c_double),
         ("ab_elems", ctypes.c_double),
+        ("levels", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:

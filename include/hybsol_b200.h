@@ -228,17 +228,21 @@ HYB_API uint64_t hyb_last_launch_count(const hyb_system *sys);
 
 typedef struct
 {
-    uint64_t launches; /* Schur-update kernel launches timed */
+    uint64_t launches; /* levels whose Schur-update kernels were timed */
     double total_ms;   /* sum of their device durations (CUDA events on the handle's stream) */
     double flops;      /* algorithmic flops they performed */
     double c_elems;    /* target scalars each read and written once */
     double ab_elems;   /* operand scalars (lower-column and upper-row blocks) */
+    uint64_t levels;   /* levels of the decomposition that have a Schur update, timed or not */
 } hyb_kernel_profile;
 
-/* When enabled, later decompositions record CUDA events around every level's
- * Schur-update kernel inside the factorization graph; hyb_profile_read returns the
- * totals of the last decomposition. */
-HYB_API int hyb_profile_enable(hyb_system *sys, int enable);
+/* With stride n >= 1, later decompositions record CUDA events around the Schur-update
+ * kernels of every n-th level that has an update (n = 1: all of them) inside the
+ * factorization graph; 0 turns this off. Each event pair adds a few microseconds to the
+ * stage it brackets, so a stride of 16 or more keeps a timed run within about 1% of an
+ * untimed one. hyb_profile_read returns the totals of the timed levels of the last
+ * decomposition. */
+HYB_API int hyb_profile_enable(hyb_system *sys, int stride);
 HYB_API int hyb_profile_read(const hyb_system *sys, hyb_kernel_profile *update);
 
 /* Dense single-block kernels on device (the fine-grained surface of

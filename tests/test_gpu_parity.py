@@ -232,6 +232,34 @@ def test_lookahead_schedule_matches_in_order(gpu, prec):
     assert all(np.array_equal(x, y) for x, y in zip(blocks, blocks2))
 
 
+@pytest.mark.parametrize("prec", [0, 1])
+def test_sampled_update_profile(gpu, prec):
+    """Event pairs around every n-th level's update: ceil(levels / n) timed levels, the same
+    level count for every stride, and factors identical to an untimed decomposition."""
+    import ctypes
+
+    mat, b = _mesh(10, 8, seed=23)
+    order, pm, ns = _native_from(gpu, mat)
+    lib = gpu.lib()
+    ns.decompose(prec)
+    ref = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
+    counts = {}
+    for stride in (1, 4):
+        assert lib.hyb_profile_enable(ns._h, stride) == 0
+        ns.set_values(pm.vals)
+        ns.decompose(prec)
+        prof = gpu.KernelProfile()
+        assert lib.hyb_profile_read(ns._h, ctypes.byref(prof)) == 0
+        counts[stride] = (prof.launches, prof.levels)
+        assert prof.total_ms > 0 and prof.c_elems > 0
+        blocks = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
+        assert all(np.array_equal(x, y) for x, y in zip(ref, blocks))
+    levels = counts[1][1]
+    assert levels > 4 and counts[1] == (levels, levels) and counts[4] == ((levels + 3) // 4, levels)
+    assert lib.hyb_profile_enable(ns._h, -1) != 0
+    assert lib.hyb_profile_enable(ns._h, 0) == 0
+
+
 @pytest.mark.parametrize("n", [5, 12])
 def test_tensor_core_mixed_matches_cuda_core_mixed(gpu, n):
     """The tcgen05 split-BF16 updates and the FP32 CUDA-core updates both refine to 1e-12
