@@ -150,6 +150,7 @@ struct hyb_system
     int factored = -1; // -1, HYB_PRECISION_FP64 or HYB_PRECISION_MIXED
     double *d_f64 = nullptr;
     float *d_f32 = nullptr;
+    float *d_dinv = nullptr; // FP32 inverses of the 64-row diagonal blocks (mixed form), n_inv x 4096
     // BF16 operand splits of tensor-core levels, two level-parity halves of split_half bytes
     unsigned char *d_ops = nullptr;
     size_t split_half = 0;
@@ -191,6 +192,7 @@ struct hyb_system
         cudaFree(d_flow32);
         cudaFree(d_f64);
         cudaFree(d_f32);
+        cudaFree(d_dinv);
         cudaFree(d_ops);
         cudaFree(d_tgt);
         free_solve_buffers();
@@ -280,6 +282,8 @@ int upload_symbolic(hyb_system *h)
         {S.bwd_first.data(), S.bwd_first.size() * 8, (const void **)&d.bwd_first},
         {S.fwd_rows.data(), S.fwd_rows.size() * 8, (const void **)&d.fwd_rows},
         {S.bwd_rows.data(), S.bwd_rows.size() * 8, (const void **)&d.bwd_rows},
+        {S.inv_idx.data(), S.inv_idx.size() * 4, (const void **)&d.inv_idx},
+        {S.inv_row.data(), S.inv_row.size() * 4, (const void **)&d.inv_row},
         {S.mt_tgt.data(), S.mt_tgt.size() * 4, (const void **)&d.mt_tgt},
         {S.mt_row.data(), S.mt_row.size() * 4, (const void **)&d.mt_row},
         {S.mt_col.data(), S.mt_col.size() * 4, (const void **)&d.mt_col},
@@ -412,6 +416,23 @@ template <typename T> int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cuda
     return enqueue_split<T>(h, slab, l, st, launches);
 }
 
+// FP32 inverses of every 64-row diagonal block (mixed form), in one launch after the last
+// level. Only the solves read them; launched beside the stages instead, they slowed the
+// update CTAs that shared their SMs, and each level waits for its slowest update CTA.
+template <typename T> int enqueue_inverses(hyb_system *h, T *slab, uint64_t &launches)
+{
+    if constexpr (std::is_same_v<T, float>)
+    {
+        if (!h->d_dinv || h->S.n_inv == 0)
+            return HYB_SUCCESS;
+        hyb::k_diag_inv64<float>
+            <<<(unsigned)h->S.n_inv, hyb::kInvThreads, 0, h->stream>>>(h->ds, slab, h->d_dinv);
+        ++launches;
+        HYB_LAUNCHED("k_diag_inv64", h->S.n_levels - 1);
+    }
+    return HYB_SUCCESS;
+}
+
 // Schur-complement updates of level l: mode 0 all of them, 1 / 2 the lookahead split.
 template <typename T> int enqueue_update(hyb_system *h, T *slab, int64_t l, cudaStream_t st, int mode,
                                          uint64_t &launches)
@@ -540,15 +561,27 @@ template <typename T> int enqueue_factor(hyb_system *h, T *slab, uint64_t &launc
         HYB_CUDA(cudaEventRecord(h->ev_join, st2));
         HYB_CUDA(cudaStreamWaitEvent(st, h->ev_join, 0));
     }
+    if ((rc = enqueue_inverses<T>(h, slab, launches)) != HYB_SUCCESS)
+        return rc;
     HYB_CUDA(cudaGetLastError());
     return HYB_SUCCESS;
 }
 
 // Forward + backward substitution of y (type V, dof x nrhs) with the factors in `slab`.
+// The FP32 diagonal inverses a solve with factors of type T uses (mixed form only).
+template <typename T> const T *solve_dinv(const hyb_system *h)
+{
+    if constexpr (std::is_same_v<T, float>)
+        return h->d_dinv;
+    else
+        return nullptr;
+}
+
 template <typename T, typename V> int enqueue_solve(hyb_system *h, const T *slab, V *y, V *scratch, int nrhs,
                                                     uint64_t &launches)
 {
     const Symbolic &S = h->S;
+    const T *dinv = solve_dinv<T>(h);
     const DevSym &ds = h->ds;
     cudaStream_t st = h->stream;
     // tickets return to zero after every stage; clearing them guards against an aborted solve
@@ -562,7 +595,7 @@ template <typename T, typename V> int enqueue_solve(hyb_system *h, const T *slab
         const int diag_bytes = mp * (mp | 1) * (int)sizeof(T);
         const int stage = acc_bytes + diag_bytes <= solve_smem_cap() ? 1 : 0;
         hyb::k_fwd_stage<T, V><<<(unsigned)units, hyb::kThreads, acc_bytes + (stage ? diag_bytes : 0), st>>>(
-            ds, slab, y, scratch, h->d_tickets, p0, p1, nrhs, stage);
+            ds, slab, y, scratch, h->d_tickets, p0, p1, nrhs, stage, dinv);
         ++launches;
     }
     for (int64_t l = S.n_levels - 1; l >= 0; --l)
@@ -637,11 +670,13 @@ template <typename T, typename V> int enqueue_solve_flow(hyb_system *h, const T 
     DevSym ds = h->ds;
     V *scratch = scr;
     int *tickets = h->d_tickets, *flags = h->d_flags, *pflags = h->d_pflags, *status = h->d_solve_status;
+    const T *dinv = solve_dinv<T>(h);
     int64_t nf = (int64_t)S.fwd_item_p.size(), nb = (int64_t)S.bwd_item_p.size();
     const int sms = sm_count();
     {
         const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nf, (int64_t)per_sm_f * sms));
-        void *args[] = {&ds, (void *)&slab, &y, &scratch, &tickets, &flags, &pflags, &tag_f, &nf, &nrhs, &stage, &status};
+        void *args[] = {&ds,    (void *)&slab, &y,     &scratch, &tickets, &flags, &pflags,
+                        &tag_f, &nf,           &nrhs,  &stage,   &dinv,    &status};
         HYB_CUDA(cudaLaunchCooperativeKernel((const void *)hyb::k_fwd_flow<T, V>, dim3(grid), dim3(hyb::kThreads),
                                              args, fwd_smem, st));
     }
@@ -972,6 +1007,12 @@ HYB_API int hyb_system_copy(const hyb_system *src, hyb_system **out)
         HYB_CUDA(cudaMalloc(&h->d_f32, slab * sizeof(float)));
         HYB_CUDA(cudaMemcpyAsync(h->d_f32, src->d_f32, slab * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
     }
+    if (src->d_dinv)
+    {
+        const size_t bytes = (size_t)h->S.n_inv * 4096 * sizeof(float);
+        HYB_CUDA(cudaMalloc(&h->d_dinv, bytes));
+        HYB_CUDA(cudaMemcpyAsync(h->d_dinv, src->d_dinv, bytes, cudaMemcpyDeviceToDevice, h->stream));
+    }
     h->factored = src->factored;
     HYB_CUDA(cudaStreamSynchronize(h->stream));
     *out = h.release();
@@ -1077,7 +1118,9 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
         if (h->d_f32)
         {
             cudaFree(h->d_f32);
+            cudaFree(h->d_dinv);
             h->d_f32 = nullptr;
+            h->d_dinv = nullptr;
             h->g_factor[1].reset();
             h->g_solve.clear();
         }
@@ -1110,6 +1153,8 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
         if (!h->d_f32)
         {
             HYB_CUDA(cudaMalloc(&h->d_f32, slab * sizeof(float)));
+            if (S.n_inv > 0)
+                HYB_CUDA(cudaMalloc(&h->d_dinv, (size_t)S.n_inv * 4096 * sizeof(float)));
             h->g_factor[1].reset();
             h->g_solve.clear();
         }

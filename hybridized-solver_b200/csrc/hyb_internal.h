@@ -59,6 +59,9 @@ struct Symbolic
     std::vector<int64_t> bwd_first;  // [n] first backward item of each pivot slot
     std::vector<int64_t> fwd_rows;  // [n+1] prefix of lower-row block count * pivot size, padded to 4 (scratch rows)
     std::vector<int64_t> bwd_rows;  // [n+1] prefix of upper-row block count * pivot size, padded to 4
+    std::vector<int32_t> inv_idx;   // [n] slot of a 64-row block row's FP32 diagonal inverse (-1: other sizes)
+    std::vector<int32_t> inv_row;   // [n_inv] block row of each inverse slot
+    int64_t n_inv = 0;              // block rows of 64
 
     // Levels whose pivots share target rows get explicit target lists, each target's
     // sources in ascending pivot order (a fixed order, no atomics).

@@ -46,6 +46,8 @@ struct DevSym
     const int64_t *bwd_first;  // [n] first backward item of pivot slot p
     const int64_t *fwd_rows;
     const int64_t *bwd_rows;
+    const int32_t *inv_idx; // [n] slot of a 64-row block row's FP32 diagonal inverse (-1: none)
+    const int32_t *inv_row; // [n_inv] block row of each inverse slot
     const int32_t *mt_tgt;
     const int32_t *mt_row;
     const int32_t *mt_col;
@@ -1314,14 +1316,93 @@ template <typename T> __device__ __forceinline__ void diag_load(DiagRegs<T> &dv,
     }
 }
 
-// y_k <- D_k^{-1} acc for pivot k (acc: m x nrhs in shared memory), D_k staged in shared
-// memory with an odd row stride (column reads of the substitution hit distinct banks) when
-// stage_diag, from the registers `dv` filled by diag_load.
+// Explicit inverses of the 64x64 diagonal blocks for the FP32 solves inside the mixed
+// form's refinement, where the inner solve only has to be a good approximation (the FP64
+// residual decides convergence): X = D^{-1} from D's LU factors, column j of X by thread
+// j as U^{-1} (L^{-1} e_j) with the substitution's arithmetic (unit L, multiply by the
+// reciprocal of U's diagonal), stored transposed (xt[j * 64 + i] = X(i, j)) so the
+// forward solve's register layout reads it directly. One CTA per inverse slot.
+constexpr int kInvThreads = 64;
+template <typename T>
+__global__ void __launch_bounds__(kInvThreads) k_diag_inv64(DevSym S, const T *__restrict__ slab, T *__restrict__ dinv)
+{
+    __shared__ __align__(16) T sd[64 * 64];
+    const int32_t slot = blockIdx.x;
+    const int64_t k = S.inv_row[slot];
+    const T *gd = slab + S.blk_off[S.diag_pos[k]];
+    for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
+        sd[i] = gd[i];
+    __syncthreads();
+    const int j = threadIdx.x;
+    T y[64];
+#pragma unroll
+    for (int i = 0; i < 64; ++i)
+    {
+        T s = i == j ? T(1) : T(0);
+#pragma unroll
+        for (int c = 0; c < i; ++c)
+            s -= sd[i * 64 + c] * y[c];
+        y[i] = s;
+    }
+#pragma unroll
+    for (int i = 63; i >= 0; --i)
+    {
+        T s = y[i];
+#pragma unroll
+        for (int c = i + 1; c < 64; ++c)
+            s -= sd[i * 64 + c] * y[c];
+        y[i] = s * (T(1) / sd[i * 64 + i]);
+    }
+    T *xt = dinv + (int64_t)slot * 4096 + j * 64;
+#pragma unroll
+    for (int i = 0; i < 64; ++i)
+        xt[i] = y[i];
+}
+
+// The registers a forward finisher fills for pivot k before it waits: k's inverse when
+// the factorization built one (dinv set), else D_k when it will be staged.
+template <typename T>
+__device__ __forceinline__ void fwd_preload(DiagRegs<T> &dv, const DevSym &S, const T *__restrict__ slab,
+                                            const T *__restrict__ dinv, int64_t k, int stage_diag)
+{
+    if (dinv && S.inv_idx[k] >= 0)
+        diag_load(dv, dinv + (int64_t)S.inv_idx[k] * 4096, 4096);
+    else if (stage_diag)
+        diag_load(dv, slab + S.blk_off[S.diag_pos[k]], S.size[k] * S.size[k]);
+}
+
+// y_k <- D_k^{-1} acc for pivot k (acc: m x nrhs in shared memory). With an inverse (dinv
+// set, 64-row pivot): a product with the inverse held in `dv` -- thread t has
+// X(t mod 64, 4q + t / 64), q < 16 -- its four partial sums per row added in a fixed
+// order. Otherwise substitution with the LU factors, D_k staged in shared memory with an
+// odd row stride (column reads of the substitution hit distinct banks) when stage_diag,
+// from the registers `dv` filled by diag_load.
 template <typename T, typename V>
-__device__ void fwd_solve_store(const DevSym &S, const T *__restrict__ slab, V *__restrict__ yk, int64_t k, int nrhs,
-                                int stage_diag, unsigned char *smem_raw, V *acc, const DiagRegs<T> &dv)
+__device__ void fwd_solve_store(const DevSym &S, const T *__restrict__ slab, const T *__restrict__ dinv,
+                                V *__restrict__ yk, int64_t k, int nrhs, int stage_diag, unsigned char *smem_raw,
+                                V *acc, const DiagRegs<T> &dv)
 {
     const int m = S.size[k];
+    static_assert(kStageRegs * kThreads == 64 * 64, "one 64x64 inverse fills the finisher's registers");
+    if (dinv && S.inv_idx[k] >= 0)
+    {
+        __shared__ V s_part[kThreads];
+        const int tid = threadIdx.x, g = tid >> 6;
+        __syncthreads(); // acc is complete
+        for (int c = 0; c < nrhs; ++c)
+        {
+            V s = V(0);
+#pragma unroll
+            for (int q = 0; q < kStageRegs; ++q)
+                s += (V)dv.v[q] * acc[(4 * q + g) * nrhs + c];
+            s_part[tid] = s;
+            __syncthreads();
+            if (tid < 64)
+                yk[tid * nrhs + c] = (s_part[tid] + s_part[64 + tid]) + (s_part[128 + tid] + s_part[192 + tid]);
+            __syncthreads();
+        }
+        return;
+    }
     const T *gd = slab + S.blk_off[S.diag_pos[k]];
     const int mm = m * m, nt = blockDim.x, tid = threadIdx.x;
     const T *d = gd;
@@ -1387,7 +1468,8 @@ __device__ void fwd_solve_store(const DevSym &S, const T *__restrict__ slab, V *
 template <typename T, typename V>
 __global__ void __launch_bounds__(kThreads, 1)
     k_fwd_stage(DevSym S, const T *__restrict__ slab, V *__restrict__ y, V *__restrict__ scratch,
-                int *__restrict__ tickets, int64_t p0, int64_t p1, int nrhs, int stage_diag)
+                int *__restrict__ tickets, int64_t p0, int64_t p1, int nrhs, int stage_diag,
+                const T *__restrict__ dinv)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int64_t u = S.fwdu_pref[p0] + blockIdx.x;
@@ -1408,8 +1490,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     __shared__ __align__(16) V red[kThreads * 16 / sizeof(V)];
     DiagRegs<T> dv;
-    if (stage_diag)
-        diag_load(dv, slab + S.blk_off[S.diag_pos[k]], m * m);
+    fwd_preload(dv, S, slab, dinv, k, stage_diag);
     if (nparts > 1)
     {
         sum_partials(part, nparts - 1, E, part, red);
@@ -1418,7 +1499,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     V *acc = reinterpret_cast<V *>(smem_raw);
     V *yk = y + S.dof_off[k] * nrhs;
     combine_partials(acc, yk, nparts > 1 ? part : nullptr, nparts > 0 ? part + (nparts - 1) * E : nullptr, true, E);
-    fwd_solve_store(S, slab, yk, k, nrhs, stage_diag, smem_raw, acc, dv);
+    fwd_solve_store(S, slab, dinv, yk, k, nrhs, stage_diag, smem_raw, acc, dv);
 }
 
 // Backward stage: y_k -= sum_c U(k,c) y_c over the upper blocks of the stage's pivots
@@ -1594,7 +1675,7 @@ template <typename T, typename V>
 __global__ void __launch_bounds__(kThreads, 1)
     k_fwd_flow(DevSym S, const T *__restrict__ slab, V *__restrict__ y, V *__restrict__ scratch,
                int *__restrict__ tickets, int *__restrict__ flags, int *__restrict__ pflags, int tag, int64_t n_items,
-               int nrhs, int stage_diag, int *status)
+               int nrhs, int stage_diag, const T *__restrict__ dinv, int *status)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(16) V red[kThreads * 16 / sizeof(V)];
@@ -1612,10 +1693,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         DiagRegs<T> dv;
         if (nparts == 0)
         {
-            if (stage_diag)
-                diag_load(dv, gd, m * m);
+            fwd_preload(dv, S, slab, dinv, k, stage_diag);
             combine_partials(acc, yk, (const V *)nullptr, (const V *)nullptr, false, E);
-            fwd_solve_store(S, slab, yk, k, nrhs, stage_diag, smem_raw, acc, dv);
+            fwd_solve_store(S, slab, dinv, yk, k, nrhs, stage_diag, smem_raw, acc, dv);
             publish_flag(flags + k, tag);
             continue;
         }
@@ -1624,10 +1704,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int64_t blk = S.row_ptr[k] + local;
         const int32_t src = S.cols[blk];
         const int K = S.size[src];
-        if (local == 0 && !late && stage_diag) // the finisher will stage D_k: bring it into L2 now
-            prefetch_l2(gd, (int64_t)m * m);
-        if (late && stage_diag)
-            diag_load(dv, gd, m * m);
+        const bool inv = dinv && S.inv_idx[k] >= 0;
+        if (local == 0 && !late && (stage_diag || inv)) // the finisher will load D_k or its inverse: into L2 now
+            prefetch_l2(inv ? dinv + (int64_t)S.inv_idx[k] * 4096 : gd, inv ? (int64_t)4096 : (int64_t)m * m);
+        if (late)
+            fwd_preload(dv, S, slab, dinv, k, stage_diag);
         GemvRegs<T> g;
         gemv_load(g, slab + S.blk_off[blk], m, K);
         if (!wait_flag(flags + src, tag, status))
@@ -1649,7 +1730,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             return;
         __syncthreads(); // the late partial is in acc
         combine_partials(acc, yk, nparts > 1 ? (const V *)part : nullptr, (const V *)acc, false, E);
-        fwd_solve_store(S, slab, yk, k, nrhs, stage_diag, smem_raw, acc, dv);
+        fwd_solve_store(S, slab, dinv, yk, k, nrhs, stage_diag, smem_raw, acc, dv);
         publish_flag(flags + k, tag);
     }
 }

@@ -235,6 +235,15 @@ int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, co
     S.fwdu_pref.assign(n + 1, 0);
     S.fwd_rows.assign(n + 1, 0);
     S.bwd_rows.assign(n + 1, 0);
+    S.inv_idx.assign(n, -1);
+    S.inv_row.clear();
+    for (int64_t k = 0; k < n; ++k)
+        if (S.size[k] == 64)
+        {
+            S.inv_idx[k] = (int32_t)S.inv_row.size();
+            S.inv_row.push_back((int32_t)k);
+        }
+    S.n_inv = (int64_t)S.inv_row.size();
     double flops = 0;
     std::vector<double> piv_upd_flops(n), piv_upd_c(n), piv_upd_ab(n);
     for (int64_t p = 0; p < n; ++p)
