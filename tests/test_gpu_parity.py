@@ -351,6 +351,26 @@ def test_dataflow_solve_matches_staged(gpu, n, p, nrhs, prec):
     assert rel_err(x_flow, osys.solve(bn)) < (TOL_X if prec == 0 else TOL_X_MIXED)
 
 
+@pytest.mark.parametrize("umma", [True, False])
+def test_mixed_inner_solve_with_diagonal_inverses(gpu, umma):
+    """The mixed form's FP32 solve applies explicit inverses of the 64x64 diagonal blocks:
+    unrefined it is already close to the FP64 solution, and one refinement step reaches
+    1e-12, as with substitution."""
+    mat, b = _mesh(10, 8, seed=29)
+    order, pm, ns = _native_from(gpu, mat)
+    bn = reorder_rhs(mat.sizes, order, b)
+    ns.decompose(gpu.FP64)
+    x64, _ = ns.solve(bn)
+    ns.set_tensor_core_mixed(umma)
+    ns.set_values(pm.vals)
+    ns.decompose(gpu.MIXED)
+    x0, info0 = ns.solve(bn, max_iter=0)
+    assert rel_err(x0, x64) < 1e-4
+    x1, info1 = ns.solve(bn)
+    assert info1["converged"] and info1["iterations"] <= 2
+    assert info1["relative_residual"] <= 1e-12 and rel_err(x1, x64) < TOL_X_MIXED
+
+
 @pytest.mark.parametrize("prec", [0, 1])
 def test_uneven_orders_large_pivot_grids(gpu, prec):
     """64x64 mesh with per-element orders 2..10: pivots of 33-64 rows take the padded fused
