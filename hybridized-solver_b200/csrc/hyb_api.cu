@@ -489,6 +489,17 @@ template <typename T> int enqueue_update(hyb_system *h, T *slab, int64_t l, cuda
             return HYB_SUCCESS;
         }
     }
+    if (std::max(sh.max_row, sh.max_col) <= 8 * hyb::kSmallTile)
+    {
+        // 64-thread CTAs of one 32x32 tile each (grid.y: the tiles of the largest target)
+        const unsigned t32 = (unsigned)(((sh.max_row + hyb::kSmallTile - 1) / hyb::kSmallTile) *
+                                        ((sh.max_col + hyb::kSmallTile - 1) / hyb::kSmallTile));
+        hyb::k_update32<T><<<dim3((unsigned)nu, t32), hyb::kSmallThreads, 0, st>>>(ds, slab, p0, p1, mode, sh.la_i0,
+                                                                                  sh.la_j0);
+        ++launches;
+        HYB_LAUNCHED("k_update32", l);
+        return HYB_SUCCESS;
+    }
     // one CTA per target block, looping over its 64x64 tiles
     hyb::k_update<T><<<(unsigned)nu, hyb::kThreads, 0, st>>>(ds, slab, p0, p1, mode, sh.la_i0, sh.la_j0);
     ++launches;
@@ -1104,6 +1115,8 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
             allow_smem(hyb::k_split64, 0),
             allow_smem(hyb::k_update<double>, 0),
             allow_smem(hyb::k_update<float>, 0),
+            allow_smem(hyb::k_update32<double>, 0),
+            allow_smem(hyb::k_update32<float>, 0),
         };
         for (cudaError_t e : errs)
             if (e != cudaSuccess)

@@ -694,6 +694,101 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
 }
 
+// Small-tile form of k_update for levels of uneven block sizes: 64 threads and one 32x32
+// output tile per CTA (grid.y: the tiles of a target block; CTAs past a block's last tile
+// return), so the tiles of one target run side by side and a 6x10 target no longer holds
+// a 256-thread CTA. Every element is C - sum_k A(i,k) B(k,j) with one FMA per term in
+// ascending k (K in 16-wide chunks; the zero terms past K are exact no-ops), as in
+// k_update: both kernels give the same bits.
+constexpr int kSmallTile = 32;
+constexpr int kSmallThreads = 64;
+constexpr int kSmallKC = 16;
+template <typename T>
+__global__ void __launch_bounds__(kSmallThreads, 8)
+    k_update32(DevSym S, T *__restrict__ slab, int64_t p0, int64_t p1, int mode, int i0, int j0)
+{
+    constexpr int TL = kSmallTile, NT = kSmallThreads, TPR = TL / 4, KC = kSmallKC, LDA = TL + 1;
+    constexpr int kPer = TL * KC / NT; // chunk values per thread, each of A and B
+    __shared__ __align__(16) T sa[KC * LDA];
+    __shared__ __align__(16) T sb[KC * TL];
+    const UpdUnit w = update_unit(S, p0, p1, mode, i0, j0);
+    const int64_t k = w.k, li = w.li, bu = w.bu;
+    const int32_t t = S.lcol_row[li];
+    const int32_t c = S.cols[bu];
+    const int M = S.size[t], N = S.size[c], K = S.size[k];
+    const int tn = (N + TL - 1) / TL, tm = (M + TL - 1) / TL;
+    if ((int)blockIdx.y >= tm * tn)
+        return;
+    const int r0 = ((int)blockIdx.y / tn) * TL, c0 = ((int)blockIdx.y % tn) * TL;
+    const int Mr = M - r0, Nr = N - c0;
+    const int64_t tgt = warp_find_col(S.cols, S.row_ptr[t], S.row_ptr[t + 1], c);
+    T *cb = slab + S.blk_off[tgt] + (int64_t)r0 * N + c0;
+    const T *a = slab + S.blk_off[S.lcol_blk[li]] + (int64_t)r0 * K;
+    const T *b = slab + S.blk_off[bu] + c0;
+    const int tid = threadIdx.x, ty = tid / TPR, tx = tid % TPR;
+    T acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            const int r = ty * 4 + i, cc = tx + TPR * j;
+            acc[i][j] = (r < Mr && cc < Nr) ? cb[r * N + cc] : T(0);
+        }
+    T ra[kPer], rb[kPer];
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int q = 0; q < kPer; ++q)
+        {
+            const int idx = q * NT + tid;
+            const int r = idx / KC, kk = idx % KC; // A: rows of KC along K
+            ra[q] = (r < Mr && k0 + kk < K) ? a[(int64_t)r * K + k0 + kk] : T(0);
+            const int kr = idx / TL, cc = idx % TL; // B: rows of TL along N
+            rb[q] = (cc < Nr && k0 + kr < K) ? b[(int64_t)(k0 + kr) * N + cc] : T(0);
+        }
+    };
+    load(0);
+    for (int k0 = 0; k0 < K; k0 += KC)
+    {
+#pragma unroll
+        for (int q = 0; q < kPer; ++q)
+        {
+            const int idx = q * NT + tid;
+            sa[(idx % KC) * LDA + idx / KC] = ra[q];
+            sb[idx] = rb[q];
+        }
+        __syncthreads();
+        if (k0 + KC < K)
+            load(k0 + KC);
+#pragma unroll 8
+        for (int kk = 0; kk < KC; ++kk)
+        {
+            T av[4], bv[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                av[i] = sa[kk * LDA + ty * 4 + i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                bv[j] = sb[kk * TL + tx + TPR * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    acc[i][j] -= av[i] * bv[j];
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            const int r = ty * 4 + i, cc = tx + TPR * j;
+            if (r < Mr && cc < Nr)
+                cb[r * N + cc] = acc[i][j];
+        }
+}
+
 // ----------------------------------------------------------------------------------
 // Bulk async copies (the non-tensor TMA path) into shared memory, completed on an
 // mbarrier. Waits are bounded in time: a wait that runs out records ST_TIMEOUT and the CTA
