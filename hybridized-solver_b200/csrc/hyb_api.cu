@@ -320,7 +320,7 @@ template <typename T> int lu_smem_bytes(int m)
 
 template <typename T> int trsm_smem_bytes(int m)
 {
-    return (m * m + m * hyb::kTile) * (int)sizeof(T);
+    return (m * (m | 1) + m * (hyb::kTile | 1)) * (int)sizeof(T); // odd row strides (k_trsm)
 }
 
 // LU of the diagonal blocks of level l and the solves of their rows' upper blocks.

@@ -233,6 +233,48 @@ __device__ void lu_solve_strip(const T *d, int ldd, T *b, int ldb, int m, int w)
     }
 }
 
+// lu_solve_strip without CTA barriers, for a strip in shared memory: lane 4j + s of a warp
+// takes column 8 warp + j (and every 8 nw-th after it) and, of that column, the rows
+// r = s (mod 4). The four lanes of a column meet at __syncwarp before each step reads the
+// row the step before finished. Each element sees the same operations in the same order as
+// in lu_solve_strip, so both give the same bits.
+template <typename T>
+__device__ void lu_solve_strip_warp(const T *d, int ldd, T *b, int ldb, int m, int w)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int s = lane & 3;
+    for (int cb = warp * 8; cb < w; cb += nw * 8) // warp-uniform
+    {
+        const int c = cb + (lane >> 2);
+        const bool on = c < w;
+        T *col = b + c;
+        for (int i = 0; i < m - 1; ++i) // unit lower
+        {
+            __syncwarp();
+            if (on)
+            {
+                const T bi = col[i * ldb];
+                for (int r = i + 1 + ((s - i - 1) & 3); r < m; r += 4)
+                    col[r * ldb] -= d[r * ldd + i] * bi;
+            }
+        }
+        for (int i = m - 1; i >= 0; --i) // upper with the diagonal
+        {
+            __syncwarp();
+            if (on && s == (i & 3))
+                col[i * ldb] = col[i * ldb] / d[i * ldd + i];
+            __syncwarp();
+            if (on)
+            {
+                const T bi = col[i * ldb];
+                for (int r = s; r < i; r += 4)
+                    col[r * ldb] -= d[r * ldd + i] * bi;
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // grid.x: upper blocks of the level's pivots, grid.y: 64-column strips.
 template <typename T, bool kShared>
 __global__ void __launch_bounds__(kThreads) k_trsm(DevSym S, T *__restrict__ slab, int64_t p0, int64_t p1)
@@ -252,16 +294,19 @@ __global__ void __launch_bounds__(kThreads) k_trsm(DevSym S, T *__restrict__ sla
     T *gb = slab + S.blk_off[blk] + c0;
     if constexpr (kShared)
     {
+        // odd row strides: the rows a warp touches at once sit in different banks
+        const int ldd = m | 1, ldb = w | 1;
         T *d = reinterpret_cast<T *>(smem_raw);
-        T *b = d + m * m;
+        T *b = d + m * ldd;
         for (int i = threadIdx.x; i < m * m; i += blockDim.x)
-            d[i] = gd[i];
+            d[(i / m) * ldd + i % m] = gd[i];
         for (int i = threadIdx.x; i < m * w; i += blockDim.x)
-            b[i] = gb[(i / w) * nc + i % w];
+            b[(i / w) * ldb + i % w] = gb[(i / w) * nc + i % w];
         __syncthreads();
-        lu_solve_strip(d, m, b, w, m, w);
+        lu_solve_strip_warp(d, ldd, b, ldb, m, w);
+        __syncthreads();
         for (int i = threadIdx.x; i < m * w; i += blockDim.x)
-            gb[(i / w) * nc + i % w] = b[i];
+            gb[(i / w) * nc + i % w] = b[(i / w) * ldb + i % w];
     }
     else
     {
