@@ -578,7 +578,6 @@ template <typename T> int enqueue_factor(hyb_system *h, T *slab, uint64_t &launc
     return HYB_SUCCESS;
 }
 
-// Forward + backward substitution of y (type V, dof x nrhs) with the factors in `slab`.
 // The FP32 diagonal inverses a solve with factors of type T uses (mixed form only).
 template <typename T> const T *solve_dinv(const hyb_system *h)
 {
@@ -588,6 +587,7 @@ template <typename T> const T *solve_dinv(const hyb_system *h)
         return nullptr;
 }
 
+// Forward + backward substitution of y (type V, dof x nrhs) with the factors in `slab`.
 template <typename T, typename V> int enqueue_solve(hyb_system *h, const T *slab, V *y, V *scratch, int nrhs,
                                                     uint64_t &launches)
 {
