@@ -526,6 +526,11 @@ def run_ours(args):
         "k_update64_tc (tcgen05 split-BF16, persistent, bulk-copy C ring)",
         traffic_per_block=TC_DRAM_BYTES_PER_TARGET_BLOCK,
     )
+    if rf64 is not None:
+        rf64["traffic_note"] = (
+            "null: the FP64 update's DRAM bytes were captured only at 32x32 (profiles/k_update64_f64_mesh32_p8.md), "
+            "where a stage's targets stay in L2; the bound here is the FP64 tensor pipe, not DRAM"
+        )
     if rmix is not None:
         rmix["traffic_note"] = (
             "dram__bytes_read.sum + dram__bytes_write.sum of one stage (both launches) from a 1-pass ncu capture "
