@@ -1,1 +1,2 @@
-"""B200-specific additions: the raw C ABI (``native``) and synthetic mesh systems (``meshgen``)."""
+"""B200-specific additions: the raw C ABI (``native``), synthetic mesh systems (``meshgen``) and
+many independent systems on one device handle (``batch``)."""

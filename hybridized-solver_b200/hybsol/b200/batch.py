@@ -1,0 +1,104 @@
+"""Many independent block systems factored and solved together on one device handle.
+
+The systems are stacked block-diagonally and ordered with the reference's coloring on the
+union. First-fit coloring visits blocks in index order and a block's colour depends only
+on the blocks of its own system, and ``order_from_colors`` sorts stably by colour, so every
+system keeps exactly the relative order it would get alone (and hence its own factors).
+Pivots of different systems then share elimination stages, and with them kernel launches,
+which is what makes many small systems cheap.
+
+``BatchLayout`` is the host-side part (stacking, ordering, moving vectors in and out);
+``BatchedSystem`` adds the device handle.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import meshgen, native
+
+
+def dof_permutation(sizes, order) -> np.ndarray:
+    """``p`` with ``x_new[p] = x_old`` when old block ``i`` becomes block ``order[i]``
+    (the renumbering of ``BlockMatrix.permuted`` and of the reference's ``reorder_blocks``)."""
+    sizes = np.asarray(sizes, dtype=np.int64)
+    order = np.asarray(order, dtype=np.int64)
+    new_sizes = np.empty_like(sizes)
+    new_sizes[order] = sizes
+    off_old = np.concatenate([[0], np.cumsum(sizes)])
+    off_new = np.concatenate([[0], np.cumsum(new_sizes)])
+    block_of = np.repeat(np.arange(len(sizes)), sizes)
+    within = np.arange(off_old[-1]) - off_old[block_of]
+    return off_new[order[block_of]] + within
+
+
+class BatchLayout:
+    """Stacked, reordered form of independent systems (``meshgen.BlockMatrix`` each)."""
+
+    def __init__(self, systems, strategy: str = "first"):
+        self.systems = list(systems)
+        if not self.systems:
+            raise ValueError("no systems to batch")
+        stacked = meshgen.block_diagonal(self.systems)
+        self.order = native.compute_ordering(stacked.row_ptr, stacked.cols, strategy).astype(np.int64)
+        self.matrix = stacked.permuted(self.order)
+        self.perm = dof_permutation(stacked.sizes, self.order)
+        self.dof_off = np.concatenate([[0], np.cumsum([m.dof for m in self.systems])]).astype(np.int64)
+        self.block_off = np.concatenate([[0], np.cumsum([m.n_blocks for m in self.systems])]).astype(np.int64)
+
+    @property
+    def count(self) -> int:
+        return len(self.systems)
+
+    def to_solver(self, rhs) -> np.ndarray:
+        """One right-hand side per system (``(dof_i,)`` or ``(dof_i, k)``, the same k for all)
+        -> the stacked vector in the solver's block order."""
+        if len(rhs) != self.count:
+            raise ValueError(f"expected {self.count} right-hand sides, got {len(rhs)}")
+        parts = [np.asarray(r, dtype=np.float64) for r in rhs]
+        for i, r in enumerate(parts):
+            if r.shape[0] != self.dof_off[i + 1] - self.dof_off[i]:
+                raise ValueError(f"right-hand side {i} has {r.shape[0]} rows, its system {self.dof_off[i + 1] - self.dof_off[i]}")
+        b = np.concatenate(parts)
+        out = np.empty_like(b)
+        out[self.perm] = b
+        return out
+
+    def from_solver(self, x) -> list:
+        """The solver's stacked solution -> one solution per system."""
+        y = np.asarray(x)[self.perm]
+        return [y[self.dof_off[i] : self.dof_off[i + 1]] for i in range(self.count)]
+
+    def values(self, systems) -> np.ndarray:
+        """New values for the same patterns, in the solver's order (for a refactorization)."""
+        systems = list(systems)
+        if len(systems) != self.count:
+            raise ValueError(f"expected {self.count} systems, got {len(systems)}")
+        for a, b in zip(systems, self.systems):
+            if not (
+                np.array_equal(a.sizes, b.sizes) and np.array_equal(a.row_ptr, b.row_ptr) and np.array_equal(a.cols, b.cols)
+            ):
+                raise ValueError("a system's block pattern differs from the batch's")
+        return meshgen.block_diagonal(systems).permuted(self.order).vals
+
+
+class BatchedSystem:
+    """Independent systems factored and solved on one device handle (see the module text)."""
+
+    def __init__(self, systems, strategy: str = "first"):
+        self.layout = BatchLayout(systems, strategy)
+        self.native = native.NativeSystem.from_matrix(self.layout.matrix)
+
+    def set_values(self, systems):
+        self.native.set_values(self.layout.values(systems))
+
+    def decompose(self, precision: int = native.FP64) -> dict:
+        return self.native.decompose(precision)
+
+    def solve(self, rhs, tol: float = 1e-12, max_iter: int = 50):
+        """Solve every system for its right-hand side; returns (solutions, info)."""
+        x, info = self.native.solve(self.layout.to_solver(rhs), tol=tol, max_iter=max_iter)
+        return self.layout.from_solver(x), info
+
+    def close(self):
+        self.native.close()

@@ -1,0 +1,117 @@
+"""Independent systems batched into one handle (hybsol.b200.batch).
+
+CPU: the host layout -- the stacked system ordered with the reference's coloring keeps each
+system's own relative order, and vectors moved in and out through the layout give, with the
+oracle solving the stacked system, each system's own solution. GPU: the device path against
+one handle per system.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import rel_err, reorder_rhs
+from oracle import oracle as O
+
+SPECS = [(3, 3), (5, 4), (4, 6), (2, 5), (3, 8)]
+
+
+def _systems(nrhs=1):
+    from hybsol.b200 import meshgen
+
+    mats, rhs = [], []
+    for k, (side, p) in enumerate(SPECS):
+        m, b = meshgen.mesh_system(side, p, seed=40 + k, nrhs=nrhs)
+        mats.append(m)
+        rhs.append(b)
+    return mats, rhs
+
+
+def test_dof_permutation_matches_block_moves(native):
+    from hybsol.b200 import batch
+
+    rng = np.random.default_rng(3)
+    sizes = rng.integers(1, 7, 23)
+    order = rng.permutation(23)
+    b = rng.standard_normal(int(sizes.sum()))
+    p = batch.dof_permutation(sizes, order)
+    moved = np.empty_like(b)
+    moved[p] = b
+    assert np.array_equal(moved, reorder_rhs(sizes, order, b))
+    assert np.array_equal(np.sort(p), np.arange(len(b)))
+
+
+def test_layout_keeps_each_system_order(native):
+    from hybsol.b200 import batch
+
+    mats, _ = _systems()
+    lay = batch.BatchLayout(mats)
+    for i, m in enumerate(mats):
+        own = native.compute_ordering(m.row_ptr, m.cols, "first").astype(np.int64)
+        sub = lay.order[lay.block_off[i] : lay.block_off[i + 1]]
+        assert np.array_equal(np.argsort(sub, kind="stable"), np.argsort(own, kind="stable"))
+
+
+@pytest.mark.parametrize("nrhs", [1, 2])
+def test_layout_round_trip_with_oracle(native, nrhs):
+    from hybsol.b200 import batch
+
+    mats, rhs = _systems(nrhs)
+    lay = batch.BatchLayout(mats)
+    big = O.OracleSystem.from_csr(lay.matrix.sizes, lay.matrix.row_ptr, lay.matrix.cols, lay.matrix.vals)
+    big.decompose()
+    parts = lay.from_solver(big.solve(lay.to_solver(rhs)))
+    for m, b, x in zip(mats, rhs, parts):
+        order = native.compute_ordering(m.row_ptr, m.cols, "first").astype(np.int64)
+        pm = m.permuted(order)
+        alone = O.OracleSystem.from_csr(pm.sizes, pm.row_ptr, pm.cols, pm.vals)
+        alone.decompose()
+        xs = alone.solve(reorder_rhs(m.sizes, order, b))
+        inv = np.argsort(order)
+        assert rel_err(x, reorder_rhs(pm.sizes, inv, xs)) < 1e-13
+        assert rel_err(m.matvec(x), b) < 1e-12
+
+
+def test_layout_rejects_mismatches(native):
+    from hybsol.b200 import batch, meshgen
+
+    mats, rhs = _systems()
+    lay = batch.BatchLayout(mats)
+    with pytest.raises(ValueError):
+        lay.to_solver(rhs[:-1])
+    with pytest.raises(ValueError):
+        lay.to_solver([rhs[1]] + rhs[1:])
+    other, _ = meshgen.mesh_system(3, 2, seed=1)
+    with pytest.raises(ValueError):
+        lay.values([other] + mats[1:])
+    with pytest.raises(ValueError):
+        batch.BatchLayout([])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [0, 1])
+def test_batched_system_matches_single_handles(gpu, prec):
+    from hybsol.b200 import batch
+
+    mats, rhs = _systems(nrhs=2)
+    bs = batch.BatchedSystem(mats)
+    bs.decompose(prec)
+    xs, info = bs.solve(rhs)
+    assert info["converged"]
+    for m, b, x in zip(mats, rhs, xs):
+        order = gpu.compute_ordering(m.row_ptr, m.cols, "first").astype(np.int64)
+        pm = m.permuted(order)
+        ns = gpu.NativeSystem.from_matrix(pm)
+        ns.decompose(gpu.FP64)
+        x1, _ = ns.solve(reorder_rhs(m.sizes, order, b))
+        ns.close()
+        assert rel_err(x, reorder_rhs(pm.sizes, np.argsort(order), x1)) < (1e-12 if prec == 0 else 1e-11)
+    # refactorization with new values through the layout
+    scaled = [type(m)(m.sizes, m.row_ptr, m.cols, m.val_ptr, 2.0 * m.vals) for m in mats]
+    bs.set_values(scaled)
+    bs.decompose(prec)
+    xs2, _ = bs.solve(rhs)
+    for x, x2 in zip(xs, xs2):
+        assert rel_err(2.0 * x2, x) < (1e-12 if prec == 0 else 1e-11)
+    bs.close()
