@@ -8,7 +8,9 @@ Pivots of different systems then share elimination stages, and with them kernel 
 which is what makes many small systems cheap.
 
 ``BatchLayout`` is the host-side part (stacking, ordering, moving vectors in and out);
-``BatchedSystem`` adds the device handle.
+``BatchedSystem`` adds the device handle. When the systems' factors exceed one device,
+``plan_waves`` packs them into waves under a byte budget (from the exact symbolic fill of
+each system) and ``solve_many`` runs the waves one after another.
 """
 
 from __future__ import annotations
@@ -102,3 +104,61 @@ class BatchedSystem:
 
     def close(self):
         self.native.close()
+
+
+def device_bytes(system, precision: int = native.FP64, strategy: str = "first") -> int:
+    """Device memory one system needs on a handle: its factor slab (FP64, or FP32 for the
+    mixed form) from the exact symbolic fill under the reference's ordering, the original
+    FP64 values, and the solve vectors; an estimate of the handle's footprint, not a bound
+    on the allocator's."""
+    order = native.compute_ordering(system.row_ptr, system.cols, strategy).astype(np.int64)
+    pm = system.permuted(order)
+    a = native.analyze(pm.sizes, pm.row_ptr, pm.cols)
+    slab = int(a["slab_bytes_fp64"]) // (2 if precision == native.MIXED else 1)
+    inv = 16384 * int(np.count_nonzero(np.asarray(system.sizes) == 64)) if precision == native.MIXED else 0
+    return slab + 8 * len(system.vals) + 64 * int(system.dof) + inv
+
+
+def plan_waves(weights, budget: int) -> list:
+    """Indices of systems per wave: largest first, each into the first wave with room
+    (first-fit decreasing); a system larger than the budget gets a wave of its own.
+    Waves and their indices are in ascending order, so every caller gets the same plan."""
+    if budget <= 0:
+        raise ValueError("budget must be positive")
+    w = [int(x) for x in weights]
+    order = sorted(range(len(w)), key=lambda i: (-w[i], i))
+    waves, room = [], []
+    for i in order:
+        for k in range(len(waves)):
+            if w[i] <= room[k]:
+                waves[k].append(i)
+                room[k] -= w[i]
+                break
+        else:
+            waves.append([i])
+            room.append(budget - w[i])
+    waves = [sorted(v) for v in waves]
+    waves.sort(key=lambda v: v[0])
+    return waves
+
+
+def solve_many(systems, rhs, budget: int, precision: int = native.FP64, tol: float = 1e-12, max_iter: int = 50):
+    """Factor and solve independent systems in waves of at most ``budget`` device bytes
+    (``plan_waves`` on ``device_bytes``); returns (solutions in input order, per-wave infos)."""
+    systems = list(systems)
+    if len(rhs) != len(systems):
+        raise ValueError(f"expected {len(systems)} right-hand sides, got {len(rhs)}")
+    waves = plan_waves([device_bytes(m, precision) for m in systems], budget)
+    out = [None] * len(systems)
+    infos = []
+    for wave in waves:
+        bs = BatchedSystem([systems[i] for i in wave])
+        try:
+            bs.decompose(precision)
+            xs, info = bs.solve([rhs[i] for i in wave], tol=tol, max_iter=max_iter)
+        finally:
+            bs.close()
+        for i, x in zip(wave, xs):
+            out[i] = x
+        infos.append(info)
+    return out, infos

@@ -115,3 +115,51 @@ def test_batched_system_matches_single_handles(gpu, prec):
     for x, x2 in zip(xs, xs2):
         assert rel_err(2.0 * x2, x) < (1e-12 if prec == 0 else 1e-11)
     bs.close()
+
+
+def test_plan_waves_properties():
+    from hybsol.b200 import batch
+
+    rng = np.random.default_rng(7)
+    w = rng.integers(1, 100, 40)
+    budget = 150
+    waves = batch.plan_waves(w, budget)
+    flat = sorted(i for v in waves for i in v)
+    assert flat == list(range(40))
+    assert all(sum(int(w[i]) for i in v) <= budget for v in waves)
+    assert waves == batch.plan_waves(list(w), budget)  # deterministic
+    assert waves == sorted(waves, key=lambda v: v[0]) and all(v == sorted(v) for v in waves)
+    # a system above the budget gets a wave of its own
+    big = batch.plan_waves([5, 500, 5], 100)
+    assert [1] in big and sorted(i for v in big for i in v) == [0, 1, 2]
+    with pytest.raises(ValueError):
+        batch.plan_waves([1], 0)
+
+
+def test_device_bytes_from_the_symbolic_fill(native):
+    from hybsol.b200 import batch, meshgen
+
+    m, _ = meshgen.mesh_system(4, 4, seed=1)
+    order = native.compute_ordering(m.row_ptr, m.cols, "first").astype(np.int64)
+    pm = m.permuted(order)
+    slab = native.analyze(pm.sizes, pm.row_ptr, pm.cols)["slab_bytes_fp64"]
+    b64 = batch.device_bytes(m, native.FP64)
+    b32 = batch.device_bytes(m, native.MIXED)
+    assert b64 == slab + 8 * len(m.vals) + 64 * m.dof
+    assert b32 == slab // 2 + 8 * len(m.vals) + 64 * m.dof  # no 64-row blocks at p=4
+    m8, _ = meshgen.mesh_system(2, 8, seed=1)
+    assert batch.device_bytes(m8, native.MIXED) > batch.device_bytes(m8, native.FP64) // 2
+
+
+@pytest.mark.gpu
+def test_solve_many_in_waves(gpu):
+    from hybsol.b200 import batch
+
+    mats, rhs = _systems()
+    sizes = [batch.device_bytes(m) for m in mats]
+    budget = max(sizes) + min(sizes)  # forces several waves
+    assert len(batch.plan_waves(sizes, budget)) > 1
+    xs, infos = batch.solve_many(mats, rhs, budget)
+    assert len(infos) == len(batch.plan_waves(sizes, budget))
+    for m, b, x in zip(mats, rhs, xs):
+        assert rel_err(m.matvec(x), b) < 1e-12
