@@ -464,6 +464,36 @@ static void bs_dealloc(PyObject *obj)
 /* ------------------------------------------------------------------------------- */
 /* assembly and accessors                                                          */
 
+/* Adds block (r, c) with row-major values `src` to the host rows: summed into a block already
+ * present (block_system_add_block, src/blocks.c:36-45), else inserted in column order.
+ * Returns -1 with RuntimeError set when memory runs out. */
+static int host_add(bs_object *s, uint64_t r, uint64_t c, const double *src)
+{
+    const uint64_t nv = bsize(s, r) * bsize(s, c);
+    hrow_t *row = s->rows + r;
+    const uint64_t p = row_find_geq(row, c);
+    if (p < row->count && row->e[p].col == c)
+    {
+        double *dst = row->e[p].vals;
+        for (uint64_t i = 0; i < nv; ++i)
+            dst[i] += src[i];
+        return 0;
+    }
+    double *vals = (double *)PyMem_RawMalloc(nv * sizeof(double));
+    if (!vals || row_reserve(row, row->count + 1) < 0)
+    {
+        PyMem_RawFree(vals);
+        PyErr_SetString(PyExc_RuntimeError, "Failed to add block to block system.");
+        return -1;
+    }
+    memcpy(vals, src, nv * sizeof(double));
+    memmove(row->e + p + 1, row->e + p, (row->count - p) * sizeof(entry_t));
+    row->e[p].col = c;
+    row->e[p].vals = vals;
+    row->count += 1;
+    return 0;
+}
+
 static PyObject *bs_add_block(PyObject *self, PyTypeObject *cls, PyObject *const *args, Py_ssize_t nargs,
                               PyObject *kwnames)
 {
@@ -480,34 +510,91 @@ static PyObject *bs_add_block(PyObject *self, PyTypeObject *cls, PyObject *const
     PyArrayObject *arr = as_block(val, bsize(s, r), bsize(s, c), "val");
     if (!arr)
         return NULL;
-    const uint64_t nv = bsize(s, r) * bsize(s, c);
-    const double *src = (const double *)PyArray_DATA(arr);
-    hrow_t *row = s->rows + r;
-    const uint64_t p = row_find_geq(row, (uint64_t)c);
-    if (p < row->count && row->e[p].col == (uint64_t)c)
+    const int rc = host_add(s, (uint64_t)r, (uint64_t)c, (const double *)PyArray_DATA(arr));
+    Py_DECREF(arr);
+    if (rc < 0)
+        return NULL;
+    Py_RETURN_NONE;
+}
+
+/* A 1-D int64 C-contiguous array from an integer array-like. */
+static PyArrayObject *as_index_array(PyObject *obj, const char *name)
+{
+    PyArrayObject *a = (PyArrayObject *)PyArray_FROM_O(obj);
+    if (!a)
+        return NULL;
+    if (PyArray_NDIM(a) != 1 || (!PyArray_ISINTEGER(a) && PyArray_SIZE(a) != 0))
     {
-        /* A block already present is summed into (block_system_add_block, src/blocks.c:36-45). */
-        double *dst = row->e[p].vals;
-        for (uint64_t i = 0; i < nv; ++i)
-            dst[i] += src[i];
-        Py_DECREF(arr);
-        Py_RETURN_NONE;
-    }
-    double *vals = (double *)PyMem_RawMalloc(nv * sizeof(double));
-    if (!vals || row_reserve(row, row->count + 1) < 0)
-    {
-        PyMem_RawFree(vals);
-        Py_DECREF(arr);
-        PyErr_SetString(PyExc_RuntimeError, "Failed to add block to block system.");
+        PyErr_Format(PyExc_ValueError, "Array %s must be a 1-D array of integers.", name);
+        Py_DECREF(a);
         return NULL;
     }
-    memcpy(vals, src, nv * sizeof(double));
-    Py_DECREF(arr);
-    memmove(row->e + p + 1, row->e + p, (row->count - p) * sizeof(entry_t));
-    row->e[p].col = (uint64_t)c;
-    row->e[p].vals = vals;
-    row->count += 1;
-    Py_RETURN_NONE;
+    PyArrayObject *out = (PyArrayObject *)PyArray_FROMANY((PyObject *)a, NPY_INT64, 1, 1,
+                                                          NPY_ARRAY_C_CONTIGUOUS | NPY_ARRAY_ALIGNED | NPY_ARRAY_FORCECAST);
+    Py_DECREF(a);
+    return out;
+}
+
+/* Bulk form of add_block (no counterpart in the reference): block i is (rows[i], cols[i])
+ * with its row-major values next in the 1-D `values`. Everything is checked before the
+ * first block is added; blocks are then added in order, so repeated positions are summed
+ * exactly as by successive add_block calls. */
+static PyObject *bs_add_blocks(PyObject *self, PyTypeObject *cls, PyObject *const *args, Py_ssize_t nargs,
+                               PyObject *kwnames)
+{
+    bs_object *s = check_self(self, cls);
+    if (!s || ensure_not_decomposed(s) < 0)
+        return NULL;
+    PyObject *orows, *ocols, *ovals;
+    const argspec_t spec[] = {{ARG_OBJECT, "rows", &orows, 0, 0},
+                              {ARG_OBJECT, "cols", &ocols, 0, 0},
+                              {ARG_OBJECT, "values", &ovals, 0, 0},
+                              {0}};
+    if (parse_args(args, nargs, kwnames, spec) < 0)
+        return NULL;
+    PyArrayObject *ar = as_index_array(orows, "rows");
+    PyArrayObject *ac = ar ? as_index_array(ocols, "cols") : NULL;
+    PyArrayObject *av =
+        ac ? (PyArrayObject *)PyArray_FROMANY(ovals, NPY_DOUBLE, 1, 1, NPY_ARRAY_C_CONTIGUOUS | NPY_ARRAY_ALIGNED) : NULL;
+    PyObject *result = NULL;
+    if (!av)
+        goto done;
+    const npy_intp nb = PyArray_DIM(ar, 0);
+    if (PyArray_DIM(ac, 0) != nb)
+    {
+        PyErr_Format(PyExc_ValueError, "Arrays rows and cols have %zd and %zd entries.", (Py_ssize_t)nb,
+                     (Py_ssize_t)PyArray_DIM(ac, 0));
+        goto done;
+    }
+    const int64_t *rr = (const int64_t *)PyArray_DATA(ar), *cc = (const int64_t *)PyArray_DATA(ac);
+    uint64_t total = 0;
+    for (npy_intp i = 0; i < nb; ++i)
+    {
+        if (check_index(s->n, (Py_ssize_t)rr[i], "Row index") < 0 || check_index(s->n, (Py_ssize_t)cc[i], "Column index") < 0)
+            goto done;
+        total += bsize(s, (uint64_t)rr[i]) * bsize(s, (uint64_t)cc[i]);
+    }
+    if ((uint64_t)PyArray_DIM(av, 0) != total)
+    {
+        PyErr_Format(PyExc_ValueError, "Array values has %zd entries, the blocks need %" PRIu64 ".",
+                     (Py_ssize_t)PyArray_DIM(av, 0), total);
+        goto done;
+    }
+    const double *v = (const double *)PyArray_DATA(av);
+    for (npy_intp i = 0; i < nb; ++i)
+    {
+        const uint64_t r = (uint64_t)rr[i], c = (uint64_t)cc[i];
+        if (host_add(s, r, c, v) < 0)
+            goto done;
+        v += bsize(s, r) * bsize(s, c);
+    }
+    result = Py_None;
+    Py_INCREF(result);
+done:
+    Py_XDECREF(ar);
+    Py_XDECREF(ac);
+    Py_XDECREF(av);
+    return result;
 }
 
 static PyObject *bs_is_valid(PyObject *self, PyTypeObject *cls, PyObject *const *Py_UNUSED(args), Py_ssize_t nargs,
@@ -1716,6 +1803,10 @@ static PyMethodDef bs_methods[] = {
     METH("add_block", bs_add_block,
          "add_block(row: int, col: int, val: numpy.typing.ArrayLike)\nAdd a block to the system (summed into an "
          "existing block)."),
+    METH("add_blocks", bs_add_blocks,
+         "add_blocks(rows: numpy.typing.ArrayLike, cols: numpy.typing.ArrayLike, values: numpy.typing.ArrayLike)\n"
+         "Add many blocks: block i is (rows[i], cols[i]) with its row-major values next in the 1-D values "
+         "(summed into existing blocks, in order). Not in the reference: a bulk form of add_block."),
     METH("is_valid", bs_is_valid, "is_valid() -> bool\nCheck if the system has symmetric sparsity and has diagonal blocks."),
     METH("as_array", bs_as_array, "as_array() -> numpy.typing.NDArray[numpy.double]\nReturn the system as a full matrix."),
     METH("get_row_block_indices", bs_get_row_block_indices,
