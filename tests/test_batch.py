@@ -163,3 +163,22 @@ def test_solve_many_in_waves(gpu):
     assert len(infos) == len(batch.plan_waves(sizes, budget))
     for m, b, x in zip(mats, rhs, xs):
         assert rel_err(m.matvec(x), b) < 1e-12
+
+
+def test_batched_systems_share_stages(native):
+    """The stacked system has as many elimination stages as its deepest member, not their
+    sum: pivots of different systems run in the same stages (and launches)."""
+    from hybsol.b200 import batch
+
+    mats, _ = _systems()
+    lay = batch.BatchLayout(mats)
+    stacked = native.analyze(lay.matrix.sizes, lay.matrix.row_ptr, lay.matrix.cols)
+    levels, flops = [], 0.0
+    for m in mats:
+        order = native.compute_ordering(m.row_ptr, m.cols, "first").astype(np.int64)
+        pm = m.permuted(order)
+        a = native.analyze(pm.sizes, pm.row_ptr, pm.cols)
+        levels.append(a["n_levels"])
+        flops += a["factor_flops"]
+    assert stacked["n_levels"] == max(levels) < sum(levels)
+    assert stacked["factor_flops"] == pytest.approx(flops, rel=1e-12)
