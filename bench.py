@@ -132,19 +132,19 @@ def element_orders(n, p):
     return int(p)
 
 
-def build_workload(n, p):
+def build_workload(n, p, with_order=False):
     import numpy as np
 
-    from hybsol.b200 import meshgen, native
+    from hybsol.b200 import batch, meshgen, native
 
     mat, b = meshgen.mesh_system(n, element_orders(n, p), seed=0)
     order = native.compute_ordering(mat.row_ptr, mat.cols, "first")
     pm = mat.permuted(order)
-    off_o = np.concatenate([[0], np.cumsum(mat.sizes)])
-    off_n = np.concatenate([[0], np.cumsum(pm.sizes)])
+    perm = batch.dof_permutation(mat.sizes, order)  # x_new[perm] = x_old
     bn = np.empty_like(b)
-    for i in range(mat.n_blocks):
-        bn[off_n[order[i]] : off_n[order[i] + 1]] = b[off_o[i] : off_o[i + 1]]
+    bn[perm] = b
+    if with_order:
+        return pm, bn, perm
     return pm, bn
 
 
@@ -219,15 +219,33 @@ class ClockSampler:
 # reference CPU path
 
 
+def load_meshgen():
+    """The synthetic mesh generator (pure NumPy), imported from its file alone: the
+    reference legs must not import the ``hybsol`` package, whose import loads this
+    repository's native library."""
+    import importlib.util
+
+    path = ROOT / "hybridized-solver_b200" / "hybsol" / "b200" / "meshgen.py"
+    spec = importlib.util.spec_from_file_location("_bench_meshgen", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def reference_sample(n, p, steps, warmup, threads):
-    """Decompose+solve of the reference extension (compiled from its sources) on a mesh."""
+    """Decompose + solve of the reference extension (compiled from its own sources in
+    oracle/_ref) on the n x n mesh, through its public BlockSystem API: assembly, the
+    reference's coloring, reorder_blocks, decompose(n_threads) and solve. Returns the
+    per-step times (s), the relative residual, the solution in the mesh's numbering and
+    the algorithmic flops counted from the reference's own factored pattern."""
     import numpy as np
 
-    from hybsol.b200 import meshgen
     from oracle import oracle as O
 
+    mg = load_meshgen()
     ref = O.load_reference()
-    mat, b = meshgen.mesh_system(n, element_orders(n, p), seed=0)
+    orders = mg.random_orders(n, 2, 10, seed=0) if str(p) == "rand" else int(p)
+    mat, b = mg.mesh_system(n, orders, seed=0)
     times = []
     for it in range(warmup + steps):
         s = ref.BlockSystem(*[int(x) for x in mat.sizes])
@@ -244,23 +262,22 @@ def reference_sample(n, p, steps, warmup, threads):
             times.append(dt)
     xo = s.reorder_vector(order, x)
     res = float(np.linalg.norm(mat.matvec(xo) - b) / np.linalg.norm(b))
-    return times, res
+    flops = O.factor_flops(np.asarray(s.block_sizes), [s.get_row_block_indices(i) for i in range(mat.n_blocks)])
+    return times, res, xo, flops
 
 
-def analyze_flops(n, p):
-    from hybsol.b200 import native
-
-    pm, _ = build_workload(n, p)
-    return native.analyze(pm.sizes, pm.row_ptr, pm.cols)["factor_flops"]
+def sample_workload_name(n, p):
+    return workload_config(n, p)["workload"]
 
 
-def cpu_baseline(full_flops, p, sample_mesh, steps=1, warmup=0):
+def cpu_baseline(full_flops, p, sample_mesh):
+    """The reference on the box's host cores, on the sample mesh; `value` extrapolates
+    the measured time to the benchmarked workload by algorithmic GFLOP (marked as such)."""
     from oracle import oracle as O
 
     cores = O.cpu_count()
     os.environ["OMP_NUM_THREADS"] = str(cores)
-    times, res = reference_sample(sample_mesh, p, steps, warmup, cores)
-    sample_flops = analyze_flops(sample_mesh, p)
+    times, res, x, sample_flops = reference_sample(sample_mesh, p, 1, 0, cores)
     best = min(times)
     scale = full_flops / sample_flops
     return {
@@ -268,18 +285,24 @@ def cpu_baseline(full_flops, p, sample_mesh, steps=1, warmup=0):
         "unit": "ms",
         "cores": cores,
         "kind": "reference",
+        "extrapolated": True,
         "sample": (
             f"reference extension (oracle/_ref, built from the reference's src/*.c) decompose(n_threads={cores}) + "
-            f"solve on the {sample_mesh}x{sample_mesh} p={p} mesh ({sample_flops / 1e9:.1f} GFLOP): "
-            f"{best * 1e3:.1f} ms ({sample_flops / best / 1e9:.1f} GFLOP/s, residual {res:.1e}), scaled by "
-            f"GFLOP to the {full_flops / 1e9:.0f}-GFLOP workload"
+            f"solve on the {sample_mesh}x{sample_mesh} p={p} mesh ({sample_flops / 1e9:.1f} GFLOP): measured "
+            f"{best * 1e3:.1f} ms ({sample_flops / best / 1e9:.1f} GFLOP/s, residual {res:.1e}); `value` is that "
+            f"time EXTRAPOLATED by GFLOP to the {full_flops / 1e9:.0f}-GFLOP workload, not measured"
         ),
         "sample_ms": best * 1e3,
         "sample_gflops": sample_flops / best / 1e9,
-    }
+        "sample_workload": sample_workload_name(sample_mesh, p),
+    }, x
 
 
 def run_reference(args):
+    """The reference's own CPU path, measured on the sample mesh it can finish within the
+    run (default 20x20 at the benchmark's p): `value` is the measured time per step of that
+    mesh, and `config` names it. The same mesh is timed on the GPU by our arm
+    (`same_mesh_pair` in its line), which is the like-for-like comparison."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -288,21 +311,18 @@ def run_reference(args):
     if not O.reference_available():
         print(json.dumps({"impl": "reference", "unavailable": "reference extension not built (oracle/_ref missing)"}))
         return 0
-    full = analyze_flops(args.mesh, args.p)
     cores = O.cpu_count()
     os.environ["OMP_NUM_THREADS"] = str(cores)
-    times, res = reference_sample(args.cpu_sample_mesh, args.p, args.steps, args.warmup, cores)
-    sample_flops = analyze_flops(args.cpu_sample_mesh, args.p)
-    scale = full / sample_flops
-    ms = statistics.mean(times) * 1e3 * scale
+    n = args.cpu_sample_mesh
+    times, res, _, flops = reference_sample(n, args.p, args.steps, args.warmup, cores)
+    ms = statistics.mean(times) * 1e3
     cpu = {
         "value": ms,
         "unit": "ms",
         "cores": cores,
         "kind": "reference",
-        "sample": f"{args.cpu_sample_mesh}x{args.cpu_sample_mesh} p={args.p} mesh per step "
-        f"({sample_flops / 1e9:.1f} GFLOP, {statistics.mean(times) * 1e3:.1f} ms, residual {res:.1e}), "
-        f"scaled by GFLOP to the {full / 1e9:.0f}-GFLOP workload",
+        "sample": f"the whole {n}x{n} p={args.p} mesh per step ({flops / 1e9:.1f} GFLOP, "
+        f"{flops / (ms * 1e-3) / 1e9:.1f} GFLOP/s, residual {res:.1e}); measured, not extrapolated",
     }
     line = {
         "impl": "reference",
@@ -318,7 +338,16 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": workload_config(args.mesh, args.p, {"factor_gflop": full / 1e9}),
+        "config": workload_config(
+            n,
+            args.p,
+            {
+                "factor_gflop": flops / 1e9,
+                "sample_of": workload_config(args.mesh, args.p)["workload"],
+                "note": f"the reference's CPU path cannot finish the {args.mesh}x{args.mesh} mesh within a run; "
+                "this line measures the largest mesh it finishes per step, and our arm times the same mesh on the GPU",
+            },
+        ),
         "cpu_baseline": cpu,
         "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -357,6 +386,79 @@ def gemm_peak(dtype):
     del a, b
     torch.cuda.empty_cache()
     return 2 * n**3 / (best * 1e-3) / 1e12
+
+
+def same_mesh_pair(args, x_ref, ref_ms):
+    """Our FP64 and mixed forms on the mesh the reference's CPU path was measured on (the
+    cpu_baseline sample), with the same step protocol as the headline (device-resident
+    inputs, CUDA events, warm-up) and end to end through the C ABI from pinned host
+    buffers; the FP64 solution is compared element-wise with the reference's."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from hybsol.b200 import native
+
+    lib = native.lib()
+    n = args.cpu_sample_mesh
+    pm, bn, perm = build_workload(n, args.p, with_order=True)
+    ns = native.NativeSystem(pm.sizes, pm.row_ptr, pm.cols)
+    stream = torch.cuda.ExternalStream(ns.stream)
+    d_vals = torch.from_numpy(pm.vals).to("cuda")
+    d_b = torch.from_numpy(bn).to("cuda")
+    d_x = torch.empty_like(d_b)
+    out = {"workload": sample_workload_name(n, args.p), "reference_ms": ref_ms, "reference_kind": "oracle/_ref"}
+    steps, warmup = max(3, args.steps), max(3, args.warmup)
+    for name, prec in (("fp64", native.FP64), ("mixed", native.MIXED)):
+
+        def step():
+            native._check(lib.hyb_system_set_values(ns._h, native._ptr(d_vals), native.MEMORY_DEVICE), "set_values")
+            ns.decompose(prec)
+            return ns.solve_device(d_b, d_x, 1, tol=TOL, max_iter=30, residual=(prec == native.MIXED))
+
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for e0, e1 in ev:
+            e0.record(stream)
+            info = step()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        out[f"{name}_ms"] = statistics.mean(a.elapsed_time(b) for a, b in ev)
+        if prec == native.FP64:
+            x = d_x.cpu().numpy()[perm]  # back to the mesh's numbering
+            out["fp64_rel_err_vs_reference"] = float(np.abs(x - x_ref).max() / np.abs(x_ref).max())
+        else:
+            out["mixed_iterations"] = info["iterations"]
+            out["mixed_relative_residual"] = info["relative_residual"]
+    h_vals = torch.from_numpy(pm.vals).pin_memory()
+    h_b = torch.from_numpy(bn).pin_memory()
+    h_x = torch.empty_like(h_b).pin_memory()
+    sinfo = native.SolveInfo()
+    for name, prec in (("fp64", native.FP64), ("mixed", native.MIXED)):
+
+        def e2e():
+            native._check(lib.hyb_system_set_values(ns._h, native._ptr(h_vals), native.MEMORY_HOST), "set_values")
+            ns.decompose(prec)
+            native._check(
+                lib.hyb_solve(ns._h, native._ptr(h_b), native._ptr(h_x), 1, native.MEMORY_HOST, TOL, 30,
+                              ctypes.byref(sinfo)),
+                "hyb_solve",
+            )
+
+        e2e()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            e2e()
+        out[f"e2e_{name}_ms"] = (time.perf_counter() - t0) * 1e3 / steps
+    out["e2e_speedup_mixed_vs_reference"] = ref_ms / out["e2e_mixed_ms"]
+    out["e2e_speedup_fp64_vs_reference"] = ref_ms / out["e2e_fp64_ms"]
+    out["steps"], out["warmup"] = steps, warmup
+    ns.close()
+    return out
 
 
 def run_ours(args):
@@ -541,12 +643,13 @@ def run_ours(args):
         bf16 = float(peaks.get("bf16_tflops_sustained") or 1390.5)
         rmix["tensor_bf16_tflops"] = 3 * rmix["tflops_fp_equivalent"]
         rmix["tensor_bf16_frac_of_sustained"] = 3 * rmix["tflops_fp_equivalent"] / bf16
-    cpu = None
+    cpu, pair = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
 
         if O.reference_available():
-            cpu = cpu_baseline(flops, args.p, args.cpu_sample_mesh)
+            cpu, x_ref = cpu_baseline(flops, args.p, args.cpu_sample_mesh)
+            pair = same_mesh_pair(args, x_ref, cpu["sample_ms"])
     if rank == 0:
         line = {
             "metric": METRIC,
@@ -599,6 +702,7 @@ def run_ours(args):
             "peaks": {"fp64_tflops_cublas": fp64_peak, "fp32_tflops_cublas": fp32_peak, "source": peak_src, **peaks},
             "clocks": clk,
             "cpu_baseline": cpu,
+            "same_mesh_pair": pair,
         }
         print(json.dumps(line))
     ns.close()

@@ -14,6 +14,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <type_traits>
@@ -132,6 +133,8 @@ struct hyb_system
     bool lookahead = true;
     bool umma = true; // mixed-form updates of 64-blocks on the tcgen05 tensor cores
     bool flow = true; // dataflow substitution (enqueue_solve_flow) in hyb_solve
+    uint64_t wait_ns = hyb::kWaitLimitNs; // limit of each wait of the dataflow solve
+    int64_t withhold_slot = -1;           // fault injection: pivot slot whose early partials are never released
     void *arena = nullptr;
     DevSym ds{};
     double *d_a = nullptr; // original values (FP64, CSR order)
@@ -675,25 +678,32 @@ template <typename T, typename V> int enqueue_solve_flow(hyb_system *h, const T 
     }
     cudaStream_t st = h->stream;
     HYB_CUDA(cudaMemsetAsync(h->d_tickets, 0, S.n * sizeof(int), st));
-    HYB_CUDA(cudaMemsetAsync(h->d_solve_status, 0, hyb::ST_WORDS * sizeof(int), st));
+    if (h->withhold_slot >= 0)
+    {
+        // the pivot's early-partial ticket starts far past its count, so no CTA ever takes
+        // the last one: the pre-sum is never released and the finisher's wait runs out
+        static const int kPoison = 1 << 30;
+        HYB_CUDA(cudaMemcpyAsync(h->d_tickets + h->withhold_slot, &kPoison, sizeof(int), cudaMemcpyHostToDevice, st));
+    }
     h->solve_epoch = (h->solve_epoch + 1) & 0x3fffffffu;
     int tag_f = (int)(2 * h->solve_epoch + 1), tag_b = tag_f + 1;
     DevSym ds = h->ds;
     V *scratch = scr;
     int *tickets = h->d_tickets, *flags = h->d_flags, *pflags = h->d_pflags, *status = h->d_solve_status;
     const T *dinv = solve_dinv<T>(h);
+    uint64_t wait_ns = h->wait_ns;
     int64_t nf = (int64_t)S.fwd_item_p.size(), nb = (int64_t)S.bwd_item_p.size();
     const int sms = sm_count();
     {
         const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nf, (int64_t)per_sm_f * sms));
-        void *args[] = {&ds,    (void *)&slab, &y,     &scratch, &tickets, &flags, &pflags,
-                        &tag_f, &nf,           &nrhs,  &stage,   &dinv,    &status};
+        void *args[] = {&ds,    (void *)&slab, &y,    &scratch, &tickets, &flags,  &pflags,
+                        &tag_f, &nf,           &nrhs, &stage,   &dinv,    &status, &wait_ns};
         HYB_CUDA(cudaLaunchCooperativeKernel((const void *)hyb::k_fwd_flow<T, V>, dim3(grid), dim3(hyb::kThreads),
                                              args, fwd_smem, st));
     }
     {
         const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nb, (int64_t)per_sm_b * sms));
-        void *args[] = {&ds, (void *)&slab, &y, &scratch, &tickets, &flags, &pflags, &tag_b, &nb, &nrhs, &status};
+        void *args[] = {&ds, (void *)&slab, &y, &scratch, &tickets, &flags, &pflags, &tag_b, &nb, &nrhs, &status, &wait_ns};
         HYB_CUDA(cudaLaunchCooperativeKernel((const void *)hyb::k_bwd_flow<T, V>, dim3(grid), dim3(hyb::kThreads),
                                              args, acc_bytes, st));
     }
@@ -795,6 +805,20 @@ int check_handle(const hyb_system *h)
     return h ? HYB_SUCCESS : HYB_INVALID_ARGUMENT;
 }
 
+// A device allocation released when it goes out of scope, so early returns do not leak.
+struct DevBuf
+{
+    void *p = nullptr;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf()
+    {
+        if (p)
+            cudaFree(p);
+    }
+};
+
 } // namespace
 
 // =====================================================================================
@@ -830,6 +854,8 @@ HYB_API const char *hyb_status_string(int status)
         return "iterative refinement did not converge";
     case HYB_TOO_LARGE:
         return "size beyond the supported limit";
+    case HYB_DEVICE_TIMEOUT:
+        return "a bounded device-side wait ran out";
     default:
         return "unknown status";
     }
@@ -989,6 +1015,7 @@ HYB_API int hyb_system_copy(const hyb_system *src, hyb_system **out)
     h->lookahead = src->lookahead;
     h->umma = src->umma;
     h->flow = src->flow;
+    h->wait_ns = src->wait_ns;
     HYB_CUDA(create_streams(h.get()));
     int rc = upload_symbolic(h.get());
     if (rc != HYB_SUCCESS)
@@ -1069,6 +1096,26 @@ HYB_API int hyb_system_set_option(hyb_system *h, int option, int64_t value)
     case HYB_OPTION_DATAFLOW_SOLVE:
         h->flow = value != 0;
         return HYB_SUCCESS;
+    case HYB_OPTION_WAIT_LIMIT_NS:
+        if (value <= 0)
+            return HYB_INVALID_ARGUMENT;
+        h->wait_ns = (uint64_t)std::max<int64_t>(value, 100000);
+        return HYB_SUCCESS;
+    case HYB_OPTION_WITHHOLD_ROW:
+    {
+        if (value < 0)
+        {
+            h->withhold_slot = -1;
+            return HYB_SUCCESS;
+        }
+        const Symbolic &S = h->S;
+        if (value >= S.n || S.diag_pos[value] - S.row_ptr[value] < 2)
+            return HYB_INVALID_ARGUMENT;
+        for (int64_t p = 0; p < S.n; ++p)
+            if (S.piv[p] == value)
+                h->withhold_slot = p;
+        return HYB_SUCCESS;
+    }
     default:
         return HYB_INVALID_ARGUMENT;
     }
@@ -1195,8 +1242,8 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
     HYB_CUDA(cudaStreamSynchronize(h->stream));
     if (st[hyb::ST_TIMEOUT])
     {
-        g_cuda_error = "a device-side wait ran out of its iteration limit";
-        return HYB_CUDA_ERROR;
+        g_cuda_error = "a device-side wait of the factorization ran out of its time limit";
+        return HYB_DEVICE_TIMEOUT;
     }
     h->factored = precision;
     h->launches += h->last_launches;
@@ -1304,9 +1351,13 @@ HYB_API int hyb_solve(hyb_system *h, const double *b, double *x, uint64_t nrhs, 
         {
             enqueue_residual(h, h->d_b, h->d_x, h->d_r, nr, cnt);
             enqueue_sumsq(h, h->d_r, dof, nr, h->d_norm, cnt);
+            int sst[hyb::ST_WORDS];
             HYB_CUDA(cudaMemcpyAsync(nrm.data(), h->d_norm, 2 * nr * sizeof(double), cudaMemcpyDeviceToHost,
                                      h->stream));
+            HYB_CUDA(cudaMemcpyAsync(sst, h->d_solve_status, sizeof(sst), cudaMemcpyDeviceToHost, h->stream));
             HYB_CUDA(cudaStreamSynchronize(h->stream));
+            if (sst[hyb::ST_TIMEOUT])
+                break; // reported below
             relres = 0;
             for (int r = 0; r < nr; ++r)
                 relres = std::max(relres, nrm[r + nr] > 0 ? std::sqrt(nrm[r] / nrm[r + nr]) : std::sqrt(nrm[r]));
@@ -1338,7 +1389,7 @@ HYB_API int hyb_solve(hyb_system *h, const double *b, double *x, uint64_t nrhs, 
     if (sst[hyb::ST_TIMEOUT])
     {
         g_cuda_error = "a wait of the dataflow solve ran out of its time limit";
-        return HYB_CUDA_ERROR;
+        return HYB_DEVICE_TIMEOUT;
     }
     h->launches += h->last_launches;
     if (info)
@@ -1488,28 +1539,26 @@ HYB_API int hyb_block_lu(uint64_t m, double *a, int memory)
     if (!hyb_device_available())
         return HYB_NO_DEVICE;
     const size_t bytes = m * m * sizeof(double);
+    DevBuf dbuf, st;
     double *d = a;
-    int *st = nullptr;
     if (memory != HYB_MEMORY_DEVICE)
-        HYB_CUDA(cudaMalloc(&d, bytes));
-    HYB_CUDA(cudaMalloc(&st, hyb::ST_WORDS * sizeof(int)));
-    if (memory != HYB_MEMORY_DEVICE)
+    {
+        HYB_CUDA(cudaMalloc(&dbuf.p, bytes));
+        d = static_cast<double *>(dbuf.p);
         HYB_CUDA(cudaMemcpy(d, a, bytes, cudaMemcpyHostToDevice));
-    k_status_init<<<1, 32>>>(st);
-    allow_smem(hyb::k_dense_lu, smem_optin());
+    }
+    HYB_CUDA(cudaMalloc(&st.p, hyb::ST_WORDS * sizeof(int)));
+    k_status_init<<<1, 32>>>(static_cast<int *>(st.p));
+    HYB_CUDA(allow_smem(hyb::k_dense_lu, smem_optin()));
     if ((int)bytes <= smem_optin())
-        hyb::k_dense_lu<<<1, hyb::kThreads, bytes>>>(d, (int)m, st);
+        hyb::k_dense_lu<<<1, hyb::kThreads, bytes>>>(d, (int)m, static_cast<int *>(st.p));
     else
-        hyb::k_dense_lu_global<<<1, hyb::kThreads>>>(d, (int)m, st);
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess && memory != HYB_MEMORY_DEVICE)
-        e = cudaMemcpy(a, d, bytes, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess)
-        e = cudaDeviceSynchronize();
+        hyb::k_dense_lu_global<<<1, hyb::kThreads>>>(d, (int)m, static_cast<int *>(st.p));
+    HYB_CUDA(cudaGetLastError());
     if (memory != HYB_MEMORY_DEVICE)
-        cudaFree(d);
-    cudaFree(st);
-    return e == cudaSuccess ? HYB_SUCCESS : cuda_fail(e, "hyb_block_lu");
+        HYB_CUDA(cudaMemcpy(a, d, bytes, cudaMemcpyDeviceToHost));
+    HYB_CUDA(cudaDeviceSynchronize());
+    return HYB_SUCCESS;
 }
 
 HYB_API int hyb_block_lu_solve(uint64_t m, const double *lu, uint64_t ncols, const double *b, double *out,
@@ -1520,13 +1569,17 @@ HYB_API int hyb_block_lu_solve(uint64_t m, const double *lu, uint64_t ncols, con
     if (!hyb_device_available())
         return HYB_NO_DEVICE;
     const size_t lu_bytes = m * m * sizeof(double), b_bytes = m * ncols * sizeof(double);
-    double *dlu = (double *)lu, *db = out;
+    DevBuf lu_buf, b_buf;
+    const double *dlu = lu;
+    double *db = out;
     if (memory != HYB_MEMORY_DEVICE)
     {
-        HYB_CUDA(cudaMalloc(&dlu, lu_bytes));
-        HYB_CUDA(cudaMalloc(&db, b_bytes));
-        HYB_CUDA(cudaMemcpy(dlu, lu, lu_bytes, cudaMemcpyHostToDevice));
-        HYB_CUDA(cudaMemcpy(db, b, b_bytes, cudaMemcpyHostToDevice));
+        HYB_CUDA(cudaMalloc(&lu_buf.p, lu_bytes));
+        HYB_CUDA(cudaMalloc(&b_buf.p, b_bytes));
+        HYB_CUDA(cudaMemcpy(lu_buf.p, lu, lu_bytes, cudaMemcpyHostToDevice));
+        HYB_CUDA(cudaMemcpy(b_buf.p, b, b_bytes, cudaMemcpyHostToDevice));
+        dlu = static_cast<const double *>(lu_buf.p);
+        db = static_cast<double *>(b_buf.p);
     }
     else if (b != out)
     {
@@ -1534,17 +1587,11 @@ HYB_API int hyb_block_lu_solve(uint64_t m, const double *lu, uint64_t ncols, con
     }
     hyb::k_dense_lu_solve<<<(unsigned)((ncols + hyb::kTile - 1) / hyb::kTile), hyb::kThreads>>>(dlu, (int)m, db,
                                                                                                (int)ncols);
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess && memory != HYB_MEMORY_DEVICE)
-        e = cudaMemcpy(out, db, b_bytes, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess)
-        e = cudaDeviceSynchronize();
+    HYB_CUDA(cudaGetLastError());
     if (memory != HYB_MEMORY_DEVICE)
-    {
-        cudaFree(dlu);
-        cudaFree(db);
-    }
-    return e == cudaSuccess ? HYB_SUCCESS : cuda_fail(e, "hyb_block_lu_solve");
+        HYB_CUDA(cudaMemcpy(out, db, b_bytes, cudaMemcpyDeviceToHost));
+    HYB_CUDA(cudaDeviceSynchronize());
+    return HYB_SUCCESS;
 }
 
 HYB_API int hyb_block_gemm(uint64_t m, uint64_t k, uint64_t n, const double *a, const double *b, double *c,
@@ -1555,31 +1602,29 @@ HYB_API int hyb_block_gemm(uint64_t m, uint64_t k, uint64_t n, const double *a, 
     if (!hyb_device_available())
         return HYB_NO_DEVICE;
     const size_t ab = m * k * sizeof(double), bb = k * n * sizeof(double), cb = m * n * sizeof(double);
-    double *da = (double *)a, *db = (double *)b, *dc = c;
+    DevBuf a_buf, b_buf, c_buf;
+    const double *da = a, *db = b;
+    double *dc = c;
     if (memory != HYB_MEMORY_DEVICE)
     {
-        HYB_CUDA(cudaMalloc(&da, ab + 8));
-        HYB_CUDA(cudaMalloc(&db, bb + 8));
-        HYB_CUDA(cudaMalloc(&dc, cb));
-        HYB_CUDA(cudaMemcpy(da, a, ab, cudaMemcpyHostToDevice));
-        HYB_CUDA(cudaMemcpy(db, b, bb, cudaMemcpyHostToDevice));
+        HYB_CUDA(cudaMalloc(&a_buf.p, ab + 8));
+        HYB_CUDA(cudaMalloc(&b_buf.p, bb + 8));
+        HYB_CUDA(cudaMalloc(&c_buf.p, cb));
+        HYB_CUDA(cudaMemcpy(a_buf.p, a, ab, cudaMemcpyHostToDevice));
+        HYB_CUDA(cudaMemcpy(b_buf.p, b, bb, cudaMemcpyHostToDevice));
         if (subtract)
-            HYB_CUDA(cudaMemcpy(dc, c, cb, cudaMemcpyHostToDevice));
+            HYB_CUDA(cudaMemcpy(c_buf.p, c, cb, cudaMemcpyHostToDevice));
+        da = static_cast<const double *>(a_buf.p);
+        db = static_cast<const double *>(b_buf.p);
+        dc = static_cast<double *>(c_buf.p);
     }
     const dim3 grid((unsigned)((n + hyb::kTile - 1) / hyb::kTile), (unsigned)((m + hyb::kTile - 1) / hyb::kTile));
     hyb::k_dense_gemm<<<grid, hyb::kThreads>>>(da, db, dc, (int)m, (int)k, (int)n, subtract);
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess && memory != HYB_MEMORY_DEVICE)
-        e = cudaMemcpy(c, dc, cb, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess)
-        e = cudaDeviceSynchronize();
+    HYB_CUDA(cudaGetLastError());
     if (memory != HYB_MEMORY_DEVICE)
-    {
-        cudaFree(da);
-        cudaFree(db);
-        cudaFree(dc);
-    }
-    return e == cudaSuccess ? HYB_SUCCESS : cuda_fail(e, "hyb_block_gemm");
+        HYB_CUDA(cudaMemcpy(c, dc, cb, cudaMemcpyDeviceToHost));
+    HYB_CUDA(cudaDeviceSynchronize());
+    return HYB_SUCCESS;
 }
 
 } // extern "C"
@@ -1597,21 +1642,23 @@ static __device__ __align__(256) double g_noalloc_scratch[HYB_NOALLOC_SCRATCH_DO
 namespace
 {
 constexpr int kMaxDevices = 64;
+std::once_flag g_noalloc_once[kMaxDevices];
 double *g_noalloc_ptr[kMaxDevices] = {};
+cudaError_t g_noalloc_err[kMaxDevices] = {};
 
-// Device address of the scratch array on the current device (looked up on first use).
+// Device address of the scratch array on `device`, which must be current: looked up once
+// per device (concurrent first calls wait for the one lookup).
 int noalloc_scratch(int device, double **out)
 {
     if (device < 0 || device >= kMaxDevices)
         return HYB_INVALID_ARGUMENT;
-    if (!g_noalloc_ptr[device])
-    {
+    std::call_once(g_noalloc_once[device], [device]() {
         void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess)
-            return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        g_noalloc_err[device] = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         g_noalloc_ptr[device] = static_cast<double *>(p);
-    }
+    });
+    if (g_noalloc_err[device] != cudaSuccess)
+        return cuda_fail(g_noalloc_err[device], "cudaGetSymbolAddress(g_noalloc_scratch)");
     *out = g_noalloc_ptr[device];
     return HYB_SUCCESS;
 }
@@ -1643,8 +1690,12 @@ extern "C" HYB_API int hyb_solve_fp64_noalloc(hyb_system *h, const double *b, do
     if (rc != HYB_SUCCESS)
         return rc;
     const int64_t dof = S.dof_off[S.n];
+    const uintptr_t xb = reinterpret_cast<uintptr_t>(x), bb = reinterpret_cast<uintptr_t>(b);
+    const uintptr_t len = (uintptr_t)dof * nrhs * sizeof(double);
+    if (x != b && xb < bb + len && bb < xb + len)
+        return HYB_INVALID_ARGUMENT; // overlapping but not identical: the copy below would be undefined
     if (x != b)
-        HYB_CUDA(cudaMemcpyAsync(x, b, dof * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        HYB_CUDA(cudaMemcpyAsync(x, b, len, cudaMemcpyDeviceToDevice, h->stream));
     uint64_t launches = 0;
     rc = enqueue_solve<double, double>(h, h->d_f64, x, scratch, (int)nrhs, launches);
     if (rc != HYB_SUCCESS)

@@ -844,6 +844,7 @@ enum
     ST_TIMEOUT = 3
 };
 constexpr uint64_t kWaitLimitNs = 1000000000ull; // 1 s
+constexpr int kDrainWaits = 30;                   // a timed-out CTA drains its copies for at most 30 s more
 
 __device__ __forceinline__ uint64_t global_ns()
 {
@@ -983,7 +984,12 @@ __global__ void __launch_bounds__(kUpd64Threads)
     {
         if (lane == 0)
             atomicOr(status + ST_TIMEOUT, 1);
-        mbar_wait(bar, 0); // the copies in flight land before the CTA leaves, or a second limit passes
+        // The CTA must not leave while its bulk copies can still write its shared memory:
+        // keep draining (the copies read valid global memory and complete), up to
+        // kDrainWaits further limits so the wait stays bounded.
+        for (int w = 0; w < kDrainWaits && !mbar_wait(bar, 0); ++w)
+        {
+        }
         return;
     }
 #pragma unroll
@@ -1684,8 +1690,8 @@ __global__ void __launch_bounds__(kThreads, 2)
 // product an item waits until the source block row's flag carries this solve's tag; the
 // CTA that takes a pivot's last ticket finishes it and sets the pivot's flag. Every wait
 // depends only on items earlier in the order and all CTAs are resident (cooperative
-// launch), so the waits end; each is also bounded in time (ST_TIMEOUT in `status`, after
-// which every wait returns at once). Source vectors are read from L2 (__ldcg): another
+// launch), so the waits end; each is also bounded in time (wait_ns; ST_TIMEOUT in
+// `status`, after which every wait returns at once). Source vectors are read from L2 (__ldcg): another
 // SM may have written them after this SM cached a neighbouring line.
 __device__ __forceinline__ int ld_acquire(const int *p)
 {
@@ -1699,8 +1705,8 @@ __device__ __forceinline__ void st_release(int *p, int v)
     asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Waits (thread 0, bounded) until *flag == tag; CTA-uniform result.
-__device__ __forceinline__ bool wait_flag(const int *flag, int tag, int *status)
+// Waits (thread 0, at most wait_ns) until *flag == tag; CTA-uniform result.
+__device__ __forceinline__ bool wait_flag(const int *flag, int tag, int *status, uint64_t wait_ns)
 {
     __shared__ int s_ok;
     if (threadIdx.x == 0)
@@ -1711,7 +1717,7 @@ __device__ __forceinline__ bool wait_flag(const int *flag, int tag, int *status)
             const uint64_t t0 = global_ns();
             while (ld_acquire(flag) != tag)
             {
-                if (schedule_aborted(status) || global_ns() - t0 > kWaitLimitNs)
+                if (schedule_aborted(status) || global_ns() - t0 > wait_ns)
                 {
                     atomicOr(status + ST_TIMEOUT, 1);
                     ok = 0;
@@ -1818,7 +1824,7 @@ template <typename T, typename V>
 __global__ void __launch_bounds__(kThreads, 1)
     k_fwd_flow(DevSym S, const T *__restrict__ slab, V *__restrict__ y, V *__restrict__ scratch,
                int *__restrict__ tickets, int *__restrict__ flags, int *__restrict__ pflags, int tag, int64_t n_items,
-               int nrhs, int stage_diag, const T *__restrict__ dinv, int *status)
+               int nrhs, int stage_diag, const T *__restrict__ dinv, int *status, uint64_t wait_ns)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(16) V red[kThreads * 16 / sizeof(V)];
@@ -1854,7 +1860,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             fwd_preload(dv, S, slab, dinv, k, stage_diag);
         GemvRegs<T> g;
         gemv_load(g, slab + S.blk_off[blk], m, K);
-        if (!wait_flag(flags + src, tag, status))
+        if (!wait_flag(flags + src, tag, status, wait_ns))
             return;
         V *dst = late ? acc : part + local * E;
         if (g.ok)
@@ -1869,7 +1875,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             publish_flag(pflags + p, tag);
             continue;
         }
-        if (nparts > 1 && !wait_flag(pflags + p, tag, status))
+        if (nparts > 1 && !wait_flag(pflags + p, tag, status, wait_ns))
             return;
         __syncthreads(); // the late partial is in acc
         combine_partials(acc, yk, nparts > 1 ? (const V *)part : nullptr, (const V *)acc, false, E);
@@ -1885,7 +1891,7 @@ template <typename T, typename V>
 __global__ void __launch_bounds__(kThreads, 2)
     k_bwd_flow(DevSym S, const T *__restrict__ slab, V *__restrict__ y, V *__restrict__ scratch,
                int *__restrict__ tickets, int *__restrict__ flags, int *__restrict__ pflags, int tag, int64_t n_items,
-               int nrhs, int *status)
+               int nrhs, int *status, uint64_t wait_ns)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(16) V red[kThreads * 16 / sizeof(V)];
@@ -1911,7 +1917,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         V *part = scratch + S.bwd_rows[p] * nrhs;
         GemvRegs<T> g;
         gemv_load(g, slab + S.blk_off[blk], m, K);
-        if (!wait_flag(flags + c, tag, status))
+        if (!wait_flag(flags + c, tag, status, wait_ns))
             return;
         V *dst = late ? acc : part + b * E;
         if (g.ok)
@@ -1926,7 +1932,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             publish_flag(pflags + p, tag);
             continue;
         }
-        if (nparts > 1 && !wait_flag(pflags + p, tag, status))
+        if (nparts > 1 && !wait_flag(pflags + p, tag, status, wait_ns))
             return;
         __syncthreads(); // the late partial is in acc
         V *yk = y + S.dof_off[k] * nrhs;

@@ -1,11 +1,12 @@
 """Many independent block systems factored and solved together on one device handle.
 
-The systems are stacked block-diagonally and ordered with the reference's coloring on the
-union. First-fit coloring visits blocks in index order and a block's colour depends only
-on the blocks of its own system, and ``order_from_colors`` sorts stably by colour, so every
-system keeps exactly the relative order it would get alone (and hence its own factors).
-Pivots of different systems then share elimination stages, and with them kernel launches,
-which is what makes many small systems cheap.
+The systems are stacked block-diagonally. Each system is ordered on its own with the
+reference's coloring (any strategy), and its ordered blocks keep a contiguous index range
+of the stack, so every system gets exactly the order -- and hence the factors -- it would
+get alone. Ordering the union instead would tie a system's order to the others' under the
+greedy and balanced strategies, which rank colours by counts over all blocks. Elimination
+stages come from dependencies, not from indices, so pivots of different systems still
+share stages, and with them kernel launches, which is what makes many small systems cheap.
 
 ``BatchLayout`` is the host-side part (stacking, ordering, moving vectors in and out);
 ``BatchedSystem`` adds the device handle. When the systems' factors exceed one device,
@@ -42,11 +43,16 @@ class BatchLayout:
         if not self.systems:
             raise ValueError("no systems to batch")
         stacked = meshgen.block_diagonal(self.systems)
-        self.order = native.compute_ordering(stacked.row_ptr, stacked.cols, strategy).astype(np.int64)
-        self.matrix = stacked.permuted(self.order)
-        self.perm = dof_permutation(stacked.sizes, self.order)
         self.dof_off = np.concatenate([[0], np.cumsum([m.dof for m in self.systems])]).astype(np.int64)
         self.block_off = np.concatenate([[0], np.cumsum([m.n_blocks for m in self.systems])]).astype(np.int64)
+        own = [native.compute_ordering(m.row_ptr, m.cols, strategy).astype(np.int64) for m in self.systems]
+        self.order = np.concatenate([o + b0 for o, b0 in zip(own, self.block_off[:-1])])
+        # each system's blocks stay in its own index range, in its own order
+        for i, o in enumerate(own):
+            sub = self.order[self.block_off[i] : self.block_off[i + 1]] - self.block_off[i]
+            assert np.array_equal(sub, o), "a batched system lost its own ordering"
+        self.matrix = stacked.permuted(self.order)
+        self.perm = dof_permutation(stacked.sizes, self.order)
 
     @property
     def count(self) -> int:

@@ -22,6 +22,15 @@ ORDERING = {"first": 0, "greedy": 1, "balanced": 2}
 
 SUCCESS = 0
 NOT_CONVERGED = 23
+TOO_LARGE = 24
+DEVICE_TIMEOUT = 25
+
+# hyb_option values (include/hybsol_b200.h)
+OPTION_LOOKAHEAD = 0
+OPTION_TENSOR_CORE_MIXED = 1
+OPTION_DATAFLOW_SOLVE = 2
+OPTION_WAIT_LIMIT_NS = 3
+OPTION_WITHHOLD_ROW = 4
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _i64p = ctypes.POINTER(ctypes.c_int64)
@@ -83,7 +92,7 @@ class HybError(RuntimeError):
 
     def __init__(self, status: int, what: str):
         self.status = status
-        detail = lib().hyb_last_cuda_error().decode() if status in (2, 16, 17, 19, 24) else ""
+        detail = lib().hyb_last_cuda_error().decode() if status in (2, 16, 17, 19, 24, 25) else ""
         msg = f"{what} failed: {lib().hyb_status_string(status).decode()} ({status})"
         super().__init__(msg + (f": {detail}" if detail else ""))
 
@@ -281,6 +290,10 @@ class NativeSystem:
     def set_dataflow_solve(self, enable: bool):
         """Dataflow substitution (one cooperative launch per direction) or one launch per stage."""
         _check(lib().hyb_system_set_option(self._h, 2, 1 if enable else 0), "hyb_system_set_option")
+
+    def set_option(self, option: int, value: int):
+        """Any ``hyb_option`` of the handle (``OPTION_*`` above)."""
+        _check(lib().hyb_system_set_option(self._h, option, int(value)), "hyb_system_set_option")
 
     @property
     def stream(self) -> int:

@@ -6,7 +6,7 @@
  * whose core is the hidden-visibility "block_system interface" of src/blocks.h:65-131.
  * That interface is not exported by the reference (MODULE_INTERNAL, src/module.h:3-5);
  * the entry points below are the exported equivalents a binding calls instead. The
- * package's CPython extension `hybsol._mod` binds exactly these (see INTEGRATION.md).
+ * package's CPython extension `hybsol._mod` binds exactly these.
  *
  * Conventions
  *  - Plain C types only: no CUDA or torch types cross this boundary.
@@ -46,7 +46,9 @@ typedef enum
     HYB_ZERO_PIVOT = 21,         /* a diagonal-block pivot was exactly zero */
     HYB_NON_FINITE = 22,         /* a pivot or factor entry is inf/nan */
     HYB_NOT_CONVERGED = 23,      /* iterative refinement missed its tolerance */
-    HYB_TOO_LARGE = 24           /* request beyond a documented size limit */
+    HYB_TOO_LARGE = 24,          /* request beyond a documented size limit */
+    HYB_DEVICE_TIMEOUT = 25      /* a bounded device-side wait ran out (the work was abandoned;
+                                    the context stays usable) */
 } hyb_status;
 
 typedef enum
@@ -159,7 +161,16 @@ typedef enum
     /* 1 (default): hyb_solve substitutes in one cooperative launch per direction, each
      * pivot proceeding as soon as its sources are final; 0: one launch per elimination
      * stage. Both give the same solution. */
-    HYB_OPTION_DATAFLOW_SOLVE = 2
+    HYB_OPTION_DATAFLOW_SOLVE = 2,
+    /* Time limit, in nanoseconds, of each wait of the dataflow solve for a source row
+     * (default 1e9). A wait that runs out abandons the solve, which then returns
+     * HYB_DEVICE_TIMEOUT. Values below 1e5 are raised to 1e5. */
+    HYB_OPTION_WAIT_LIMIT_NS = 3,
+    /* Fault injection on the host, for testing the timeout path (-1, the default, turns it
+     * off): in the next dataflow solves the partial sums of block row `value` are never
+     * released, so the waits for that row run out. The row must have at least two blocks
+     * left of its diagonal. */
+    HYB_OPTION_WITHHOLD_ROW = 4
 } hyb_option;
 
 /* Sets a schedule option of the handle (takes effect at the next decomposition). */
@@ -202,8 +213,11 @@ HYB_API int hyb_residual(hyb_system *sys, const double *b, const double *x, doub
  * The first call on a device looks up that array's device address (once per device, with
  * the device current); make that first call before any stream capture. All calls share
  * the one array: calls that overlap on the GPU -- from two threads, or on two handles of
- * the same device -- race on it. The call returns after the solve has finished on the
- * handle's stream. The results equal hyb_solve's for the same factors. */
+ * the same device -- race on it. `x` either is `b` or does not overlap it at all (a partial
+ * overlap returns HYB_INVALID_ARGUMENT). The looked-up address belongs to the device's
+ * current context: after cudaDeviceReset the library must be reloaded before this entry
+ * point is used again on that device. The call returns after the solve has finished on the
+ * handle's stream. The results equal hyb_solve's bit for bit for the same factors. */
 #define HYB_NOALLOC_SCRATCH_DOUBLES (1u << 20)
 HYB_API int hyb_solve_fp64_noalloc(hyb_system *sys, const double *b, double *x, uint64_t nrhs);
 

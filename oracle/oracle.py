@@ -252,3 +252,24 @@ def cpu_count() -> int:
         return len(os.sched_getaffinity(0))
     except AttributeError:  # pragma: no cover
         return os.cpu_count() or 1
+
+
+def factor_flops(sizes, rows) -> float:
+    """Algorithmic flops of the block LU from a factored pattern: for every pivot k of m
+    rows, 2/3 m^3 (diagonal LU) + 2 m^2 U (row solve over the U columns of its upper
+    blocks) + 2 L m U (Schur updates, L the rows of its lower column). ``rows[k]`` are the
+    columns of block row k after the decomposition (the fill included), e.g. the reference's
+    ``get_row_block_indices`` (src/block_system.c:312-349) of a decomposed system."""
+    sizes = np.asarray(sizes, dtype=np.float64)
+    n = len(sizes)
+    up = np.zeros(n)
+    lc = np.zeros(n)
+    for k in range(n):
+        cols = np.asarray(rows[k], dtype=np.int64)
+        upper = cols[cols > k]
+        lower = cols[cols < k]
+        up[k] = sizes[upper].sum()
+        # block (k, j) with j < k puts row k into the lower column of pivot j
+        np.add.at(lc, lower, sizes[k])
+    m = sizes
+    return float(np.sum(2.0 / 3.0 * m**3 + 2.0 * m * m * up + 2.0 * lc * m * up))

@@ -42,15 +42,20 @@ def test_dof_permutation_matches_block_moves(native):
     assert np.array_equal(np.sort(p), np.arange(len(b)))
 
 
-def test_layout_keeps_each_system_order(native):
+@pytest.mark.parametrize("strategy", ["first", "greedy", "balanced"])
+def test_layout_keeps_each_system_order(native, strategy):
     from hybsol.b200 import batch
 
     mats, _ = _systems()
-    lay = batch.BatchLayout(mats)
+    lay = batch.BatchLayout(mats, strategy)
     for i, m in enumerate(mats):
-        own = native.compute_ordering(m.row_ptr, m.cols, "first").astype(np.int64)
-        sub = lay.order[lay.block_off[i] : lay.block_off[i + 1]]
-        assert np.array_equal(np.argsort(sub, kind="stable"), np.argsort(own, kind="stable"))
+        own = native.compute_ordering(m.row_ptr, m.cols, strategy).astype(np.int64)
+        sub = lay.order[lay.block_off[i] : lay.block_off[i + 1]] - lay.block_off[i]
+        assert np.array_equal(sub, own)
+        # the stacked system's diagonal block range of system i is system i reordered alone
+        pm = m.permuted(own)
+        b0, b1 = lay.block_off[i], lay.block_off[i + 1]
+        assert np.array_equal(lay.matrix.sizes[b0:b1], pm.sizes)
 
 
 @pytest.mark.parametrize("nrhs", [1, 2])

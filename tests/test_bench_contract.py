@@ -1,7 +1,8 @@
 """bench.py's reference arm on the host: the one JSON line and its keys (tiny sizes, no GPU).
 
 The arm times the reference's own CPU implementation (the reference extension compiled from
-its sources under oracle/_ref) on a bounded sample and scales it to the workload; under
+its sources under oracle/_ref) on the sample mesh it can finish, reports that measured time
+under that mesh's name, and loads none of this repository's native libraries; under
 torchrun only rank 0 prints.
 """
 
@@ -43,10 +44,28 @@ def test_reference_arm_line():
         assert key in d, key
     assert d["higher_is_better"] is False and d["unit"] == "ms" and d["value"] > 0
     assert d["value"] == d["ms_per_step"] == d["cpu_baseline"]["value"] == d["e2e"]["value"]
-    assert d["config"]["workload"] and d["config"]["mesh"] == "12x12"
+    # the config names the mesh that was measured, and which workload it samples
+    assert d["config"]["mesh"] == "6x6" and "12x12" in d["config"]["sample_of"]
+    assert d["config"]["factor_gflop"] > 0
     cpu = d["cpu_baseline"]
     assert cpu["kind"] == "reference" and cpu["cores"] >= 1 and "6x6" in cpu["sample"]
+    assert "not extrapolated" in cpu["sample"]
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+
+
+def test_reference_arm_loads_no_repo_library():
+    """The reference leg imports the generator by file and counts flops from the reference's
+    own factored pattern: neither libhybsol_b200.so nor the hybsol._mod extension loads."""
+    code = (
+        "import sys, runpy; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0', "
+        "'--mesh', '12', '--cpu-sample-mesh', '4']\n"
+        "try:\n    runpy.run_path('bench.py', run_name='__main__')\nexcept SystemExit:\n    pass\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print('LOADED', 'libhybsol_b200' in maps, 'hybsol/_mod' in maps)\n"
+    )
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert "LOADED False False" in out.stdout, out.stdout[-500:]
 
 
 def test_reference_arm_other_ranks_are_silent():
