@@ -78,7 +78,20 @@ def parse_args():
         help="one decompose + solve per form and nothing else (the command ncu captures run)",
     )
     ap.add_argument("--form", choices=["both", "fp64", "mixed"], default="both", help="forms --single runs")
-    return ap.parse_args()
+    ap.add_argument(
+        "--shift",
+        choices=["dominant", "reduced"],
+        default="dominant",
+        help="value set: the diagonally dominant one (shift scale 1), or the reduced shift recorded for this mesh "
+        "(1-norm condition number ~1e6; the FP64 form then refines with its own factors to reach the tolerance)",
+    )
+    args = ap.parse_args()
+    args.alpha = 1.0
+    if args.shift == "reduced":
+        from hybsol.b200 import meshgen
+
+        args.alpha = meshgen.reduced_shift(args.mesh, args.p)
+    return args
 
 
 def run_single(args):
@@ -87,8 +100,9 @@ def run_single(args):
 
     from hybsol.b200 import native
 
-    pm, bn = build_workload(args.mesh, args.p)
+    pm, bn = build_workload(args.mesh, args.p, shift=args.alpha)
     ns = native.NativeSystem.from_matrix(pm)
+    ns.set_option(native.OPTION_FP64_REFINEMENT, int(args.shift == "reduced"))
     forms = {"both": (native.FP64, native.MIXED), "fp64": (native.FP64,), "mixed": (native.MIXED,)}[args.form]
     for prec in forms:
         ns.set_values(pm.vals)
@@ -97,6 +111,16 @@ def run_single(args):
         assert np.isfinite(x).all() and info["relative_residual"] < 1e-10, info
     ns.close()
     return 0
+
+
+def shift_description(alpha):
+    if alpha == 1.0:
+        return "dominant: diagonal shift = sum of the row's off-diagonal block norms + 1"
+    from hybsol.b200 import meshgen
+
+    rec = [v for v in meshgen.REDUCED_SHIFT.values() if v[0] == alpha]
+    kappa = f", kappa_1 ~ {rec[0][1]:.2g} ({rec[0][2]})" if rec else ""
+    return f"reduced: diagonal shift scaled by alpha={alpha:.6g}{kappa}"
 
 
 def workload_config(n, p, extra=None):
@@ -113,6 +137,8 @@ def workload_config(n, p, extra=None):
         "tolerance": TOL,
         "l2": "inputs larger than L2 (factor slab >> 126 MB)",
     }
+    if extra and "alpha" in extra:
+        cfg["values"] = shift_description(extra.pop("alpha"))
     if extra:
         cfg.update(extra)
     return cfg
@@ -132,12 +158,12 @@ def element_orders(n, p):
     return int(p)
 
 
-def build_workload(n, p, with_order=False):
+def build_workload(n, p, with_order=False, shift=1.0):
     import numpy as np
 
     from hybsol.b200 import batch, meshgen, native
 
-    mat, b = meshgen.mesh_system(n, element_orders(n, p), seed=0)
+    mat, b = meshgen.mesh_system(n, element_orders(n, p), seed=0, shift=shift)
     order = native.compute_ordering(mat.row_ptr, mat.cols, "first")
     pm = mat.permuted(order)
     perm = batch.dof_permutation(mat.sizes, order)  # x_new[perm] = x_old
@@ -498,11 +524,14 @@ def run_ours(args):
     fp32_peak = gemm_peak(torch.float32)
 
     t0 = time.perf_counter()
-    pm, bn = build_workload(args.mesh, args.p)
+    pm, bn = build_workload(args.mesh, args.p, shift=args.alpha)
     gen_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     ns = native.NativeSystem(pm.sizes, pm.row_ptr, pm.cols)
     analysis_ms = (time.perf_counter() - t0) * 1e3
+    reduced = args.shift == "reduced"
+    # the reduced set needs refinement in the FP64 form too (its plain solve misses 1e-12)
+    ns.set_option(native.OPTION_FP64_REFINEMENT, int(reduced))
     ana = native.analyze(pm.sizes, pm.row_ptr, pm.cols)
     flops = ana["factor_flops"]
     stream = torch.cuda.ExternalStream(ns.stream)
@@ -519,7 +548,7 @@ def run_ours(args):
         native._check(lib.hyb_system_set_values(ns._h, native._ptr(d_vals), native.MEMORY_DEVICE), "set_values")
         ns.decompose(prec)
         launches += ns.last_launch_count()
-        info = ns.solve_device(d_b, d_x, 1, tol=TOL, max_iter=30, residual=(prec == native.MIXED))
+        info = ns.solve_device(d_b, d_x, 1, tol=TOL, max_iter=60, residual=(prec == native.MIXED or reduced))
         launches += ns.last_launch_count()
         return launches, info
 
@@ -568,7 +597,7 @@ def run_ours(args):
         native._check(lib.hyb_system_set_values(ns._h, native._ptr(h_vals), native.MEMORY_HOST), "set_values")
         ns.decompose(native.MIXED)
         st = lib.hyb_solve(
-            ns._h, native._ptr(h_b), native._ptr(h_x), 1, native.MEMORY_HOST, TOL, 30, ctypes.byref(sinfo)
+            ns._h, native._ptr(h_b), native._ptr(h_x), 1, native.MEMORY_HOST, TOL, 60, ctypes.byref(sinfo)
         )
         native._check(st, "hyb_solve")
 
@@ -644,7 +673,7 @@ def run_ours(args):
         rmix["tensor_bf16_tflops"] = 3 * rmix["tflops_fp_equivalent"]
         rmix["tensor_bf16_frac_of_sustained"] = 3 * rmix["tflops_fp_equivalent"] / bf16
     cpu, pair = None, None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not reduced:
         from oracle import oracle as O
 
         if O.reference_available():
@@ -674,6 +703,7 @@ def run_ours(args):
                     "levels": int(ana["n_levels"]),
                     "factor_gflop": flops / 1e9,
                     "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                    "alpha": args.alpha,
                 },
             ),
             "fp64_ms": fp64_ms,
@@ -682,8 +712,11 @@ def run_ours(args):
             "mixed_tflops": flops / (mixed_ms * 1e-3) / 1e12,
             "accuracy": {
                 "fp64_relative_residual": fp64_relres,
+                "fp64_refinement_iterations": fp64_info["iterations"],
                 "mixed_relative_residual": mixed_info["relative_residual"],
                 "mixed_refinement_iterations": mixed_info["iterations"],
+                "mixed_krylov_iterations": mixed_info["krylov_iterations"],
+                "mixed_converged": mixed_info["converged"],
                 "mixed_rel_err_vs_fp64_solution": err_vs_fp64,
             },
             "analysis_ms": analysis_ms,

@@ -3,6 +3,7 @@
 // solves.
 #include "hyb_internal.h"
 #include "hyb_kernels.cuh"
+#include "hyb_krylov.cuh"
 #include "hyb_umma.cuh"
 
 #include "hybsol_b200.h"
@@ -135,6 +136,9 @@ struct hyb_system
     bool flow = true; // dataflow substitution (enqueue_solve_flow) in hyb_solve
     uint64_t wait_ns = hyb::kWaitLimitNs; // limit of each wait of the dataflow solve
     int64_t withhold_slot = -1;           // fault injection: pivot slot whose early partials are never released
+    int refinement = 0;                   // HYB_OPTION_REFINEMENT: 0 auto, 1 refinement only, 2 FGMRES
+    bool fp64_refine = false;             // HYB_OPTION_FP64_REFINEMENT
+    int krylov_restart = 30;              // HYB_OPTION_KRYLOV_RESTART
     void *arena = nullptr;
     DevSym ds{};
     double *d_a = nullptr; // original values (FP64, CSR order)
@@ -165,6 +169,21 @@ struct hyb_system
     double *d_b = nullptr, *d_x = nullptr, *d_r = nullptr, *d_scr64 = nullptr, *d_part = nullptr, *d_norm = nullptr;
     float *d_yf = nullptr, *d_scr32 = nullptr;
     int n_norm_parts = 0;
+    // refinement: correction and best iterate (FP64); FGMRES: kry_m + 1 basis vectors V,
+    // kry_m preconditioned vectors Z, the product w, the Hessenberg column and the
+    // combination coefficients (all sized for buf_nrhs right-hand sides)
+    double *d_z = nullptr, *d_xb = nullptr, *d_w = nullptr, *d_V = nullptr, *d_Zk = nullptr, *d_h = nullptr,
+           *d_coef = nullptr;
+    int64_t kry_m = 0;
+    // column view of the factors and of A (transposed solve, ||A||_1), built at first use
+    void *t_arena = nullptr;
+    hyb::DevTrans dt{};
+    int64_t t_max_rows = 0;
+    double *d_tscr = nullptr;
+    int64_t tscr_nrhs = 0;
+    double *d_colsum = nullptr;
+    std::vector<int64_t> t_fu_pref, t_bu_pref; // host copies of dt's unit prefixes (grid sizes)
+    std::map<int, std::unique_ptr<GraphExec>> g_solveT; // by nrhs
     std::unique_ptr<GraphExec> g_factor[2];
     std::map<std::pair<int, int>, std::unique_ptr<GraphExec>> g_solve; // (precision, nrhs)
     uint64_t launches = 0;
@@ -198,6 +217,10 @@ struct hyb_system
         cudaFree(d_dinv);
         cudaFree(d_ops);
         cudaFree(d_tgt);
+        g_solveT.clear();
+        cudaFree(t_arena);
+        cudaFree(d_tscr);
+        cudaFree(d_colsum);
         free_solve_buffers();
         for (cudaEvent_t e : {ev_prio, ev_piv, ev_join})
             if (e)
@@ -217,15 +240,25 @@ struct hyb_system
         prof_update_levels = 0;
     }
 
+    void free_krylov()
+    {
+        for (void *p : {(void *)d_w, (void *)d_V, (void *)d_Zk, (void *)d_h, (void *)d_coef})
+            cudaFree(p);
+        d_w = d_V = d_Zk = d_h = d_coef = nullptr;
+        kry_m = 0;
+    }
+
     void free_solve_buffers()
     {
         for (void *p : {(void *)d_b, (void *)d_x, (void *)d_r, (void *)d_scr64, (void *)d_part, (void *)d_norm,
-                        (void *)d_yf, (void *)d_scr32})
+                        (void *)d_yf, (void *)d_scr32, (void *)d_z, (void *)d_xb})
             cudaFree(p);
-        d_b = d_x = d_r = d_scr64 = d_part = d_norm = nullptr;
+        d_b = d_x = d_r = d_scr64 = d_part = d_norm = d_z = d_xb = nullptr;
         d_yf = d_scr32 = nullptr;
+        free_krylov();
         buf_nrhs = 0;
         g_solve.clear();
+        g_solveT.clear();
     }
 };
 
@@ -775,6 +808,8 @@ int ensure_solve_buffers(hyb_system *h, int64_t nrhs)
     HYB_CUDA(cudaMalloc(&h->d_scr32, scr * sizeof(float)));
     HYB_CUDA(cudaMalloc(&h->d_part, (size_t)h->n_norm_parts * nrhs * sizeof(double)));
     HYB_CUDA(cudaMalloc(&h->d_norm, 2 * nrhs * sizeof(double)));
+    HYB_CUDA(cudaMalloc(&h->d_z, dof * nrhs * sizeof(double)));
+    HYB_CUDA(cudaMalloc(&h->d_xb, dof * nrhs * sizeof(double)));
     h->buf_nrhs = nrhs;
     return HYB_SUCCESS;
 }
@@ -818,6 +853,430 @@ struct DevBuf
             cudaFree(p);
     }
 };
+
+// ------------------------------------------------------------------------------------
+// Refinement of the mixed form (and of the plain form with HYB_OPTION_FP64_REFINEMENT).
+
+// Squared 2-norms of the columns of v (dof x nr) into dev_out and `out` (host), with the
+// solve's status words read in the same synchronization.
+int column_sumsq(hyb_system *h, const double *v, int nr, double *dev_out, std::vector<double> &out, bool &timed_out,
+                 uint64_t &cnt)
+{
+    const int64_t dof = h->S.dof_off[h->S.n];
+    enqueue_sumsq(h, v, dof, nr, dev_out, cnt);
+    int sst[hyb::ST_WORDS];
+    out.resize(nr);
+    HYB_CUDA(cudaMemcpyAsync(out.data(), dev_out, nr * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    HYB_CUDA(cudaMemcpyAsync(sst, h->d_solve_status, sizeof(sst), cudaMemcpyDeviceToHost, h->stream));
+    HYB_CUDA(cudaStreamSynchronize(h->stream));
+    timed_out = sst[hyb::ST_TIMEOUT] != 0;
+    return HYB_SUCCESS;
+}
+
+// Largest relative residual over the columns.
+double max_relative(const std::vector<double> &rn2, const std::vector<double> &bn2)
+{
+    double m = 0;
+    for (size_t r = 0; r < rn2.size(); ++r)
+    {
+        const double v = bn2[r] > 0 ? std::sqrt(rn2[r] / bn2[r]) : std::sqrt(rn2[r]);
+        m = std::isnan(v) ? v : std::max(m, v);
+        if (std::isnan(m))
+            break;
+    }
+    return m;
+}
+
+// z = M^{-1} v, one substitution with the handle's factors: in the mixed form v is rounded
+// to FP32, substituted with the FP32 factors and widened back; otherwise FP64 throughout.
+int apply_factors(hyb_system *h, const double *v, double *z, int nr, uint64_t &cnt)
+{
+    const int64_t len = h->S.dof_off[h->S.n] * nr;
+    if (h->factored == HYB_PRECISION_MIXED)
+    {
+        hyb::k_convert<double, float><<<elementwise_grid(len), hyb::kThreads, 0, h->stream>>>(v, h->d_yf, len);
+        auto &slot = h->g_solve[{HYB_PRECISION_MIXED, nr}];
+        const int rc = substitute<float, float>(h, h->d_f32, h->d_yf, h->d_scr32, nr, slot);
+        if (rc != HYB_SUCCESS)
+            return rc;
+        hyb::k_convert<float, double><<<elementwise_grid(len), hyb::kThreads, 0, h->stream>>>(h->d_yf, z, len);
+        cnt += 2;
+        return HYB_SUCCESS;
+    }
+    if (z != v)
+        HYB_CUDA(cudaMemcpyAsync(z, v, len * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    auto &slot = h->g_solve[{HYB_PRECISION_FP64, nr}];
+    return substitute<double, double>(h, h->d_f64, z, h->d_scr64, nr, slot);
+}
+
+struct RefineResult
+{
+    uint32_t iters = 0;  // corrections applied (refinement steps + FGMRES iterations)
+    uint32_t krylov = 0; // of them, FGMRES iterations
+    double relres = -1;
+    int status = HYB_SUCCESS;
+};
+
+// A refinement step must shrink the FP64 residual by at least this factor, or the
+// automatic mode continues with FGMRES.
+constexpr double kIrContraction = 0.1;
+
+// Restarted FGMRES(m) in FP64 on A x = b from the current x (d_x), right-preconditioned
+// by the factors: Z_j = M^{-1} V_j, w = A Z_j, modified Gram-Schmidt against V, Givens
+// rotations on the host, x += Z y. Each column of a multi-RHS solve is its own Krylov
+// process (the columns share the launches). The true FP64 residual is recomputed at every
+// restart and decides convergence.
+int fgmres(hyb_system *h, int nr, double tol, uint32_t max_iter, const std::vector<double> &bn2, RefineResult &o,
+           uint64_t &cnt)
+{
+    const Symbolic &S = h->S;
+    const int m = h->krylov_restart;
+    const int64_t dof = S.dof_off[S.n], len = dof * nr;
+    const unsigned eg = elementwise_grid(len);
+    if (h->kry_m != m)
+    {
+        h->free_krylov();
+        HYB_CUDA(cudaMalloc(&h->d_w, len * sizeof(double)));
+        HYB_CUDA(cudaMalloc(&h->d_V, (size_t)(m + 1) * len * sizeof(double)));
+        HYB_CUDA(cudaMalloc(&h->d_Zk, (size_t)m * len * sizeof(double)));
+        HYB_CUDA(cudaMalloc(&h->d_h, (size_t)(m + 2) * nr * sizeof(double)));
+        HYB_CUDA(cudaMalloc(&h->d_coef, (size_t)m * nr * sizeof(double)));
+        h->kry_m = m;
+    }
+    // per column r: H (m+1 x m, row i column j at (r * (m + 1) + i) * m + j), rotations, g
+    std::vector<double> H((size_t)nr * (m + 1) * m), cs((size_t)nr * m), sn((size_t)nr * m), g((size_t)nr * (m + 1));
+    std::vector<double> hcol((size_t)(m + 2) * nr), coef((size_t)m * nr), rn2;
+    bool to = false;
+    int rc;
+    for (;;)
+    {
+        enqueue_residual(h, h->d_b, h->d_x, h->d_r, nr, cnt);
+        if ((rc = column_sumsq(h, h->d_r, nr, h->d_norm, rn2, to, cnt)) != HYB_SUCCESS)
+            return rc;
+        if (to)
+        {
+            o.status = HYB_DEVICE_TIMEOUT;
+            return HYB_SUCCESS;
+        }
+        o.relres = max_relative(rn2, bn2);
+        if (o.relres <= tol)
+            return HYB_SUCCESS;
+        if (o.iters >= max_iter || !std::isfinite(o.relres))
+        {
+            o.status = HYB_NOT_CONVERGED;
+            return HYB_SUCCESS;
+        }
+        hyb::k_normalize<<<eg, hyb::kThreads, 0, h->stream>>>(h->d_V, h->d_r, h->d_norm, dof, nr);
+        ++cnt;
+        std::fill(g.begin(), g.end(), 0.0);
+        for (int r = 0; r < nr; ++r)
+            g[(size_t)r * (m + 1)] = std::sqrt(std::max(rn2[r], 0.0));
+        int j = 0;
+        bool done = false;
+        while (j < m && o.iters < max_iter && !done)
+        {
+            double *vj = h->d_V + (size_t)j * len, *zj = h->d_Zk + (size_t)j * len;
+            if ((rc = apply_factors(h, vj, zj, nr, cnt)) != HYB_SUCCESS)
+                return rc;
+            enqueue_residual(h, nullptr, zj, h->d_w, nr, cnt); // w = A z_j
+            for (int i = 0; i <= j; ++i)
+            {
+                const double *vi = h->d_V + (size_t)i * len;
+                hyb::k_dot_partial<<<h->n_norm_parts, hyb::kThreads, 0, h->stream>>>(vi, h->d_w, dof, nr, h->d_part);
+                hyb::k_sumsq_final<<<1, 32, 0, h->stream>>>(h->d_part, h->n_norm_parts, nr, h->d_h + (size_t)i * nr);
+                hyb::k_sub_scaled<<<eg, hyb::kThreads, 0, h->stream>>>(h->d_w, vi, h->d_h + (size_t)i * nr, dof, nr);
+                cnt += 3;
+            }
+            enqueue_sumsq(h, h->d_w, dof, nr, h->d_h + (size_t)(j + 1) * nr, cnt);
+            hyb::k_normalize<<<eg, hyb::kThreads, 0, h->stream>>>(h->d_V + (size_t)(j + 1) * len, h->d_w,
+                                                                   h->d_h + (size_t)(j + 1) * nr, dof, nr);
+            ++cnt;
+            int sst[hyb::ST_WORDS];
+            HYB_CUDA(cudaMemcpyAsync(hcol.data(), h->d_h, (size_t)(j + 2) * nr * sizeof(double),
+                                     cudaMemcpyDeviceToHost, h->stream));
+            HYB_CUDA(cudaMemcpyAsync(sst, h->d_solve_status, sizeof(sst), cudaMemcpyDeviceToHost, h->stream));
+            HYB_CUDA(cudaStreamSynchronize(h->stream));
+            if (sst[hyb::ST_TIMEOUT])
+            {
+                o.status = HYB_DEVICE_TIMEOUT;
+                return HYB_SUCCESS;
+            }
+            ++o.iters;
+            ++o.krylov;
+            double est = 0;
+            for (int r = 0; r < nr; ++r)
+            {
+                auto Hc = [&](int i) -> double & { return H[((size_t)r * (m + 1) + i) * m + j]; };
+                for (int i = 0; i <= j; ++i)
+                    Hc(i) = hcol[(size_t)i * nr + r];
+                Hc(j + 1) = std::sqrt(std::max(hcol[(size_t)(j + 1) * nr + r], 0.0));
+                double *c = &cs[(size_t)r * m], *sv = &sn[(size_t)r * m], *gr = &g[(size_t)r * (m + 1)];
+                for (int i = 0; i < j; ++i)
+                {
+                    const double t = c[i] * Hc(i) + sv[i] * Hc(i + 1);
+                    Hc(i + 1) = -sv[i] * Hc(i) + c[i] * Hc(i + 1);
+                    Hc(i) = t;
+                }
+                const double a = Hc(j), bb = Hc(j + 1), d = std::hypot(a, bb);
+                c[j] = d > 0 ? a / d : 1.0;
+                sv[j] = d > 0 ? bb / d : 0.0;
+                Hc(j) = d;
+                Hc(j + 1) = 0;
+                gr[j + 1] = -sv[j] * gr[j];
+                gr[j] = c[j] * gr[j];
+                const double e = std::fabs(gr[j + 1]) / (bn2[r] > 0 ? std::sqrt(bn2[r]) : 1.0);
+                est = std::isnan(e) ? e : std::max(est, e);
+            }
+            ++j;
+            // the estimate is that of exact arithmetic: stop the cycle a little below the
+            // tolerance and let the recomputed residual decide
+            done = est <= 0.5 * tol;
+        }
+        // y = R^{-1} g on the j x j triangle, then x += Z y
+        for (int r = 0; r < nr; ++r)
+        {
+            const double *gr = &g[(size_t)r * (m + 1)];
+            std::vector<double> y(j);
+            for (int i = j - 1; i >= 0; --i)
+            {
+                double sum = gr[i];
+                for (int q = i + 1; q < j; ++q)
+                    sum -= H[((size_t)r * (m + 1) + i) * m + q] * y[q];
+                const double dii = H[((size_t)r * (m + 1) + i) * m + i];
+                y[i] = dii != 0 ? sum / dii : 0.0;
+            }
+            for (int i = 0; i < j; ++i)
+                coef[(size_t)i * nr + r] = y[i];
+        }
+        HYB_CUDA(cudaMemcpyAsync(h->d_coef, coef.data(), (size_t)j * nr * sizeof(double), cudaMemcpyHostToDevice,
+                                 h->stream));
+        hyb::k_add_combination<<<eg, hyb::kThreads, 0, h->stream>>>(h->d_x, h->d_Zk, len, h->d_coef, j, dof, nr);
+        ++cnt;
+    }
+}
+
+// x = M^{-1} b, then refinement: plain steps x += M^{-1} (b - A x) with the FP64 residual
+// (HYB_OPTION_REFINEMENT 0 and 1), continued by FGMRES (0, when a step shrinks the
+// residual less than kIrContraction, from the better of the last two iterates) or FGMRES
+// from the start (2).
+int refine(hyb_system *h, int nr, double tol, uint32_t max_iter, RefineResult &o, uint64_t &cnt)
+{
+    const Symbolic &S = h->S;
+    const int64_t len = S.dof_off[S.n] * nr;
+    const size_t bytes = len * sizeof(double);
+    int rc = apply_factors(h, h->d_b, h->d_x, nr, cnt);
+    if (rc != HYB_SUCCESS)
+        return rc;
+    std::vector<double> bn2, rn2;
+    bool to = false;
+    if ((rc = column_sumsq(h, h->d_b, nr, h->d_norm + nr, bn2, to, cnt)) != HYB_SUCCESS)
+        return rc;
+    double prev = INFINITY;
+    bool krylov = h->refinement == 2;
+    while (!krylov)
+    {
+        enqueue_residual(h, h->d_b, h->d_x, h->d_r, nr, cnt);
+        if ((rc = column_sumsq(h, h->d_r, nr, h->d_norm, rn2, to, cnt)) != HYB_SUCCESS)
+            return rc;
+        if (to)
+        {
+            o.status = HYB_DEVICE_TIMEOUT;
+            return HYB_SUCCESS;
+        }
+        o.relres = max_relative(rn2, bn2);
+        if (o.relres <= tol)
+            return HYB_SUCCESS;
+        if (h->refinement == 0 && o.iters > 0 && !(o.relres <= kIrContraction * prev))
+        {
+            if (!(o.relres <= prev)) // the last step made it worse: back to the iterate before it
+            {
+                HYB_CUDA(cudaMemcpyAsync(h->d_x, h->d_xb, bytes, cudaMemcpyDeviceToDevice, h->stream));
+                o.relres = prev;
+            }
+            krylov = true;
+            break;
+        }
+        if (o.iters >= max_iter || !std::isfinite(o.relres))
+        {
+            o.status = HYB_NOT_CONVERGED;
+            return HYB_SUCCESS;
+        }
+        if (h->refinement == 0)
+            HYB_CUDA(cudaMemcpyAsync(h->d_xb, h->d_x, bytes, cudaMemcpyDeviceToDevice, h->stream));
+        if ((rc = apply_factors(h, h->d_r, h->d_z, nr, cnt)) != HYB_SUCCESS)
+            return rc;
+        hyb::k_add_correction<double><<<elementwise_grid(len), hyb::kThreads, 0, h->stream>>>(h->d_x, h->d_z, len);
+        ++cnt;
+        ++o.iters;
+        prev = o.relres;
+    }
+    return fgmres(h, nr, tol, max_iter, bn2, o, cnt);
+}
+
+// ------------------------------------------------------------------------------------
+// Solves with A^T and the condition estimate.
+
+// Column view of the factors and of A (hyb::DevTrans), built and uploaded once per handle.
+int ensure_trans(hyb_system *h)
+{
+    if (h->t_arena)
+        return HYB_SUCCESS;
+    const Symbolic &S = h->S;
+    const int64_t n = S.n;
+    std::vector<int64_t> ucol_ptr(n + 1, 0), fu_pref(n + 1, 0), fu_rows(n + 1, 0), bu_pref(n + 1, 0),
+        bu_rows(n + 1, 0), acol_ptr(n + 1, 0);
+    for (int64_t k = 0; k < n; ++k)
+        for (int64_t j = S.diag_pos[k] + 1; j < S.row_ptr[k + 1]; ++j)
+            ++ucol_ptr[S.cols[j] + 1];
+    for (int64_t c = 0; c < n; ++c)
+        ucol_ptr[c + 1] += ucol_ptr[c];
+    std::vector<int32_t> ucol_row(ucol_ptr[n]), ucol_blk(ucol_ptr[n]);
+    {
+        std::vector<int64_t> next(ucol_ptr.begin(), ucol_ptr.end() - 1);
+        for (int64_t k = 0; k < n; ++k) // ascending rows within every column
+            for (int64_t j = S.diag_pos[k] + 1; j < S.row_ptr[k + 1]; ++j)
+            {
+                const int64_t e = next[S.cols[j]]++;
+                ucol_row[e] = (int32_t)k;
+                ucol_blk[e] = (int32_t)j;
+            }
+    }
+    for (int64_t p = 0; p < n; ++p)
+    {
+        const int64_t k = S.piv[p], m = S.size[k];
+        const int64_t nu = ucol_ptr[k + 1] - ucol_ptr[k], nl = S.lcol_ptr[k + 1] - S.lcol_ptr[k];
+        fu_pref[p + 1] = fu_pref[p] + std::max<int64_t>(1, nu);
+        fu_rows[p + 1] = fu_rows[p] + (nu * m + 3) / 4 * 4;
+        bu_pref[p + 1] = bu_pref[p] + std::max<int64_t>(1, nl);
+        bu_rows[p + 1] = bu_rows[p] + (nl * m + 3) / 4 * 4;
+    }
+    int64_t max_rows = 0;
+    for (int64_t l = 0; l < S.n_levels; ++l)
+    {
+        const int64_t p0 = S.lvl_ptr[l], p1 = S.lvl_ptr[l + 1];
+        max_rows = std::max({max_rows, fu_rows[p1] - fu_rows[p0], bu_rows[p1] - bu_rows[p0]});
+    }
+    const int64_t nnz_a = S.nnz_a();
+    for (int64_t j = 0; j < nnz_a; ++j)
+        ++acol_ptr[S.a_cols[j] + 1];
+    for (int64_t c = 0; c < n; ++c)
+        acol_ptr[c + 1] += acol_ptr[c];
+    std::vector<int32_t> acol_row(std::max<int64_t>(1, nnz_a)), acol_blk(std::max<int64_t>(1, nnz_a));
+    {
+        std::vector<int64_t> next(acol_ptr.begin(), acol_ptr.end() - 1);
+        for (int64_t r = 0; r < n; ++r)
+            for (int64_t j = S.a_row_ptr[r]; j < S.a_row_ptr[r + 1]; ++j)
+            {
+                const int64_t e = next[S.a_cols[j]]++;
+                acol_row[e] = (int32_t)r;
+                acol_blk[e] = (int32_t)j;
+            }
+    }
+    struct Item
+    {
+        const void *src;
+        size_t bytes;
+        const void **dst;
+    };
+    hyb::DevTrans &d = h->dt;
+    const std::vector<Item> items = {
+        {ucol_ptr.data(), ucol_ptr.size() * 8, (const void **)&d.ucol_ptr},
+        {ucol_row.data(), ucol_row.size() * 4, (const void **)&d.ucol_row},
+        {ucol_blk.data(), ucol_blk.size() * 4, (const void **)&d.ucol_blk},
+        {fu_pref.data(), fu_pref.size() * 8, (const void **)&d.fu_pref},
+        {fu_rows.data(), fu_rows.size() * 8, (const void **)&d.fu_rows},
+        {bu_pref.data(), bu_pref.size() * 8, (const void **)&d.bu_pref},
+        {bu_rows.data(), bu_rows.size() * 8, (const void **)&d.bu_rows},
+        {acol_ptr.data(), acol_ptr.size() * 8, (const void **)&d.acol_ptr},
+        {acol_row.data(), acol_row.size() * 4, (const void **)&d.acol_row},
+        {acol_blk.data(), acol_blk.size() * 4, (const void **)&d.acol_blk},
+    };
+    size_t total = 0;
+    for (const Item &it : items)
+        total += (it.bytes + 255) / 256 * 256 + 256;
+    std::vector<char> host(total, 0);
+    void *arena = nullptr;
+    HYB_CUDA(cudaMalloc(&arena, total));
+    size_t off = 0;
+    for (const Item &it : items)
+    {
+        if (it.bytes)
+            std::memcpy(host.data() + off, it.src, it.bytes);
+        *it.dst = (const char *)arena + off;
+        off += (it.bytes + 255) / 256 * 256 + 256;
+    }
+    const cudaError_t e = cudaMemcpy(arena, host.data(), total, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess)
+    {
+        cudaFree(arena);
+        return cuda_fail(e, "cudaMemcpy(transpose view)");
+    }
+    h->t_arena = arena;
+    h->t_max_rows = max_rows;
+    h->t_fu_pref = std::move(fu_pref);
+    h->t_bu_pref = std::move(bu_pref);
+    return HYB_SUCCESS;
+}
+
+// A^T y = z in place on y with the FP64 factors: the U^T pass by levels ascending, then
+// the L^T pass by levels descending.
+int enqueue_solve_transpose(hyb_system *h, double *y, double *scratch, int nrhs, uint64_t &launches)
+{
+    const Symbolic &S = h->S;
+    cudaStream_t st = h->stream;
+    HYB_CUDA(cudaMemsetAsync(h->d_tickets, 0, S.n * sizeof(int), st));
+    for (int64_t l = 0; l < S.n_levels; ++l)
+    {
+        const int64_t p0 = S.lvl_ptr[l], p1 = S.lvl_ptr[l + 1];
+        const int64_t units = h->t_fu_pref[p1] - h->t_fu_pref[p0];
+        hyb::k_fwdT_stage<double, double>
+            <<<(unsigned)units, hyb::kThreads, 0, st>>>(h->ds, h->dt, h->d_f64, y, scratch, h->d_tickets, p0, p1, nrhs);
+        ++launches;
+    }
+    for (int64_t l = S.n_levels - 1; l >= 0; --l)
+    {
+        const int64_t p0 = S.lvl_ptr[l], p1 = S.lvl_ptr[l + 1];
+        const int64_t units = h->t_bu_pref[p1] - h->t_bu_pref[p0];
+        const int smem = S.shape[l].max_piv * nrhs * (int)sizeof(double);
+        hyb::k_bwdT_stage<double, double><<<(unsigned)units, hyb::kThreads, smem, st>>>(
+            h->ds, h->dt, h->d_f64, y, scratch, h->d_tickets, p0, p1, nrhs);
+        ++launches;
+    }
+    HYB_CUDA(cudaGetLastError());
+    return HYB_SUCCESS;
+}
+
+// One solve of a host vector with A (plain FP64 substitution) or A^T, for the estimate.
+int solve_host_once(hyb_system *h, const double *in, double *out, bool transpose)
+{
+    const int64_t dof = h->S.dof_off[h->S.n];
+    HYB_CUDA(cudaMemcpyAsync(h->d_x, in, dof * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    int rc;
+    if (transpose)
+        rc = run_graph(h, h->g_solveT[1],
+                       [&](uint64_t &c) { return enqueue_solve_transpose(h, h->d_x, h->d_tscr, 1, c); });
+    else
+        rc = substitute<double, double>(h, h->d_f64, h->d_x, h->d_scr64, 1, h->g_solve[{HYB_PRECISION_FP64, 1}]);
+    if (rc != HYB_SUCCESS)
+        return rc;
+    HYB_CUDA(cudaMemcpyAsync(out, h->d_x, dof * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    HYB_CUDA(cudaStreamSynchronize(h->stream));
+    return HYB_SUCCESS;
+}
+
+// Scratch of the transposed solve's partial products for nrhs right-hand sides.
+int ensure_trans_scratch(hyb_system *h, int64_t nrhs)
+{
+    if (h->tscr_nrhs >= nrhs)
+        return HYB_SUCCESS;
+    cudaFree(h->d_tscr);
+    h->d_tscr = nullptr;
+    h->tscr_nrhs = 0;
+    h->g_solveT.clear();
+    HYB_CUDA(cudaMalloc(&h->d_tscr, (h->t_max_rows * nrhs + 1) * sizeof(double)));
+    h->tscr_nrhs = nrhs;
+    return HYB_SUCCESS;
+}
 
 } // namespace
 
@@ -1016,6 +1475,9 @@ HYB_API int hyb_system_copy(const hyb_system *src, hyb_system **out)
     h->umma = src->umma;
     h->flow = src->flow;
     h->wait_ns = src->wait_ns;
+    h->refinement = src->refinement;
+    h->fp64_refine = src->fp64_refine;
+    h->krylov_restart = src->krylov_restart;
     HYB_CUDA(create_streams(h.get()));
     int rc = upload_symbolic(h.get());
     if (rc != HYB_SUCCESS)
@@ -1101,6 +1563,21 @@ HYB_API int hyb_system_set_option(hyb_system *h, int option, int64_t value)
             return HYB_INVALID_ARGUMENT;
         h->wait_ns = (uint64_t)std::max<int64_t>(value, 100000);
         return HYB_SUCCESS;
+    case HYB_OPTION_REFINEMENT:
+        if (value < 0 || value > 2)
+            return HYB_INVALID_ARGUMENT;
+        h->refinement = (int)value;
+        return HYB_SUCCESS;
+    case HYB_OPTION_FP64_REFINEMENT:
+        h->fp64_refine = value != 0;
+        return HYB_SUCCESS;
+    case HYB_OPTION_KRYLOV_RESTART:
+        if (value < 1 || value > 200)
+            return HYB_INVALID_ARGUMENT;
+        if (value != h->krylov_restart)
+            h->free_krylov();
+        h->krylov_restart = (int)value;
+        return HYB_SUCCESS;
     case HYB_OPTION_WITHHOLD_ROW:
     {
         if (value < 0)
@@ -1172,6 +1649,7 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
     }
     h->last_launches = 0;
     h->factored = -1;
+    h->g_solveT.clear(); // captured with the FP64 slab's address, which may change below
     const unsigned sgrid = (unsigned)std::min<int64_t>(std::max<int64_t>(1, S.nnz_a()), 148 * 16);
     if (precision == HYB_PRECISION_FP64)
     {
@@ -1306,11 +1784,10 @@ HYB_API int hyb_solve(hyb_system *h, const double *b, double *x, uint64_t nrhs, 
         tol = 1e-12;
     HYB_CUDA(cudaMemcpyAsync(h->d_b, b, bytes, in, h->stream));
     HYB_CUDA(cudaMemsetAsync(h->d_solve_status, 0, hyb::ST_WORDS * sizeof(int), h->stream));
-    uint32_t iters = 0;
-    double relres = -1;
-    int status = HYB_SUCCESS;
-    if (h->factored == HYB_PRECISION_FP64)
+    RefineResult res;
+    if (h->factored == HYB_PRECISION_FP64 && !h->fp64_refine)
     {
+        // the plain drop-in solve: one substitution with the FP64 factors
         HYB_CUDA(cudaMemcpyAsync(h->d_x, h->d_b, bytes, cudaMemcpyDeviceToDevice, h->stream));
         auto &slot = h->g_solve[{HYB_PRECISION_FP64, nr}];
         rc = substitute<double, double>(h, h->d_f64, h->d_x, h->d_scr64, nr, slot);
@@ -1319,67 +1796,23 @@ HYB_API int hyb_solve(hyb_system *h, const double *b, double *x, uint64_t nrhs, 
         if (want_residual)
         {
             uint64_t cnt = 0;
+            std::vector<double> bn2, rn2;
+            bool to = false;
             enqueue_residual(h, h->d_b, h->d_x, h->d_r, nr, cnt);
-            enqueue_sumsq(h, h->d_r, dof, nr, h->d_norm, cnt);
-            enqueue_sumsq(h, h->d_b, dof, nr, h->d_norm + nr, cnt);
-            std::vector<double> nrm(2 * nr);
-            HYB_CUDA(cudaMemcpyAsync(nrm.data(), h->d_norm, 2 * nr * sizeof(double), cudaMemcpyDeviceToHost,
-                                     h->stream));
-            HYB_CUDA(cudaStreamSynchronize(h->stream));
-            relres = 0;
-            for (int r = 0; r < nr; ++r)
-                relres = std::max(relres, nrm[r + nr] > 0 ? std::sqrt(nrm[r] / nrm[r + nr]) : std::sqrt(nrm[r]));
+            if ((rc = column_sumsq(h, h->d_r, nr, h->d_norm, rn2, to, cnt)) != HYB_SUCCESS ||
+                (rc = column_sumsq(h, h->d_b, nr, h->d_norm + nr, bn2, to, cnt)) != HYB_SUCCESS)
+                return rc;
+            res.relres = max_relative(rn2, bn2);
             h->last_launches += cnt;
         }
     }
     else
     {
-        // Mixed: x0 = LU32^{-1} b, then x += LU32^{-1} (b - A x) with the FP64 residual.
         uint64_t cnt = 0;
-        auto &slot = h->g_solve[{HYB_PRECISION_MIXED, nr}];
-        auto solve32 = [&]() { return substitute<float, float>(h, h->d_f32, h->d_yf, h->d_scr32, nr, slot); };
-        hyb::k_convert<double, float><<<elementwise_grid(len), hyb::kThreads, 0, h->stream>>>(h->d_b, h->d_yf, len);
-        ++cnt;
-        rc = solve32();
+        rc = refine(h, nr, tol, max_iter, res, cnt);
+        h->last_launches += cnt;
         if (rc != HYB_SUCCESS)
             return rc;
-        hyb::k_convert<float, double><<<elementwise_grid(len), hyb::kThreads, 0, h->stream>>>(h->d_yf, h->d_x, len);
-        ++cnt;
-        enqueue_sumsq(h, h->d_b, dof, nr, h->d_norm + nr, cnt);
-        std::vector<double> nrm(2 * nr);
-        for (;;)
-        {
-            enqueue_residual(h, h->d_b, h->d_x, h->d_r, nr, cnt);
-            enqueue_sumsq(h, h->d_r, dof, nr, h->d_norm, cnt);
-            int sst[hyb::ST_WORDS];
-            HYB_CUDA(cudaMemcpyAsync(nrm.data(), h->d_norm, 2 * nr * sizeof(double), cudaMemcpyDeviceToHost,
-                                     h->stream));
-            HYB_CUDA(cudaMemcpyAsync(sst, h->d_solve_status, sizeof(sst), cudaMemcpyDeviceToHost, h->stream));
-            HYB_CUDA(cudaStreamSynchronize(h->stream));
-            if (sst[hyb::ST_TIMEOUT])
-                break; // reported below
-            relres = 0;
-            for (int r = 0; r < nr; ++r)
-                relres = std::max(relres, nrm[r + nr] > 0 ? std::sqrt(nrm[r] / nrm[r + nr]) : std::sqrt(nrm[r]));
-            if (!(relres > tol))
-                break;
-            if (iters >= max_iter || !std::isfinite(relres))
-            {
-                status = HYB_NOT_CONVERGED;
-                break;
-            }
-            hyb::k_convert<double, float><<<elementwise_grid(len), hyb::kThreads, 0, h->stream>>>(h->d_r, h->d_yf,
-                                                                                                len);
-            ++cnt;
-            rc = solve32();
-            if (rc != HYB_SUCCESS)
-                return rc;
-            hyb::k_add_correction<float><<<elementwise_grid(len), hyb::kThreads, 0, h->stream>>>(h->d_x, h->d_yf,
-                                                                                               len);
-            ++cnt;
-            ++iters;
-        }
-        h->last_launches += cnt;
     }
     HYB_CUDA(cudaGetLastError());
     HYB_CUDA(cudaMemcpyAsync(x, h->d_x, bytes, outk, h->stream));
@@ -1394,10 +1827,147 @@ HYB_API int hyb_solve(hyb_system *h, const double *b, double *x, uint64_t nrhs, 
     h->launches += h->last_launches;
     if (info)
     {
-        info->iterations = iters;
-        info->relative_residual = relres;
+        info->iterations = res.iters;
+        info->relative_residual = res.relres;
+        info->krylov_iterations = res.krylov;
     }
-    return status;
+    return res.status;
+}
+
+HYB_API int hyb_solve_transpose(hyb_system *h, const double *b, double *x, uint64_t nrhs, int memory)
+{
+    if (check_handle(h) || !b || !x || nrhs == 0 || nrhs > 1024)
+        return HYB_INVALID_ARGUMENT;
+    if (h->factored != HYB_PRECISION_FP64 || !h->d_f64)
+        return HYB_NOT_DECOMPOSED;
+    const Symbolic &S = h->S;
+    for (int64_t l = 0; l < S.n_levels; ++l)
+        if ((int64_t)S.shape[l].max_piv * (int64_t)nrhs * 8 > solve_smem_cap())
+            return HYB_TOO_LARGE;
+    int rc;
+    if ((rc = ensure_trans(h)) != HYB_SUCCESS || (rc = ensure_solve_buffers(h, (int64_t)nrhs)) != HYB_SUCCESS ||
+        (rc = ensure_trans_scratch(h, (int64_t)nrhs)) != HYB_SUCCESS)
+        return rc;
+    HYB_CUDA(allow_smem(hyb::k_bwdT_stage<double, double>, smem_optin()));
+    const size_t bytes = S.dof_off[S.n] * nrhs * sizeof(double);
+    const cudaMemcpyKind in = memory == HYB_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const cudaMemcpyKind outk = memory == HYB_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    HYB_CUDA(cudaMemcpyAsync(h->d_x, b, bytes, in, h->stream));
+    h->last_launches = 0;
+    const int nr = (int)nrhs;
+    rc = run_graph(h, h->g_solveT[nr], [&](uint64_t &c) { return enqueue_solve_transpose(h, h->d_x, h->d_tscr, nr, c); });
+    if (rc != HYB_SUCCESS)
+        return rc;
+    HYB_CUDA(cudaMemcpyAsync(x, h->d_x, bytes, outk, h->stream));
+    HYB_CUDA(cudaStreamSynchronize(h->stream));
+    h->launches += h->last_launches;
+    return HYB_SUCCESS;
+}
+
+HYB_API int hyb_condition_estimate(hyb_system *h, hyb_condition *out)
+{
+    if (check_handle(h) || !out)
+        return HYB_INVALID_ARGUMENT;
+    if (h->factored != HYB_PRECISION_FP64 || !h->d_f64)
+        return HYB_NOT_DECOMPOSED;
+    const Symbolic &S = h->S;
+    int rc;
+    if ((rc = ensure_trans(h)) != HYB_SUCCESS || (rc = ensure_solve_buffers(h, 1)) != HYB_SUCCESS ||
+        (rc = ensure_trans_scratch(h, 1)) != HYB_SUCCESS)
+        return rc;
+    HYB_CUDA(allow_smem(hyb::k_bwdT_stage<double, double>, smem_optin()));
+    const int64_t n = S.dof_off[S.n];
+    if (!h->d_colsum)
+        HYB_CUDA(cudaMalloc(&h->d_colsum, std::max<int64_t>(1, n) * sizeof(double)));
+    hyb::k_col_abs_sums<<<(unsigned)S.n, hyb::kThreads, 0, h->stream>>>(h->ds, h->dt, h->d_a, h->d_colsum);
+    HYB_CUDA(cudaGetLastError());
+    std::vector<double> v(n), y(n), z(n);
+    std::vector<int> sgn(n);
+    HYB_CUDA(cudaMemcpyAsync(v.data(), h->d_colsum, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    HYB_CUDA(cudaStreamSynchronize(h->stream));
+    double norm1 = 0;
+    for (double c : v)
+        norm1 = std::max(norm1, c);
+    // ||A^{-1}||_1 by Hager's method with Higham's refinements (Higham, ACM TOMS 14 (1988),
+    // Algorithm 4.1): the 1-norm of A^{-1} is the maximum of ||A^{-1} x||_1 over the unit
+    // vectors e_j; the gradient step z = A^{-T} sign(A^{-1} x) points at the next e_j to
+    // try, and a final alternating test vector guards against unlucky cases.
+    uint32_t solves = 0;
+    auto with_a = [&](const std::vector<double> &in, std::vector<double> &o) {
+        ++solves;
+        return solve_host_once(h, in.data(), o.data(), false);
+    };
+    auto with_at = [&](const std::vector<double> &in, std::vector<double> &o) {
+        ++solves;
+        return solve_host_once(h, in.data(), o.data(), true);
+    };
+    auto norm_1 = [](const std::vector<double> &a) {
+        double t = 0;
+        for (double e : a)
+            t += std::fabs(e);
+        return t;
+    };
+    auto argmax_abs = [](const std::vector<double> &a) {
+        size_t j = 0;
+        for (size_t i = 1; i < a.size(); ++i)
+            if (std::fabs(a[i]) > std::fabs(a[j]))
+                j = i;
+        return j;
+    };
+    std::fill(v.begin(), v.end(), 1.0 / (double)n);
+    if ((rc = with_a(v, y)) != HYB_SUCCESS)
+        return rc;
+    double est = norm_1(y);
+    if (n > 1)
+    {
+        for (int64_t i = 0; i < n; ++i)
+        {
+            sgn[i] = y[i] >= 0 ? 1 : -1;
+            v[i] = sgn[i];
+        }
+        if ((rc = with_at(v, z)) != HYB_SUCCESS)
+            return rc;
+        size_t j = argmax_abs(z);
+        for (int iter = 2;; ++iter)
+        {
+            std::fill(v.begin(), v.end(), 0.0);
+            v[j] = 1.0;
+            if ((rc = with_a(v, y)) != HYB_SUCCESS)
+                return rc;
+            const double old = est;
+            est = norm_1(y);
+            bool repeated = true;
+            for (int64_t i = 0; i < n && repeated; ++i)
+                repeated = (y[i] >= 0 ? 1 : -1) == sgn[i];
+            if (repeated || est <= old) // converged, or no longer increasing
+            {
+                est = std::max(est, old);
+                break;
+            }
+            for (int64_t i = 0; i < n; ++i)
+            {
+                sgn[i] = y[i] >= 0 ? 1 : -1;
+                v[i] = sgn[i];
+            }
+            if ((rc = with_at(v, z)) != HYB_SUCCESS)
+                return rc;
+            const size_t jlast = j;
+            j = argmax_abs(z);
+            if (z[jlast] == std::fabs(z[j]) || iter >= 5)
+                break;
+        }
+        // alternating test vector x_i = (-1)^i (1 + i / (n - 1))
+        for (int64_t i = 0; i < n; ++i)
+            v[i] = (i % 2 ? -1.0 : 1.0) * (1.0 + (double)i / (double)(n - 1));
+        if ((rc = with_a(v, y)) != HYB_SUCCESS)
+            return rc;
+        est = std::max(est, 2.0 * norm_1(y) / (3.0 * (double)n));
+    }
+    out->norm1 = norm1;
+    out->inv_norm1 = est;
+    out->kappa1 = norm1 * est;
+    out->solves = solves;
+    return HYB_SUCCESS;
 }
 
 HYB_API int hyb_row_count(const hyb_system *h, uint64_t row, uint64_t *count)

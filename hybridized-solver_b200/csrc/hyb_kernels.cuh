@@ -1942,7 +1942,8 @@ __global__ void __launch_bounds__(kThreads, 2)
 }
 
 // ----------------------------------------------------------------------------------
-// FP64 residual r = b - A x over the original pattern; one warp per scalar row.
+// FP64 residual r = b - A x over the original pattern (r = A x when b is null); one warp
+// per scalar row.
 __global__ void __launch_bounds__(kThreads)
     k_residual(DevSym S, const double *__restrict__ a, const double *__restrict__ b, const double *__restrict__ x,
                double *__restrict__ r, int64_t dof, int nrhs)
@@ -1979,7 +1980,7 @@ __global__ void __launch_bounds__(kThreads)
         for (int o = 16; o > 0; o >>= 1)
             s += __shfl_xor_sync(0xffffffffu, s, o);
         if (lane == 0)
-            r[g * nrhs + rr] = b[g * nrhs + rr] - s;
+            r[g * nrhs + rr] = b ? b[g * nrhs + rr] - s : s;
     }
 }
 

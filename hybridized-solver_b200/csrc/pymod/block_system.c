@@ -1361,7 +1361,7 @@ static PyObject *bs_solve(PyObject *self, PyTypeObject *cls, PyObject *const *ar
     }
     const uint64_t nrhs = PyArray_NDIM(arr) == 2 ? (uint64_t)PyArray_DIM(arr, 1) : 1;
     int st;
-    hyb_solve_info info = {0, -1.0};
+    hyb_solve_info info = {0, -1.0, 0};
     Py_BEGIN_ALLOW_THREADS;
     st = hyb_solve(s->dev, (const double *)PyArray_DATA(arr), (double *)PyArray_DATA(out), nrhs, HYB_MEMORY_HOST, tol,
                    (uint32_t)max_iter, s->precision == HYB_PRECISION_MIXED ? &info : NULL);

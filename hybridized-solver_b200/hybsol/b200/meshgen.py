@@ -22,6 +22,11 @@ Values, drawn from ``numpy.random.default_rng(seed)`` in this order:
    giving a diagonally dominant system;
 3. the right-hand sides ``U[-1, 1]`` of shape ``(dof,)`` or ``(dof, nrhs)``.
 
+Reduced-shift value sets scale the diagonal shift by ``alpha < 1`` (the same draws, so only
+the diagonals change). The system loses diagonal dominance and its condition number grows
+as ``alpha`` falls; ``tune_shift`` bisects ``alpha`` until a 1-norm condition estimate hits a
+target (1e6 for the ill-conditioned set), and ``REDUCED_SHIFT`` records the values found.
+
 The reference's coloring ("first") places all edges before all elements for this
 pattern, whatever the numbering, so the factorization sees the edge rows first.
 """
@@ -252,3 +257,103 @@ def block_diagonal(mats: list) -> BlockMatrix:
         np.concatenate(val_ptr),
         np.concatenate(vals),
     )
+
+
+# Shift scale alpha giving a 1-norm condition number of about 1e6 for the seed-0 mesh
+# system of (elements per side, p): found by tune_shift with the exact kappa_1 (dense
+# inverse) for the small meshes and with the library's Hager estimate from the FP64
+# factors on a B200 for the large ones. Value: (alpha, kappa_1 at alpha, how it was found).
+REDUCED_SHIFT: dict = {
+    (8, 8): (0.1146255054005839, 9.640e5, "exact kappa_1 (dense inverse)"),
+    (16, 4): (0.2513574752782007, 1.117e6, "exact kappa_1 (dense inverse)"),
+}
+
+
+def reduced_shift(n: int, p) -> float:
+    """The recorded shift scale of the ill-conditioned (kappa_1 ~ 1e6) set for this mesh."""
+    try:
+        return REDUCED_SHIFT[(int(n), int(p))][0]
+    except (KeyError, ValueError):
+        raise KeyError(
+            f"no reduced shift recorded for {n}x{n} p={p}: find it with `python -m hybsol.b200.tune_shift {n} {p}`"
+        ) from None
+
+
+def diagonal_weights(mat: BlockMatrix, shift_per_row: np.ndarray):
+    """Indices of the diagonal entries in ``mat.vals`` and the shift each one carries per
+    unit of ``alpha`` (its block row's ``sum of off-diagonal Frobenius norms + 1``)."""
+    idx, w = [], []
+    for r in range(mat.n_blocks):
+        b, e = int(mat.row_ptr[r]), int(mat.row_ptr[r + 1])
+        j = b + int(np.searchsorted(mat.cols[b:e], r))
+        s = int(mat.sizes[r])
+        idx.append(mat.val_ptr[j] + np.arange(s) * (s + 1))
+        w.append(np.full(s, shift_per_row[r]))
+    return np.concatenate(idx), np.concatenate(w)
+
+
+def row_shift_amounts(mat: BlockMatrix, n: int) -> np.ndarray:
+    """Per block row, the diagonal shift of ``alpha = 1``: the sum of the Frobenius norms of
+    the row's off-diagonal blocks, plus one (as the generator adds it)."""
+    out = np.ones(mat.n_blocks)
+    for r in range(mat.n_blocks):
+        for j in range(int(mat.row_ptr[r]), int(mat.row_ptr[r + 1])):
+            if int(mat.cols[j]) != r:
+                out[r] += np.linalg.norm(mat.vals[mat.val_ptr[j] : mat.val_ptr[j + 1]])
+    return out
+
+
+def shifted_values(mat: BlockMatrix, alpha_from: float, alpha_to: float, weights=None) -> np.ndarray:
+    """Values of ``mat`` (generated with shift ``alpha_from``) re-shifted to ``alpha_to``
+    without regenerating the draws (equal to ``mesh_system(shift=alpha_to)`` up to one
+    rounding of each diagonal entry). ``weights`` from ``diagonal_weights`` may be reused."""
+    idx, w = weights if weights is not None else diagonal_weights(mat, row_shift_amounts(mat, 0))
+    vals = mat.vals.copy()
+    vals[idx] += (alpha_to - alpha_from) * w
+    return vals
+
+
+def tune_shift(kappa_of_alpha, target: float = 1e6, tol_decades: float = 0.1, alpha_hi: float = 1.0,
+               max_steps: int = 30):
+    """Bisect the shift scale so that ``kappa_of_alpha(alpha)`` is within ``tol_decades``
+    (log10) of ``target``. Starts at ``alpha_hi`` (which must be better conditioned than
+    the target), halves alpha until the condition number passes the target, then bisects
+    the bracket in log alpha. Returns ``(alpha, kappa, [(alpha, kappa), ...])``."""
+    history = []
+
+    def kap(a):
+        k = float(kappa_of_alpha(a))
+        history.append((a, k))
+        return k
+
+    hi, k_hi = alpha_hi, kap(alpha_hi)
+    if not k_hi < target:
+        raise ValueError(f"alpha={alpha_hi} is already at kappa {k_hi:.3g} >= {target:.3g}")
+    lo = hi
+    for _ in range(max_steps):
+        lo = lo / 2
+        k_lo = kap(lo)
+        if abs(np.log10(k_lo / target)) <= tol_decades:
+            return lo, k_lo, history
+        if k_lo >= target:
+            break
+        hi, k_hi = lo, k_lo
+    else:
+        raise RuntimeError("no alpha above the target condition number was found")
+    for _ in range(max_steps):
+        mid = float(np.sqrt(lo * hi))
+        k_mid = kap(mid)
+        if abs(np.log10(k_mid / target)) <= tol_decades:
+            return mid, k_mid, history
+        if k_mid >= target:
+            lo = mid
+        else:
+            hi = mid
+    raise RuntimeError(f"bisection did not reach kappa {target:.3g} within {max_steps} steps: {history[-3:]}")
+
+
+def exact_kappa1(mat: BlockMatrix, vals=None) -> float:
+    """1-norm condition number from the dense inverse (small systems only)."""
+    m = mat if vals is None else BlockMatrix(mat.sizes, mat.row_ptr, mat.cols, mat.val_ptr, vals)
+    a = m.to_dense()
+    return float(np.abs(a).sum(axis=0).max() * np.abs(np.linalg.inv(a)).sum(axis=0).max())

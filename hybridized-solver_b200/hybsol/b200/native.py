@@ -31,6 +31,9 @@ OPTION_TENSOR_CORE_MIXED = 1
 OPTION_DATAFLOW_SOLVE = 2
 OPTION_WAIT_LIMIT_NS = 3
 OPTION_WITHHOLD_ROW = 4
+OPTION_REFINEMENT = 5  # 0 auto (refinement, then FGMRES when it stalls), 1 refinement only, 2 FGMRES
+OPTION_FP64_REFINEMENT = 6
+OPTION_KRYLOV_RESTART = 7
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _i64p = ctypes.POINTER(ctypes.c_int64)
@@ -53,10 +56,30 @@ class DecomposeInfo(ctypes.Structure):
 
 
 class SolveInfo(ctypes.Structure):
-    _fields_ = [("iterations", ctypes.c_uint32), ("relative_residual", ctypes.c_double)]
+    _fields_ = [
+        ("iterations", ctypes.c_uint32),
+        ("relative_residual", ctypes.c_double),
+        ("krylov_iterations", ctypes.c_uint32),
+    ]
 
     def as_dict(self) -> dict:
-        return {"iterations": self.iterations, "relative_residual": self.relative_residual}
+        return {
+            "iterations": self.iterations,
+            "relative_residual": self.relative_residual,
+            "krylov_iterations": self.krylov_iterations,
+        }
+
+
+class Condition(ctypes.Structure):
+    _fields_ = [
+        ("kappa1", ctypes.c_double),
+        ("norm1", ctypes.c_double),
+        ("inv_norm1", ctypes.c_double),
+        ("solves", ctypes.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 class Analysis(ctypes.Structure):
@@ -135,6 +158,11 @@ EXPORTS = {
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int],
     ),
+    "hyb_solve_transpose": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int],
+    ),
+    "hyb_condition_estimate": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Condition)]),
     "hyb_row_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _u64p]),
     "hyb_row_cols": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _u64p]),
     "hyb_get_block": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, _f64p]),
@@ -337,6 +365,20 @@ class NativeSystem:
         d = info.as_dict()
         d["converged"] = st == SUCCESS
         return d
+
+    def solve_transpose(self, b) -> np.ndarray:
+        """Solve A^T x = b (host arrays) with the FP64 factors."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.empty_like(b)
+        nrhs = 1 if b.ndim == 1 else b.shape[1]
+        _check(lib().hyb_solve_transpose(self._h, _ptr(b), _ptr(x), nrhs, MEMORY_HOST), "hyb_solve_transpose")
+        return x
+
+    def condition_estimate(self) -> dict:
+        """1-norm condition estimate from the FP64 factors (kappa1, norm1, inv_norm1, solves)."""
+        c = Condition()
+        _check(lib().hyb_condition_estimate(self._h, ctypes.byref(c)), "hyb_condition_estimate")
+        return c.as_dict()
 
     def residual(self, b, x) -> np.ndarray:
         b = np.ascontiguousarray(b, dtype=np.float64)

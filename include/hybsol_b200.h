@@ -85,8 +85,9 @@ typedef struct
 
 typedef struct
 {
-    uint32_t iterations;       /* refinement steps taken (0 for the plain form) */
-    double relative_residual;  /* max over columns of ||b - A x||_2 / ||b||_2 (FP64), -1 if not computed */
+    uint32_t iterations;         /* refinement steps taken: corrections applied (0 for the plain form) */
+    double relative_residual;    /* max over columns of ||b - A x||_2 / ||b||_2 (FP64), -1 if not computed */
+    uint32_t krylov_iterations;  /* of `iterations`, the FGMRES steps (see HYB_OPTION_REFINEMENT) */
 } hyb_solve_info;
 
 /* Library ----------------------------------------------------------------------- */
@@ -170,7 +171,20 @@ typedef enum
      * off): in the next dataflow solves the partial sums of block row `value` are never
      * released, so the waits for that row run out. The row must have at least two blocks
      * left of its diagonal. */
-    HYB_OPTION_WITHHOLD_ROW = 4
+    HYB_OPTION_WITHHOLD_ROW = 4,
+    /* How hyb_solve refines (mixed form, or the plain form with HYB_OPTION_FP64_REFINEMENT):
+     * 0 (default) iterative refinement x += LU^{-1} (b - A x) while each step shrinks the
+     * FP64 residual at least tenfold, then -- from the best iterate -- restarted FGMRES in
+     * FP64 preconditioned by the factors, which converges where plain refinement stalls
+     * (condition number x growth x factor precision near or above 1); 1 refinement only;
+     * 2 FGMRES from the first correction. Every step (a refinement step or an FGMRES
+     * iteration) costs one substitution with the factors. */
+    HYB_OPTION_REFINEMENT = 5,
+    /* 1: the plain FP64 form refines too (with its FP64 factors, as above), for systems
+     * whose plain FP64 solve misses the tolerance; 0 (default): the drop-in plain solve. */
+    HYB_OPTION_FP64_REFINEMENT = 6,
+    /* FGMRES restart length (Krylov vectors kept, 1..200, default 30). */
+    HYB_OPTION_KRYLOV_RESTART = 7
 } hyb_option;
 
 /* Sets a schedule option of the handle (takes effect at the next decomposition). */
@@ -198,6 +212,27 @@ HYB_API int hyb_solve(hyb_system *sys, const double *b, double *x, uint64_t nrhs
 
 /* FP64 residual r = b - A x against the original values (device or host vectors). */
 HYB_API int hyb_residual(hyb_system *sys, const double *b, const double *x, double *r, uint64_t nrhs, int memory);
+
+/* Solves A^T x = b with the FP64 factors (HYB_PRECISION_FP64; HYB_NOT_DECOMPOSED otherwise).
+ * No counterpart in the reference, whose factors only solve with A: with A = L U, A^T =
+ * U^T L^T, a forward pass with the transposed upper blocks (unit diagonal blocks) and a
+ * backward pass with the transposed lower blocks and diagonal-block LUs, level by level.
+ * `b` and `x` may alias. */
+HYB_API int hyb_solve_transpose(hyb_system *sys, const double *b, double *x, uint64_t nrhs, int memory);
+
+typedef struct
+{
+    double kappa1;    /* norm1 * inv_norm1: estimate of the 1-norm condition number */
+    double norm1;     /* ||A||_1 of the original values (exact: largest column sum of |a|) */
+    double inv_norm1; /* estimate of ||A^{-1}||_1 (a lower bound, usually within a small factor) */
+    uint32_t solves;  /* solves with A and A^T the estimate took */
+} hyb_condition;
+
+/* 1-norm condition estimate of the original matrix from its FP64 factors: Hager's method
+ * with Higham's refinements (the scheme of LAPACK's xLACN2: at most five sign-vector
+ * iterations, each a solve with A and one with A^T, plus one alternating test vector).
+ * No counterpart in the reference. Requires HYB_PRECISION_FP64 factors. */
+HYB_API int hyb_condition_estimate(hyb_system *sys, hyb_condition *out);
 
 /* Allocation-free FP64 solve. No counterpart in the reference: it exists for callers that
  * must not allocate device memory when they solve -- for example a host application

@@ -1,0 +1,146 @@
+"""Solves with A^T, the condition estimate, and refinement on the ill-conditioned sets.
+
+The reduced-shift value sets (diagonal shift scaled by the recorded alpha, 1-norm
+condition number about 1e6) are where plain iterative refinement with FP32 / BF16-split
+factors stalls or diverges (condition number x factor growth x factor precision near
+one). The mixed form then continues with FGMRES preconditioned by its factors. Solutions
+are checked against the oracle's FP64 factors with one FP64 refinement step.
+
+Bar for the forward error at kappa ~ 1e6: two solutions with relative residuals r1 and r2
+differ by at most about kappa_1 (r1 + r2) relative to the solution, so the 1e-11 agreement
+of the well-conditioned tests is out of reach by construction; the tests assert the
+residual contract (<= 1e-12) and that bound.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import rel_err, reorder_rhs
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(native, n, p, seed=0, shift=1.0, nrhs=1):
+    from hybsol.b200 import meshgen
+
+    mat, b = meshgen.mesh_system(n, p, seed=seed, nrhs=nrhs, shift=shift)
+    order = native.compute_ordering(mat.row_ptr, mat.cols, "first")
+    pm = mat.permuted(order)
+    return native.NativeSystem.from_matrix(pm), pm, reorder_rhs(mat.sizes, order, b)
+
+
+def _oracle_refined(pm, b):
+    """The oracle's FP64 solve plus one FP64 refinement step (its own factors)."""
+    osys = O.OracleSystem.from_csr(pm.sizes, pm.row_ptr, pm.cols, pm.vals)
+    osys.decompose()
+    x = osys.solve(b)
+    x = x + osys.solve(b - pm.matvec(x))
+    res = float(np.linalg.norm(b - pm.matvec(x)) / np.linalg.norm(b))
+    return x, res
+
+
+@pytest.mark.parametrize(("n", "p", "nrhs"), [(6, 4, 1), (8, 8, 3), (6, "rand", 2)])
+def test_transpose_solve_matches_dense(gpu, n, p, nrhs):
+    from hybsol.b200 import meshgen
+
+    pp = meshgen.random_orders(n, 2, 10, seed=4) if p == "rand" else p
+    ns, pm, bn = _system(gpu, n, pp, seed=9, nrhs=nrhs)
+    ns.decompose(gpu.FP64)
+    x = ns.solve_transpose(bn)
+    assert rel_err(x, np.linalg.solve(pm.to_dense().T, bn)) < 1e-12
+    x2 = ns.solve_transpose(bn)  # the cached launch graph gives the same bits
+    assert np.array_equal(x, x2)
+    ns.decompose(gpu.MIXED)  # FP32 factors: the transposed solve needs FP64 ones
+    with pytest.raises(gpu.HybError) as err:
+        ns.solve_transpose(bn)
+    assert err.value.status == 18
+
+
+@pytest.mark.parametrize(("n", "p", "reduced"), [(8, 8, False), (8, 8, True), (16, 4, True)])
+def test_condition_estimate_against_exact(gpu, n, p, reduced):
+    from hybsol.b200 import meshgen
+
+    alpha = meshgen.reduced_shift(n, p) if reduced else 1.0
+    ns, pm, _ = _system(gpu, n, p, shift=alpha)
+    ns.decompose(gpu.FP64)
+    c = ns.condition_estimate()
+    a = pm.to_dense()
+    exact = meshgen.exact_kappa1(pm)
+    assert c["norm1"] == pytest.approx(np.abs(a).sum(axis=0).max(), rel=1e-13)
+    # a lower bound on kappa_1 (up to the rounding of the solves) ...
+    assert c["kappa1"] <= exact * (1 + 1e-6)
+    # ... that Hager's method rarely misses by more than a small factor
+    assert c["kappa1"] >= exact / 10, (c, exact)
+    assert 3 <= c["solves"] <= 11
+
+
+@pytest.mark.parametrize(("n", "p"), [(8, 8), (16, 4)])
+@pytest.mark.parametrize("mode", [0, 2])
+def test_mixed_refines_the_ill_conditioned_set(gpu, n, p, mode):
+    from hybsol.b200 import meshgen
+
+    ns, pm, bn = _system(gpu, n, p, shift=meshgen.reduced_shift(n, p))
+    kappa = meshgen.exact_kappa1(pm)
+    ns.set_option(gpu.OPTION_REFINEMENT, mode)
+    ns.decompose(gpu.MIXED)
+    x, info = ns.solve(bn, max_iter=60)
+    assert info["converged"] and info["relative_residual"] <= 1e-12, info
+    if mode == 2:
+        assert info["krylov_iterations"] == info["iterations"]
+    xo, ro = _oracle_refined(pm, bn)
+    assert ro <= 1e-12
+    assert rel_err(x, xo) <= 10 * kappa * (info["relative_residual"] + ro), (rel_err(x, xo), info)
+
+
+def test_fp64_refinement_reaches_the_tolerance(gpu):
+    from hybsol.b200 import meshgen
+
+    ns, pm, bn = _system(gpu, 8, 8, shift=meshgen.reduced_shift(8, 8))
+    ns.decompose(gpu.FP64)
+    x0, i0 = ns.solve(bn)  # the plain drop-in solve: no refinement
+    assert i0["iterations"] == 0
+    ns.set_option(gpu.OPTION_FP64_REFINEMENT, 1)
+    x1, i1 = ns.solve(bn)
+    assert i1["converged"] and i1["relative_residual"] <= min(1e-12, i0["relative_residual"])
+    xo, ro = _oracle_refined(pm, bn)
+    kappa = meshgen.exact_kappa1(pm)
+    assert rel_err(x1, xo) <= 10 * kappa * (i1["relative_residual"] + ro)
+
+
+def test_refinement_modes_on_the_dominant_set(gpu):
+    """Where plain refinement converges fast the automatic mode never switches (same bits
+    as refinement only); FGMRES from the start reaches the same accuracy."""
+    ns, pm, bn = _system(gpu, 8, 8, seed=3, nrhs=3)
+    ns.decompose(gpu.MIXED)
+    xa, ia = ns.solve(bn)
+    ns.set_option(gpu.OPTION_REFINEMENT, 1)
+    xi, ii = ns.solve(bn)
+    assert np.array_equal(xa, xi) and ia["krylov_iterations"] == 0 and ia["iterations"] == ii["iterations"]
+    ns.set_option(gpu.OPTION_REFINEMENT, 2)
+    xg, ig = ns.solve(bn)
+    assert ig["converged"] and ig["krylov_iterations"] == ig["iterations"] >= 1
+    assert rel_err(xg, xa) < 1e-11
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_non_finite_solution_is_never_reported_converged(gpu, mode):
+    """A zero diagonal block makes the factors inf/nan (unpivoted, as the reference); the
+    refinement must report that it did not converge, never a residual of 0."""
+    from hybsol.b200 import meshgen
+
+    mat, b = meshgen.mesh_system(6, 4, seed=1)
+    order = gpu.compute_ordering(mat.row_ptr, mat.cols, "first")
+    pm = mat.permuted(order)
+    j = int(np.searchsorted(pm.cols[pm.row_ptr[0] : pm.row_ptr[1]], 0))  # block (0, 0)
+    pm.vals[pm.val_ptr[j] : pm.val_ptr[j + 1]] = 0.0
+    ns = gpu.NativeSystem.from_matrix(pm)
+    ns.set_option(gpu.OPTION_REFINEMENT, mode)
+    d = ns.decompose(gpu.MIXED)
+    assert d["zero_pivots"] >= 1
+    x, info = ns.solve(reorder_rhs(mat.sizes, order, b))
+    assert not info["converged"]
+    assert not (info["relative_residual"] <= 1e-12)
+    assert not np.isfinite(x).all()
