@@ -139,6 +139,14 @@ struct hyb_system
     int refinement = 0;                   // HYB_OPTION_REFINEMENT: 0 auto, 1 refinement only, 2 FGMRES
     bool fp64_refine = false;             // HYB_OPTION_FP64_REFINEMENT
     int krylov_restart = 30;              // HYB_OPTION_KRYLOV_RESTART
+    // independent systems stacked in one handle (hyb_system_set_segments): unknown offsets,
+    // their device copy, norms per segment and column, and the last solve's results
+    std::vector<int64_t> seg_off;
+    int64_t *d_seg_off = nullptr;
+    double *d_seg_norm = nullptr;
+    int64_t seg_norm_cap = 0;
+    std::vector<uint32_t> seg_first;
+    std::vector<double> seg_relres;
     void *arena = nullptr;
     DevSym ds{};
     double *d_a = nullptr; // original values (FP64, CSR order)
@@ -218,6 +226,8 @@ struct hyb_system
         cudaFree(d_ops);
         cudaFree(d_tgt);
         g_solveT.clear();
+        cudaFree(d_seg_off);
+        cudaFree(d_seg_norm);
         cudaFree(t_arena);
         cudaFree(d_tscr);
         cudaFree(d_colsum);
@@ -857,23 +867,56 @@ struct DevBuf
 // ------------------------------------------------------------------------------------
 // Refinement of the mixed form (and of the plain form with HYB_OPTION_FP64_REFINEMENT).
 
-// Squared 2-norms of the columns of v (dof x nr) into dev_out and `out` (host), with the
-// solve's status words read in the same synchronization.
+// Squared 2-norms of the columns of v (dof x nr) into dev_out (on the device) and `out`
+// (host) -- for a segmented system, of every segment of every column (nseg x nr) -- with
+// the solve's status words read in the same synchronization.
 int column_sumsq(hyb_system *h, const double *v, int nr, double *dev_out, std::vector<double> &out, bool &timed_out,
                  uint64_t &cnt)
 {
     const int64_t dof = h->S.dof_off[h->S.n];
     enqueue_sumsq(h, v, dof, nr, dev_out, cnt);
     int sst[hyb::ST_WORDS];
-    out.resize(nr);
-    HYB_CUDA(cudaMemcpyAsync(out.data(), dev_out, nr * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    const int64_t nseg = h->seg_off.empty() ? 0 : (int64_t)h->seg_off.size() - 1;
+    const double *src = dev_out;
+    if (nseg > 0)
+    {
+        if (h->seg_norm_cap < nseg * nr)
+        {
+            cudaFree(h->d_seg_norm);
+            h->d_seg_norm = nullptr;
+            h->seg_norm_cap = 0;
+            HYB_CUDA(cudaMalloc(&h->d_seg_norm, nseg * nr * sizeof(double)));
+            h->seg_norm_cap = nseg * nr;
+        }
+        hyb::k_sumsq_segments<<<(unsigned)nseg, hyb::kThreads, 0, h->stream>>>(v, h->d_seg_off, nr, h->d_seg_norm);
+        ++cnt;
+        src = h->d_seg_norm;
+    }
+    out.resize(nseg > 0 ? nseg * nr : nr);
+    HYB_CUDA(cudaMemcpyAsync(out.data(), src, out.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     HYB_CUDA(cudaMemcpyAsync(sst, h->d_solve_status, sizeof(sst), cudaMemcpyDeviceToHost, h->stream));
     HYB_CUDA(cudaStreamSynchronize(h->stream));
     timed_out = sst[hyb::ST_TIMEOUT] != 0;
     return HYB_SUCCESS;
 }
 
-// Largest relative residual over the columns.
+// Per segment and column, the steps after which its relative residual was first measured
+// at or below tol, and the latest relative residual (segmented systems).
+void record_segments(hyb_system *h, const std::vector<double> &rn2, const std::vector<double> &bn2, double tol,
+                     uint32_t iters)
+{
+    if (h->seg_off.empty())
+        return;
+    for (size_t i = 0; i < rn2.size(); ++i)
+    {
+        const double rel = bn2[i] > 0 ? std::sqrt(rn2[i] / bn2[i]) : std::sqrt(rn2[i]);
+        h->seg_relres[i] = rel;
+        if (rel <= tol && h->seg_first[i] == UINT32_MAX)
+            h->seg_first[i] = iters;
+    }
+}
+
+// Largest relative residual over the columns (segments and columns when segmented).
 double max_relative(const std::vector<double> &rn2, const std::vector<double> &bn2)
 {
     double m = 0;
@@ -946,6 +989,14 @@ int fgmres(hyb_system *h, int nr, double tol, uint32_t max_iter, const std::vect
     // per column r: H (m+1 x m, row i column j at (r * (m + 1) + i) * m + j), rotations, g
     std::vector<double> H((size_t)nr * (m + 1) * m), cs((size_t)nr * m), sn((size_t)nr * m), g((size_t)nr * (m + 1));
     std::vector<double> hcol((size_t)(m + 2) * nr), coef((size_t)m * nr), rn2;
+    // The Arnoldi estimate is the norm of a whole column; a column's residual is small
+    // enough for every segment once it is below tol times the smallest segment norm of b.
+    std::vector<double> col_scale(nr, INFINITY);
+    for (size_t i = 0; i < bn2.size(); ++i)
+    {
+        const double v = std::sqrt(bn2[i]);
+        col_scale[i % nr] = std::min(col_scale[i % nr], v > 0 ? v : 1.0);
+    }
     bool to = false;
     int rc;
     for (;;)
@@ -959,6 +1010,7 @@ int fgmres(hyb_system *h, int nr, double tol, uint32_t max_iter, const std::vect
             return HYB_SUCCESS;
         }
         o.relres = max_relative(rn2, bn2);
+        record_segments(h, rn2, bn2, tol, o.iters);
         if (o.relres <= tol)
             return HYB_SUCCESS;
         if (o.iters >= max_iter || !std::isfinite(o.relres))
@@ -969,8 +1021,11 @@ int fgmres(hyb_system *h, int nr, double tol, uint32_t max_iter, const std::vect
         hyb::k_normalize<<<eg, hyb::kThreads, 0, h->stream>>>(h->d_V, h->d_r, h->d_norm, dof, nr);
         ++cnt;
         std::fill(g.begin(), g.end(), 0.0);
+        std::vector<double> beta2(nr, 0.0); // column norms of r (the segments' sums when segmented)
+        for (size_t i = 0; i < rn2.size(); ++i)
+            beta2[i % nr] += rn2[i];
         for (int r = 0; r < nr; ++r)
-            g[(size_t)r * (m + 1)] = std::sqrt(std::max(rn2[r], 0.0));
+            g[(size_t)r * (m + 1)] = std::sqrt(std::max(beta2[r], 0.0));
         int j = 0;
         bool done = false;
         while (j < m && o.iters < max_iter && !done)
@@ -1024,7 +1079,7 @@ int fgmres(hyb_system *h, int nr, double tol, uint32_t max_iter, const std::vect
                 Hc(j + 1) = 0;
                 gr[j + 1] = -sv[j] * gr[j];
                 gr[j] = c[j] * gr[j];
-                const double e = std::fabs(gr[j + 1]) / (bn2[r] > 0 ? std::sqrt(bn2[r]) : 1.0);
+                const double e = std::fabs(gr[j + 1]) / col_scale[r];
                 est = std::isnan(e) ? e : std::max(est, e);
             }
             ++j;
@@ -1071,6 +1126,11 @@ int refine(hyb_system *h, int nr, double tol, uint32_t max_iter, RefineResult &o
     bool to = false;
     if ((rc = column_sumsq(h, h->d_b, nr, h->d_norm + nr, bn2, to, cnt)) != HYB_SUCCESS)
         return rc;
+    if (!h->seg_off.empty())
+    {
+        h->seg_first.assign(bn2.size(), UINT32_MAX);
+        h->seg_relres.assign(bn2.size(), -1.0);
+    }
     double prev = INFINITY;
     bool krylov = h->refinement == 2;
     while (!krylov)
@@ -1084,6 +1144,7 @@ int refine(hyb_system *h, int nr, double tol, uint32_t max_iter, RefineResult &o
             return HYB_SUCCESS;
         }
         o.relres = max_relative(rn2, bn2);
+        record_segments(h, rn2, bn2, tol, o.iters);
         if (o.relres <= tol)
             return HYB_SUCCESS;
         if (h->refinement == 0 && o.iters > 0 && !(o.relres <= kIrContraction * prev))
@@ -1598,6 +1659,43 @@ HYB_API int hyb_system_set_option(hyb_system *h, int option, int64_t value)
     }
 }
 
+HYB_API int hyb_system_set_segments(hyb_system *h, uint64_t nseg, const uint64_t *offsets)
+{
+    if (check_handle(h) || (nseg > 0 && !offsets))
+        return HYB_INVALID_ARGUMENT;
+    const int64_t dof = h->S.dof_off[h->S.n];
+    if (nseg > 0 && (offsets[0] != 0 || offsets[nseg] != (uint64_t)dof || nseg > (uint64_t)dof))
+        return HYB_INVALID_ARGUMENT;
+    for (uint64_t s = 0; s < nseg; ++s)
+        if (offsets[s + 1] <= offsets[s])
+            return HYB_INVALID_ARGUMENT;
+    cudaFree(h->d_seg_off);
+    h->d_seg_off = nullptr;
+    h->seg_off.clear();
+    h->seg_first.clear();
+    h->seg_relres.clear();
+    if (nseg == 0)
+        return HYB_SUCCESS;
+    std::vector<int64_t> off(offsets, offsets + nseg + 1);
+    HYB_CUDA(cudaMalloc(&h->d_seg_off, off.size() * sizeof(int64_t)));
+    HYB_CUDA(cudaMemcpy(h->d_seg_off, off.data(), off.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+    h->seg_off = std::move(off);
+    return HYB_SUCCESS;
+}
+
+HYB_API int hyb_segment_results(const hyb_system *h, uint32_t *iterations, double *relative_residual)
+{
+    if (check_handle(h) || h->seg_off.empty())
+        return HYB_INVALID_ARGUMENT;
+    if (h->seg_first.empty())
+        return HYB_NOT_DECOMPOSED; // no refined solve yet
+    if (iterations)
+        std::memcpy(iterations, h->seg_first.data(), h->seg_first.size() * sizeof(uint32_t));
+    if (relative_residual)
+        std::memcpy(relative_residual, h->seg_relres.data(), h->seg_relres.size() * sizeof(double));
+    return HYB_SUCCESS;
+}
+
 HYB_API int hyb_system_set_values(hyb_system *h, const double *values, int memory)
 {
     if (check_handle(h) || (!values && h->S.a_val_off.back() > 0))
@@ -1803,6 +1901,12 @@ HYB_API int hyb_solve(hyb_system *h, const double *b, double *x, uint64_t nrhs, 
                 (rc = column_sumsq(h, h->d_b, nr, h->d_norm + nr, bn2, to, cnt)) != HYB_SUCCESS)
                 return rc;
             res.relres = max_relative(rn2, bn2);
+            if (!h->seg_off.empty())
+            {
+                h->seg_first.assign(bn2.size(), UINT32_MAX);
+                h->seg_relres.assign(bn2.size(), -1.0);
+                record_segments(h, rn2, bn2, tol, 0);
+            }
             h->last_launches += cnt;
         }
     }

@@ -224,6 +224,35 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
+// Squared 2-norms of the segments of every column: out[s * nrhs + r] = sum over rows
+// [off[s], off[s+1]) of v[i][r]^2. One CTA per segment, a fixed-order reduction.
+__global__ void __launch_bounds__(kThreads)
+    k_sumsq_segments(const double *__restrict__ v, const int64_t *__restrict__ off, int nrhs, double *__restrict__ out)
+{
+    __shared__ double red[kThreads];
+    const int64_t seg = blockIdx.x, b = off[seg], e = off[seg + 1];
+    for (int r = 0; r < nrhs; ++r)
+    {
+        double s = 0;
+        for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x)
+        {
+            const double x = v[i * nrhs + r];
+            s += x * x;
+        }
+        red[threadIdx.x] = s;
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1)
+        {
+            if ((int)threadIdx.x < o)
+                red[threadIdx.x] += red[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0)
+            out[seg * nrhs + r] = red[0];
+        __syncthreads();
+    }
+}
+
 // y[i][r] -= coef[r] * x[i][r] (the coefficients stay on the device between launches).
 __global__ void k_sub_scaled(double *__restrict__ y, const double *__restrict__ x, const double *__restrict__ coef,
                              int64_t rows, int nrhs)

@@ -96,16 +96,36 @@ class BatchedSystem:
     def __init__(self, systems, strategy: str = "first"):
         self.layout = BatchLayout(systems, strategy)
         self.native = native.NativeSystem.from_matrix(self.layout.matrix)
+        # every system's unknowns are one contiguous range of the stack: refinement judges
+        # each system by its own residual, not by the norm of the whole stack
+        self.native.set_segments(self.layout.dof_off)
+        self._precision = None
 
     def set_values(self, systems):
         self.native.set_values(self.layout.values(systems))
 
     def decompose(self, precision: int = native.FP64) -> dict:
+        self._precision = precision
         return self.native.decompose(precision)
 
     def solve(self, rhs, tol: float = 1e-12, max_iter: int = 50):
-        """Solve every system for its right-hand side; returns (solutions, info)."""
-        x, info = self.native.solve(self.layout.to_solver(rhs), tol=tol, max_iter=max_iter)
+        """Solve every system for its right-hand side; returns (solutions, info). ``info``
+        is the stack's solve info plus ``systems``: per system, ``iterations`` (the
+        refinement steps after which its own relative residual first met ``tol``, None if
+        it never did) and ``relative_residual`` (its own ||b_i - A_i x_i|| / ||b_i||, the
+        largest over its right-hand sides)."""
+        b = self.layout.to_solver(rhs)
+        nrhs = 1 if b.ndim == 1 else b.shape[1]
+        x, info = self.native.solve(b, tol=tol, max_iter=max_iter)
+        first, rel = self.native.segment_results(nrhs)
+        never = np.iinfo(np.uint32).max
+        info["systems"] = [
+            {
+                "iterations": None if (first[i] == never).any() else int(first[i].max()),
+                "relative_residual": float(rel[i].max()),
+            }
+            for i in range(self.layout.count)
+        ]
         return self.layout.from_solver(x), info
 
     def close(self):

@@ -163,6 +163,8 @@ EXPORTS = {
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int],
     ),
     "hyb_condition_estimate": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Condition)]),
+    "hyb_system_set_segments": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _u64p]),
+    "hyb_segment_results": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), _f64p]),
     "hyb_row_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _u64p]),
     "hyb_row_cols": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _u64p]),
     "hyb_get_block": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, _f64p]),
@@ -379,6 +381,29 @@ class NativeSystem:
         c = Condition()
         _check(lib().hyb_condition_estimate(self._h, ctypes.byref(c)), "hyb_condition_estimate")
         return c.as_dict()
+
+    def set_segments(self, offsets):
+        """Independent systems stacked in this handle: segment s holds the unknowns
+        [offsets[s], offsets[s+1]). Refinement then converges every segment on its own."""
+        off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        self._nseg = max(0, len(off) - 1)
+        _check(
+            lib().hyb_system_set_segments(self._h, self._nseg, off.ctypes.data_as(_u64p) if self._nseg else None),
+            "hyb_system_set_segments",
+        )
+
+    def segment_results(self, nrhs: int = 1):
+        """(first converged step per segment and column, UINT32_MAX if never; final relative
+        residuals), each of shape (nseg, nrhs), after a refined solve."""
+        it = np.empty((self._nseg, nrhs), dtype=np.uint32)
+        rr = np.empty((self._nseg, nrhs), dtype=np.float64)
+        _check(
+            lib().hyb_segment_results(
+                self._h, it.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), rr.ctypes.data_as(_f64p)
+            ),
+            "hyb_segment_results",
+        )
+        return it, rr
 
     def residual(self, b, x) -> np.ndarray:
         b = np.ascontiguousarray(b, dtype=np.float64)

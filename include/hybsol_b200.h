@@ -86,7 +86,7 @@ typedef struct
 typedef struct
 {
     uint32_t iterations;         /* refinement steps taken: corrections applied (0 for the plain form) */
-    double relative_residual;    /* max over columns of ||b - A x||_2 / ||b||_2 (FP64), -1 if not computed */
+    double relative_residual;    /* max over columns (and segments) of ||b - A x||_2 / ||b||_2 (FP64), -1 if not computed */
     uint32_t krylov_iterations;  /* of `iterations`, the FGMRES steps (see HYB_OPTION_REFINEMENT) */
 } hyb_solve_info;
 
@@ -189,6 +189,21 @@ typedef enum
 
 /* Sets a schedule option of the handle (takes effect at the next decomposition). */
 HYB_API int hyb_system_set_option(hyb_system *sys, int option, int64_t value);
+
+/* Declares the system to be `nseg` independent systems stacked block-diagonally, segment s
+ * holding the unknowns [offsets[s], offsets[s+1]) (offsets[0] = 0, ascending, offsets[nseg]
+ * = dof). No counterpart in the reference. Refinement (mixed form, or the plain form with
+ * HYB_OPTION_FP64_REFINEMENT) then measures every segment's residual against its own
+ * right-hand side and iterates until each segment of each column meets the tolerance, so
+ * one badly scaled or ill-conditioned member of a batch is not declared converged by the
+ * norm of the whole stack. nseg = 0 removes the segmentation. */
+HYB_API int hyb_system_set_segments(hyb_system *sys, uint64_t nseg, const uint64_t *offsets);
+
+/* After hyb_solve on a segmented system, per segment and column (nseg x nrhs, row-major):
+ * the refinement steps after which its relative residual was first measured at or below
+ * the tolerance (UINT32_MAX if never) and its final relative residual ||b_s - (A x)_s|| /
+ * ||b_s|| (FP64). Either array may be NULL. */
+HYB_API int hyb_segment_results(const hyb_system *sys, uint32_t *iterations, double *relative_residual);
 
 /* Decomposition and solve -------------------------------------------------------- */
 

@@ -187,3 +187,38 @@ def test_batched_systems_share_stages(native):
         flops += a["factor_flops"]
     assert stacked["n_levels"] == max(levels) < sum(levels)
     assert stacked["factor_flops"] == pytest.approx(flops, rel=1e-12)
+
+
+@pytest.mark.gpu
+def test_every_batched_system_converges_on_its_own_residual(gpu):
+    """A batch of two well-conditioned systems and one ill-conditioned one (reduced shift,
+    kappa_1 ~ 1e6) whose right-hand side is scaled by 1e-12, so that it is invisible in
+    the norm of the whole stack: judged by the stack's norm the batch converges while that
+    system is far from converged; judged per system (the batch's segments) refinement
+    continues until it meets the tolerance too, and each system reports its own steps."""
+    from hybsol.b200 import batch, meshgen
+
+    easy1, b1 = meshgen.mesh_system(10, 4, seed=61)
+    easy2, b2 = meshgen.mesh_system(9, 3, seed=62)
+    hard, b3 = meshgen.mesh_system(8, 8, seed=0, shift=meshgen.reduced_shift(8, 8))
+    mats, rhs = [easy1, easy2, hard], [b1, b2, 1e-12 * b3]
+
+    def own_residuals(xs):
+        return [float(np.linalg.norm(m.matvec(x) - b) / np.linalg.norm(b)) for m, x, b in zip(mats, xs, rhs)]
+
+    bs = batch.BatchedSystem(mats)
+    bs.decompose(gpu.MIXED)
+    bs.native.set_segments([])  # judged by the whole stack
+    x, ig = bs.native.solve(bs.layout.to_solver(rhs), max_iter=60)
+    res_global = own_residuals(bs.layout.from_solver(x))
+    assert ig["converged"] and res_global[2] > 1e-10, (ig, res_global)
+    bs.native.set_segments(bs.layout.dof_off)  # judged system by system
+    xs, info = bs.solve(rhs, max_iter=80)
+    res = own_residuals(xs)
+    assert info["converged"] and max(res) <= 1e-12 * 1.01, (info, res)
+    per = info["systems"]
+    assert all(s["iterations"] is not None for s in per)
+    assert per[2]["iterations"] > max(per[0]["iterations"], per[1]["iterations"])
+    for s, r in zip(per, res):
+        assert s["relative_residual"] == pytest.approx(r, rel=1e-3, abs=1e-15)
+    bs.close()

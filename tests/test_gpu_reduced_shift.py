@@ -70,11 +70,19 @@ def test_condition_estimate_against_exact(gpu, n, p, reduced):
     a = pm.to_dense()
     exact = meshgen.exact_kappa1(pm)
     assert c["norm1"] == pytest.approx(np.abs(a).sum(axis=0).max(), rel=1e-13)
-    # a lower bound on kappa_1 (up to the rounding of the solves) ...
-    assert c["kappa1"] <= exact * (1 + 1e-6)
-    # ... that Hager's method rarely misses by more than a small factor
-    assert c["kappa1"] >= exact / 10, (c, exact)
-    assert 3 <= c["solves"] <= 11
+    ok = exact / 10 <= c["kappa1"] <= exact * (1 + 1e-6) and 3 <= c["solves"] <= 11
+    if not ok:  # what the estimate's solves gave, against dense ones
+        x = np.full(a.shape[0], 1.0 / a.shape[0])
+        y, _ = ns.solve(x, residual=False)
+        yd = np.linalg.solve(a, x)
+        sgn = np.where(yd >= 0, 1.0, -1.0)
+        z = ns.solve_transpose(sgn)
+        zd = np.linalg.solve(a.T, sgn)
+        again = ns.condition_estimate()
+        diag = dict(A_inv=rel_err(y, yd), A_invT=rel_err(z, zd), argmax=(int(np.abs(z).argmax()), int(np.abs(zd).argmax())), again=again)
+        raise AssertionError(f"estimate {c} against exact kappa_1 {exact}: {diag}")
+    # a lower bound on kappa_1 (up to the rounding of the solves) that Hager's method rarely
+    # misses by more than a small factor (checked together above)
 
 
 @pytest.mark.parametrize(("n", "p"), [(8, 8), (16, 4)])
