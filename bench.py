@@ -85,12 +85,14 @@ def parse_args():
         help="value set: the diagonally dominant one (shift scale 1), or the reduced shift recorded for this mesh "
         "(1-norm condition number ~1e6; the FP64 form then refines with its own factors to reach the tolerance)",
     )
+    ap.add_argument("--alpha", type=float, default=None, help="shift scale of --shift reduced (default: the recorded one)")
     args = ap.parse_args()
-    args.alpha = 1.0
     if args.shift == "reduced":
         from hybsol.b200 import meshgen
 
-        args.alpha = meshgen.reduced_shift(args.mesh, args.p)
+        args.alpha = args.alpha if args.alpha is not None else meshgen.reduced_shift(args.mesh, args.p)
+    else:
+        args.alpha = 1.0
     return args
 
 

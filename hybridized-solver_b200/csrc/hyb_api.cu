@@ -1320,8 +1320,15 @@ int solve_host_once(hyb_system *h, const double *in, double *out, bool transpose
         rc = substitute<double, double>(h, h->d_f64, h->d_x, h->d_scr64, 1, h->g_solve[{HYB_PRECISION_FP64, 1}]);
     if (rc != HYB_SUCCESS)
         return rc;
+    int sst[hyb::ST_WORDS];
     HYB_CUDA(cudaMemcpyAsync(out, h->d_x, dof * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    HYB_CUDA(cudaMemcpyAsync(sst, h->d_solve_status, sizeof(sst), cudaMemcpyDeviceToHost, h->stream));
     HYB_CUDA(cudaStreamSynchronize(h->stream));
+    if (sst[hyb::ST_TIMEOUT])
+    {
+        g_cuda_error = "a wait of the dataflow solve ran out of its time limit";
+        return HYB_DEVICE_TIMEOUT;
+    }
     return HYB_SUCCESS;
 }
 
@@ -1981,6 +1988,7 @@ HYB_API int hyb_condition_estimate(hyb_system *h, hyb_condition *out)
         return rc;
     HYB_CUDA(allow_smem(hyb::k_bwdT_stage<double, double>, smem_optin()));
     const int64_t n = S.dof_off[S.n];
+    HYB_CUDA(cudaMemsetAsync(h->d_solve_status, 0, hyb::ST_WORDS * sizeof(int), h->stream));
     if (!h->d_colsum)
         HYB_CUDA(cudaMalloc(&h->d_colsum, std::max<int64_t>(1, n) * sizeof(double)));
     hyb::k_col_abs_sums<<<(unsigned)S.n, hyb::kThreads, 0, h->stream>>>(h->ds, h->dt, h->d_a, h->d_colsum);
