@@ -266,6 +266,9 @@ def block_diagonal(mats: list) -> BlockMatrix:
 REDUCED_SHIFT: dict = {
     (8, 8): (0.1146255054005839, 9.640e5, "exact kappa_1 (dense inverse)"),
     (16, 4): (0.2513574752782007, 1.117e6, "exact kappa_1 (dense inverse)"),
+    (32, 8): (0.2013112914936568, 1.206e6, "Hager estimate from the FP64 factors on a B200"),
+    (64, 8): (0.2420077241865368, 1.090e6, "Hager estimate from the FP64 factors on a B200"),
+    (128, 8): (0.25, 1.008e6, "Hager estimate from the FP64 factors on a B200"),
 }
 
 
