@@ -64,6 +64,13 @@ def parse_args():
         help="element order: an integer, or 'rand' for a per-element order drawn uniformly from 2..10 (seed 0)",
     )
     ap.add_argument("--cpu-sample-mesh", type=int, default=CPU_SAMPLE_MESH)
+    ap.add_argument(
+        "--ref-threads",
+        type=int,
+        default=0,
+        help="threads of the reference's decompose (default: every host core the process may use)",
+    )
+    ap.add_argument("--ref-child", nargs=6, metavar=("N", "P", "STEPS", "WARMUP", "THREADS", "OUT"), help=argparse.SUPPRESS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-profile", action="store_true", help="do not time the dominant kernel with events")
     ap.add_argument(
@@ -260,7 +267,45 @@ def load_meshgen():
     return mod
 
 
+# The reference's multi-threaded decompose can hang: its phase-2 scheduler (src/blocks.c
+# of the reference, the claim loop of block_system_decompose) spins on plain, unsynchronised
+# reads of the target states, the open-target count and the search start, which the
+# compiler may hoist out of the loops; on small systems, where most threads spin, a run
+# occasionally never returns. Each sample therefore runs in a child process with a time
+# limit, and is retried once.
+REF_CHILD_TIMEOUT_S = 900
+
+
 def reference_sample(n, p, steps, warmup, threads):
+    """reference_sample_inline in a child process (see above); raises RuntimeError when
+    both tries ran out of time."""
+    import numpy as np
+
+    for attempt in range(2):
+        with tempfile.TemporaryDirectory() as tmp:
+            out = os.path.join(tmp, "ref.npz")
+            cmd = [sys.executable, str(Path(__file__).resolve()), "--ref-child", str(n), str(p), str(steps),
+                   str(warmup), str(threads), out]
+            env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+            try:
+                subprocess.run(cmd, check=True, timeout=REF_CHILD_TIMEOUT_S, env=env, stdout=subprocess.DEVNULL)
+            except subprocess.TimeoutExpired:
+                continue
+            d = np.load(out)
+            return list(d["times"]), float(d["res"]), d["x"], float(d["flops"])
+    raise RuntimeError(f"the reference's decompose did not return within {REF_CHILD_TIMEOUT_S} s, twice")
+
+
+def reference_child(args):
+    import numpy as np
+
+    n, p, steps, warmup, threads, out = args.ref_child
+    times, res, x, flops = reference_sample_inline(int(n), p, int(steps), int(warmup), int(threads))
+    np.savez(out, times=np.asarray(times), res=res, x=x, flops=flops)
+    return 0
+
+
+def reference_sample_inline(n, p, steps, warmup, threads):
     """Decompose + solve of the reference extension (compiled from its own sources in
     oracle/_ref) on the n x n mesh, through its public BlockSystem API: assembly, the
     reference's coloring, reorder_blocks, decompose(n_threads) and solve. Returns the
@@ -298,13 +343,12 @@ def sample_workload_name(n, p):
     return workload_config(n, p)["workload"]
 
 
-def cpu_baseline(full_flops, p, sample_mesh):
+def cpu_baseline(full_flops, p, sample_mesh, threads=0):
     """The reference on the box's host cores, on the sample mesh; `value` extrapolates
     the measured time to the benchmarked workload by algorithmic GFLOP (marked as such)."""
     from oracle import oracle as O
 
-    cores = O.cpu_count()
-    os.environ["OMP_NUM_THREADS"] = str(cores)
+    cores = threads or O.cpu_count()
     times, res, x, sample_flops = reference_sample(sample_mesh, p, 1, 0, cores)
     best = min(times)
     scale = full_flops / sample_flops
@@ -339,10 +383,13 @@ def run_reference(args):
     if not O.reference_available():
         print(json.dumps({"impl": "reference", "unavailable": "reference extension not built (oracle/_ref missing)"}))
         return 0
-    cores = O.cpu_count()
-    os.environ["OMP_NUM_THREADS"] = str(cores)
+    cores = args.ref_threads or O.cpu_count()
     n = args.cpu_sample_mesh
-    times, res, _, flops = reference_sample(n, args.p, args.steps, args.warmup, cores)
+    try:
+        times, res, _, flops = reference_sample(n, args.p, args.steps, args.warmup, cores)
+    except RuntimeError as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"{e} (a data race in its OpenMP scheduler)"}))
+        return 0
     ms = statistics.mean(times) * 1e3
     cpu = {
         "value": ms,
@@ -679,8 +726,11 @@ def run_ours(args):
         from oracle import oracle as O
 
         if O.reference_available():
-            cpu, x_ref = cpu_baseline(flops, args.p, args.cpu_sample_mesh)
-            pair = same_mesh_pair(args, x_ref, cpu["sample_ms"])
+            try:
+                cpu, x_ref = cpu_baseline(flops, args.p, args.cpu_sample_mesh, args.ref_threads)
+                pair = same_mesh_pair(args, x_ref, cpu["sample_ms"])
+            except RuntimeError as e:
+                cpu = {"unavailable": str(e)}
     if rank == 0:
         line = {
             "metric": METRIC,
@@ -748,6 +798,8 @@ def run_ours(args):
 
 def main():
     args = parse_args()
+    if args.ref_child:
+        return reference_child(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.single:

@@ -108,6 +108,8 @@ __global__ void k_status_init(int *st)
         st[hyb::ST_NON_FINITE] = 0;
         st[hyb::ST_FIRST_BAD] = INT_MAX;
         st[3] = 0;
+        st[hyb::ST_GROWTH_FP64] = 0;
+        st[hyb::ST_GROWTH_KEPT] = 0;
     }
 }
 
@@ -139,6 +141,16 @@ struct hyb_system
     int refinement = 0;                   // HYB_OPTION_REFINEMENT: 0 auto, 1 refinement only, 2 FGMRES
     bool fp64_refine = false;             // HYB_OPTION_FP64_REFINEMENT
     int krylov_restart = 30;              // HYB_OPTION_KRYLOV_RESTART
+    float growth_limit = 1024.0f;         // HYB_OPTION_GROWTH_LIMIT (mixed form)
+    bool block_scaling = false;           // HYB_OPTION_BLOCK_SCALING (mixed form)
+    bool factors_scaled = false;          // the current mixed factors are those of S A S
+    double *d_bscale = nullptr;           // s_k per block row
+    double *d_dscale = nullptr;           // s_k per unknown
+    // mixed form, pivots of at most hyb::kGrowthSmallRows rows: FP64 LU of a high-growth
+    // pivot (offsets per block row, -1 for larger ones) and the flags k_trsm reads
+    int *d_hg = nullptr;
+    double *d_piv64 = nullptr;
+    int64_t *d_g64_off = nullptr;
     // independent systems stacked in one handle (hyb_system_set_segments): unknown offsets,
     // their device copy, norms per segment and column, and the last solve's results
     std::vector<int64_t> seg_off;
@@ -228,6 +240,11 @@ struct hyb_system
         g_solveT.clear();
         cudaFree(d_seg_off);
         cudaFree(d_seg_norm);
+        cudaFree(d_hg);
+        cudaFree(d_bscale);
+        cudaFree(d_dscale);
+        cudaFree(d_piv64);
+        cudaFree(d_g64_off);
         cudaFree(t_arena);
         cudaFree(d_tscr);
         cudaFree(d_colsum);
@@ -424,6 +441,8 @@ template <typename T> int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cuda
     const int optin = smem_optin();
     const int64_t p0 = S.lvl_ptr[l], p1 = S.lvl_ptr[l + 1];
     const Symbolic::LevelShape &sh = S.shape[l];
+    // growth check and FP64 fallback of the mixed form (0: off, and always for FP64 factors)
+    const float glim = std::is_same_v<T, float> && h->d_hg ? h->growth_limit : 0.0f;
     if (sh.max_piv > 32 && sh.max_piv <= 64 && sh.max_up <= 128)
     {
         // fused: diagonal LU (padded to 64x64) and the solves of the pivot rows' upper blocks;
@@ -432,30 +451,35 @@ template <typename T> int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cuda
         const dim3 grid((unsigned)units, sh.max_up > 64 ? 2u : 1u);
         if (sh.piv64) // every pivot and upper block exactly 64: no padding
             hyb::k_lu_trsm64<T, false><<<grid, hyb::kThreads, hyb::lu_trsm64_smem<T>(), st>>>(
-                ds, slab, p0, p1, ds.lu_pref, h->d_lu_tickets, h->d_status);
+                ds, slab, p0, p1, ds.lu_pref, h->d_lu_tickets, h->d_status, glim);
         else
             hyb::k_lu_trsm64<T, true><<<grid, hyb::kThreads, hyb::lu_trsm64_smem<T>(), st>>>(
-                ds, slab, p0, p1, ds.lu_pref, h->d_lu_tickets, h->d_status);
+                ds, slab, p0, p1, ds.lu_pref, h->d_lu_tickets, h->d_status, glim);
         ++launches;
         HYB_LAUNCHED("k_lu_trsm64", l);
         return enqueue_split<T>(h, slab, l, st, launches);
     }
     const int lu_bytes = lu_smem_bytes<T>(sh.max_piv);
+    int *hg = glim > 0 ? h->d_hg : nullptr;
     if (lu_bytes <= optin)
-        hyb::k_lu<T, true><<<(unsigned)(p1 - p0), hyb::kThreads, lu_bytes, st>>>(ds, slab, p0, h->d_status);
+        hyb::k_lu<T, true><<<(unsigned)(p1 - p0), hyb::kThreads, lu_bytes, st>>>(ds, slab, p0, h->d_status, glim, hg,
+                                                                                 h->d_piv64, h->d_g64_off);
     else
-        hyb::k_lu<T, false><<<(unsigned)(p1 - p0), hyb::kThreads, 0, st>>>(ds, slab, p0, h->d_status);
+        hyb::k_lu<T, false><<<(unsigned)(p1 - p0), hyb::kThreads, 0, st>>>(ds, slab, p0, h->d_status, glim, hg,
+                                                                          h->d_piv64, h->d_g64_off);
     ++launches;
     HYB_LAUNCHED("k_lu", l);
     const int64_t n_trsm = S.trsm_pref[p1] - S.trsm_pref[p0];
     if (n_trsm > 0)
     {
         dim3 grid((unsigned)n_trsm, (unsigned)((sh.max_up + hyb::kTile - 1) / hyb::kTile));
-        const int bytes = trsm_smem_bytes<T>(sh.max_piv);
+        int bytes = trsm_smem_bytes<T>(sh.max_piv);
+        if (hg && sh.max_piv <= hyb::kGrowthSmallRows) // room for an FP64 strip of a refactored pivot
+            bytes = std::max(bytes, sh.max_piv * (hyb::kTile | 1) * (int)sizeof(double));
         if (bytes <= optin)
-            hyb::k_trsm<T, true><<<grid, hyb::kThreads, bytes, st>>>(ds, slab, p0, p1);
+            hyb::k_trsm<T, true><<<grid, hyb::kThreads, bytes, st>>>(ds, slab, p0, p1, hg, h->d_piv64, h->d_g64_off);
         else
-            hyb::k_trsm<T, false><<<grid, hyb::kThreads, 0, st>>>(ds, slab, p0, p1);
+            hyb::k_trsm<T, false><<<grid, hyb::kThreads, 0, st>>>(ds, slab, p0, p1, hg, h->d_piv64, h->d_g64_off);
         ++launches;
         HYB_LAUNCHED("k_trsm", l);
     }
@@ -565,6 +589,8 @@ template <typename T> int enqueue_factor(hyb_system *h, T *slab, uint64_t &launc
     k_status_init<<<1, 32, 0, st>>>(h->d_status);
     ++launches;
     HYB_CUDA(cudaMemsetAsync(h->d_lu_tickets, 0, S.n * sizeof(int), st)); // an aborted run may leave tickets
+    if (std::is_same_v<T, float> && h->d_hg)
+        HYB_CUDA(cudaMemsetAsync(h->d_hg, 0, S.n * sizeof(int), st));
     int rc = HYB_SUCCESS;
     bool next_pivots_issued = false, forked = false;
     for (int64_t l = 0; l < S.n_levels; ++l)
@@ -937,12 +963,21 @@ int apply_factors(hyb_system *h, const double *v, double *z, int nr, uint64_t &c
     const int64_t len = h->S.dof_off[h->S.n] * nr;
     if (h->factored == HYB_PRECISION_MIXED)
     {
-        hyb::k_convert<double, float><<<elementwise_grid(len), hyb::kThreads, 0, h->stream>>>(v, h->d_yf, len);
+        const int64_t dof = h->S.dof_off[h->S.n];
+        const unsigned eg = elementwise_grid(len);
+        // with scaled factors (of S A S): A^{-1} v ~ S (LU)^{-1} (S v)
+        if (h->factors_scaled)
+            hyb::k_convert_scaled<double, float><<<eg, hyb::kThreads, 0, h->stream>>>(v, h->d_yf, h->d_dscale, dof, nr);
+        else
+            hyb::k_convert<double, float><<<eg, hyb::kThreads, 0, h->stream>>>(v, h->d_yf, len);
         auto &slot = h->g_solve[{HYB_PRECISION_MIXED, nr}];
         const int rc = substitute<float, float>(h, h->d_f32, h->d_yf, h->d_scr32, nr, slot);
         if (rc != HYB_SUCCESS)
             return rc;
-        hyb::k_convert<float, double><<<elementwise_grid(len), hyb::kThreads, 0, h->stream>>>(h->d_yf, z, len);
+        if (h->factors_scaled)
+            hyb::k_convert_scaled<float, double><<<eg, hyb::kThreads, 0, h->stream>>>(h->d_yf, z, h->d_dscale, dof, nr);
+        else
+            hyb::k_convert<float, double><<<eg, hyb::kThreads, 0, h->stream>>>(h->d_yf, z, len);
         cnt += 2;
         return HYB_SUCCESS;
     }
@@ -1546,6 +1581,8 @@ HYB_API int hyb_system_copy(const hyb_system *src, hyb_system **out)
     h->refinement = src->refinement;
     h->fp64_refine = src->fp64_refine;
     h->krylov_restart = src->krylov_restart;
+    h->growth_limit = src->growth_limit;
+    h->block_scaling = src->block_scaling;
     HYB_CUDA(create_streams(h.get()));
     int rc = upload_symbolic(h.get());
     if (rc != HYB_SUCCESS)
@@ -1645,6 +1682,18 @@ HYB_API int hyb_system_set_option(hyb_system *h, int option, int64_t value)
         if (value != h->krylov_restart)
             h->free_krylov();
         h->krylov_restart = (int)value;
+        return HYB_SUCCESS;
+    case HYB_OPTION_BLOCK_SCALING:
+        h->block_scaling = value != 0;
+        return HYB_SUCCESS;
+    case HYB_OPTION_GROWTH_LIMIT:
+        if (value < 0)
+            return HYB_INVALID_ARGUMENT;
+        if ((float)value != h->growth_limit)
+        {
+            h->growth_limit = (float)value;
+            h->g_factor[1].reset();
+        }
         return HYB_SUCCESS;
     case HYB_OPTION_WITHHOLD_ROW:
     {
@@ -1774,7 +1823,7 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
             h->g_solve.clear();
         }
         HYB_CUDA(cudaMemsetAsync(h->d_f64, 0, slab * sizeof(double), h->stream));
-        hyb::k_scatter<double><<<sgrid, hyb::kThreads, 0, h->stream>>>(h->ds, h->d_a, h->d_f64, S.nnz_a());
+        hyb::k_scatter<double><<<sgrid, hyb::kThreads, 0, h->stream>>>(h->ds, h->d_a, h->d_f64, S.nnz_a(), nullptr);
         h->last_launches += 1;
         const int rc = run_graph(h, h->g_factor[0], [&](uint64_t &count) {
             h->free_profile_events();
@@ -1801,6 +1850,23 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
             h->g_factor[1].reset();
             h->g_solve.clear();
         }
+        if (!h->d_hg)
+        {
+            // FP64 LU slots for the high-growth fallback of pivots of at most kGrowthSmallRows rows
+            std::vector<int64_t> off(S.n, -1);
+            int64_t total = 0;
+            for (int64_t k = 0; k < S.n; ++k)
+                if (S.size[k] <= hyb::kGrowthSmallRows)
+                {
+                    off[k] = total;
+                    total += (int64_t)S.size[k] * S.size[k];
+                }
+            HYB_CUDA(cudaMalloc(&h->d_hg, S.n * sizeof(int)));
+            HYB_CUDA(cudaMalloc(&h->d_piv64, std::max<int64_t>(1, total) * sizeof(double)));
+            HYB_CUDA(cudaMalloc(&h->d_g64_off, S.n * sizeof(int64_t)));
+            HYB_CUDA(cudaMemcpy(h->d_g64_off, off.data(), S.n * sizeof(int64_t), cudaMemcpyHostToDevice));
+            h->g_factor[1].reset();
+        }
         if (h->umma && !h->d_ops && S.max_split_blocks > 0)
         {
             h->split_half = (size_t)S.max_split_blocks * hyb::kSplitBytes;
@@ -1810,7 +1876,20 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
             h->g_factor[1].reset();
         }
         HYB_CUDA(cudaMemsetAsync(h->d_f32, 0, slab * sizeof(float), h->stream));
-        hyb::k_scatter<float><<<sgrid, hyb::kThreads, 0, h->stream>>>(h->ds, h->d_a, h->d_f32, S.nnz_a());
+        h->factors_scaled = false;
+        if (h->block_scaling)
+        {
+            if (!h->d_bscale)
+            {
+                HYB_CUDA(cudaMalloc(&h->d_bscale, S.n * sizeof(double)));
+                HYB_CUDA(cudaMalloc(&h->d_dscale, std::max<int64_t>(1, S.dof_off[S.n]) * sizeof(double)));
+            }
+            hyb::k_block_scales<<<(unsigned)S.n, 128, 0, h->stream>>>(h->ds, h->d_a, h->d_bscale, h->d_dscale);
+            h->last_launches += 1;
+            h->factors_scaled = true;
+        }
+        hyb::k_scatter<float><<<sgrid, hyb::kThreads, 0, h->stream>>>(h->ds, h->d_a, h->d_f32, S.nnz_a(),
+                                                                       h->factors_scaled ? h->d_bscale : nullptr);
         h->last_launches += 1;
         const int rc = run_graph(h, h->g_factor[1], [&](uint64_t &count) {
             h->free_profile_events();
@@ -1839,6 +1918,8 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
         info->zero_pivots = (uint64_t)st[hyb::ST_ZERO_PIVOTS];
         info->non_finite = (uint64_t)st[hyb::ST_NON_FINITE];
         info->first_bad_pivot = st[hyb::ST_FIRST_BAD] == INT_MAX ? -1 : st[hyb::ST_FIRST_BAD];
+        info->growth_fp64 = (uint64_t)st[hyb::ST_GROWTH_FP64];
+        info->growth_kept = (uint64_t)st[hyb::ST_GROWTH_KEPT];
     }
     return HYB_SUCCESS;
 }

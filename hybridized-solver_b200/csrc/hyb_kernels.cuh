@@ -67,7 +67,10 @@ enum
     ST_ZERO_PIVOTS = 0,
     ST_NON_FINITE = 1,
     ST_FIRST_BAD = 2, // atomicMin of the block row, INT32_MAX if none
-    ST_WORDS = 4
+    // (3: ST_TIMEOUT, below)
+    ST_GROWTH_FP64 = 4, // mixed form: pivots whose FP32 LU grew past the limit, refactored in FP64
+    ST_GROWTH_KEPT = 5, // mixed form: pivots past the limit of a size without the FP64 path (kept FP32)
+    ST_WORDS = 6
 };
 
 constexpr int kThreads = 256;
@@ -133,19 +136,94 @@ template <typename T> __device__ __forceinline__ bool finite_val(T v)
     return isfinite(v);
 }
 
+// Largest v over the CTA (every thread calls it; NaN operands are ignored).
+template <typename T> __device__ __forceinline__ T cta_max(T v)
+{
+    __shared__ T s_max[32];
+    for (int o = 16; o > 0; o >>= 1)
+        v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __syncthreads(); // s_max is free
+    if ((threadIdx.x & 31) == 0)
+        s_max[threadIdx.x >> 5] = v;
+    __syncthreads();
+    T r = s_max[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+        r = fmax(r, s_max[w]);
+    __syncthreads();
+    return r;
+}
+
+// Growth of an m x m pivot block's LU held at `a` (row stride lda): the largest |U| entry
+// (on or above the diagonal) over `amax`, the largest |entry| of the block before it was
+// factored. Every thread calls it.
+template <typename T> __device__ __forceinline__ T lu_growth(const T *a, int m, int lda, T amax)
+{
+    T umax = T(0);
+    for (int i = threadIdx.x; i < m * m; i += blockDim.x)
+    {
+        const int r = i / m, c = i - r * m;
+        if (c >= r)
+            umax = fmax(umax, fabs(a[r * lda + c]));
+    }
+    umax = cta_max(umax);
+    return umax / amax;
+}
+
 // ----------------------------------------------------------------------------------
-// Values -> slab: original blocks are copied (and converted) to their filled slots.
+// Values -> slab: original blocks are copied (and converted) to their filled slots; with
+// `bscale` (per block row), block (r, c) is scaled by bscale[r] * bscale[c] on the way.
 template <typename T>
-__global__ void k_scatter(DevSym S, const double *__restrict__ a, T *__restrict__ slab, int64_t nnz_a)
+__global__ void k_scatter(DevSym S, const double *__restrict__ a, T *__restrict__ slab, int64_t nnz_a,
+                          const double *__restrict__ bscale)
 {
     for (int64_t b = blockIdx.x; b < nnz_a; b += gridDim.x)
     {
         const int64_t src = S.a_val_off[b];
         const int64_t cnt = S.a_val_off[b + 1] - src;
         T *dst = slab + S.blk_off[S.a_to_f[b]];
+        double f = 1.0;
+        if (bscale)
+        {
+            int64_t lo = 0, hi = S.n; // block row of b
+            while (hi - lo > 1)
+            {
+                const int64_t mid = (lo + hi) >> 1;
+                if (S.a_row_ptr[mid] <= b)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            f = bscale[lo] * bscale[S.a_cols[b]];
+        }
         for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x)
-            dst[i] = (T)a[src + i];
+            dst[i] = (T)(bscale ? a[src + i] * f : a[src + i]);
     }
+}
+
+// Per-block diagonal scaling of the mixed form: bscale[k] = 1 / sqrt(max |A_kk|) (1 for an
+// all-zero diagonal block), and its expansion to every unknown of block row k.
+__global__ void __launch_bounds__(128)
+    k_block_scales(DevSym S, const double *__restrict__ a, double *__restrict__ bscale, double *__restrict__ dscale)
+{
+    __shared__ double s_f;
+    const int64_t k = blockIdx.x;
+    int64_t j = S.a_row_ptr[k];
+    while (S.a_cols[j] != (int32_t)k) // the diagonal block (every row holds it)
+        ++j;
+    const double *blk = a + S.a_val_off[j];
+    const int64_t cnt = S.a_val_off[j + 1] - S.a_val_off[j];
+    double m = 0;
+    for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x)
+        m = fmax(m, fabs(blk[i]));
+    m = cta_max(m);
+    if (threadIdx.x == 0)
+    {
+        s_f = m > 0 ? 1.0 / sqrt(m) : 1.0;
+        bscale[k] = s_f;
+    }
+    __syncthreads();
+    for (int64_t i = threadIdx.x; i < S.size[k]; i += blockDim.x)
+        dscale[S.dof_off[k] + i] = s_f;
 }
 
 // ----------------------------------------------------------------------------------
@@ -178,13 +256,31 @@ __device__ void lu_inplace(T *a, int m, int lda, int *status, int row_id)
     }
 }
 
+// Pivots of at most this many rows keep an FP64 copy of a high-growth pivot's LU (mixed
+// form) for the solves of their rows' upper blocks.
+constexpr int kGrowthSmallRows = 32;
+
+// LU of the level's diagonal blocks. Mixed form (T = float, growth_limit > 0): a pivot whose
+// FP32 LU grows past the limit is refactored from its original values in FP64 -- into
+// piv64 at g64_off[k] for pivots of at most kGrowthSmallRows rows, flagged in hg[k] for
+// k_trsm, stored back rounded to FP32 -- or, larger, only counted.
 template <typename T, bool kShared>
-__global__ void __launch_bounds__(kThreads) k_lu(DevSym S, T *__restrict__ slab, int64_t p0, int *status)
+__global__ void __launch_bounds__(kThreads)
+    k_lu(DevSym S, T *__restrict__ slab, int64_t p0, int *status, float growth_limit, int *__restrict__ hg,
+         double *__restrict__ piv64, const int64_t *__restrict__ g64_off)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int64_t k = S.piv[p0 + blockIdx.x];
     const int m = S.size[k];
     T *g = slab + S.blk_off[S.diag_pos[k]];
+    const bool check = std::is_same_v<T, float> && growth_limit > 0;
+    T amax = T(0);
+    if (check)
+    {
+        for (int i = threadIdx.x; i < m * m; i += blockDim.x)
+            amax = fmax(amax, fabs(g[i]));
+        amax = cta_max(amax);
+    }
     if constexpr (kShared)
     {
         T *a = reinterpret_cast<T *>(smem_raw);
@@ -192,12 +288,37 @@ __global__ void __launch_bounds__(kThreads) k_lu(DevSym S, T *__restrict__ slab,
             a[i] = g[i];
         __syncthreads();
         lu_inplace(a, m, m, status, (int)k);
+        if (check && lu_growth(a, m, m, amax) > (T)growth_limit)
+        {
+            if (m <= kGrowthSmallRows && g64_off[k] >= 0)
+            {
+                double *a64 = piv64 + g64_off[k];
+                for (int i = threadIdx.x; i < m * m; i += blockDim.x)
+                    a64[i] = (double)g[i]; // the original values: the slab is written below
+                __syncthreads();
+                lu_inplace(a64, m, m, (int *)nullptr, (int)k);
+                for (int i = threadIdx.x; i < m * m; i += blockDim.x)
+                    a[i] = (T)a64[i];
+                if (threadIdx.x == 0)
+                {
+                    hg[k] = 1;
+                    atomicAdd(status + ST_GROWTH_FP64, 1);
+                }
+                __syncthreads();
+            }
+            else if (threadIdx.x == 0)
+            {
+                atomicAdd(status + ST_GROWTH_KEPT, 1);
+            }
+        }
         for (int i = threadIdx.x; i < m * m; i += blockDim.x)
             g[i] = a[i];
     }
     else
     {
         lu_inplace(g, m, m, status, (int)k);
+        if (check && lu_growth(g, m, m, amax) > (T)growth_limit && threadIdx.x == 0)
+            atomicAdd(status + ST_GROWTH_KEPT, 1);
     }
 }
 
@@ -275,9 +396,13 @@ __device__ void lu_solve_strip_warp(const T *d, int ldd, T *b, int ldb, int m, i
     }
 }
 
-// grid.x: upper blocks of the level's pivots, grid.y: 64-column strips.
+// grid.x: upper blocks of the level's pivots, grid.y: 64-column strips. A pivot that k_lu
+// refactored in FP64 (hg[k], mixed form) has its strips solved in FP64 with that LU, the
+// strip staged in shared memory as doubles (the launch provides m x (w | 1) doubles).
 template <typename T, bool kShared>
-__global__ void __launch_bounds__(kThreads) k_trsm(DevSym S, T *__restrict__ slab, int64_t p0, int64_t p1)
+__global__ void __launch_bounds__(kThreads)
+    k_trsm(DevSym S, T *__restrict__ slab, int64_t p0, int64_t p1, const int *__restrict__ hg,
+           const double *__restrict__ piv64, const int64_t *__restrict__ g64_off)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int64_t u = S.trsm_pref[p0] + blockIdx.x;
@@ -292,6 +417,22 @@ __global__ void __launch_bounds__(kThreads) k_trsm(DevSym S, T *__restrict__ sla
     const int w = min(kTile, nc - c0);
     const T *gd = slab + S.blk_off[S.diag_pos[k]];
     T *gb = slab + S.blk_off[blk] + c0;
+    if constexpr (kShared && std::is_same_v<T, float>)
+    {
+        if (hg && hg[k])
+        {
+            const int ldb = w | 1;
+            double *b = reinterpret_cast<double *>(smem_raw);
+            for (int i = threadIdx.x; i < m * w; i += blockDim.x)
+                b[(i / w) * ldb + i % w] = (double)gb[(i / w) * nc + i % w];
+            __syncthreads();
+            lu_solve_strip_warp(piv64 + g64_off[k], m, b, ldb, m, w);
+            __syncthreads();
+            for (int i = threadIdx.x; i < m * w; i += blockDim.x)
+                gb[(i / w) * nc + i % w] = (T)b[(i / w) * ldb + i % w];
+            return;
+        }
+    }
     if constexpr (kShared)
     {
         // odd row strides: the rows a warp touches at once sit in different banks
@@ -496,15 +637,75 @@ template <typename T> constexpr int lu_trsm64_smem()
     return (64 * kLd65 + 2 * 64 * kLdT + 64 + 256) * (int)sizeof(T);
 }
 
+// The FP64 path of k_lu_trsm64<float> for a pivot whose FP32 LU grew past the limit (see
+// there). Shared memory, reinterpreted: the 64 x 65 FP64 block, its two pivot-row/column
+// buffers, and one 64 x 33 FP64 half strip -- 52 KB, inside the FP32 kernel's 54 KB.
+constexpr int kLd33 = 33;
+static_assert((64 * kLd65 + 256 + 64 * kLd33) * 8 <= lu_trsm64_smem<float>(), "FP64 redo fits the FP32 working set");
+
+__device__ __noinline__ void lu_trsm64_fp64(const DevSym &S, float *__restrict__ slab, float *gd, int64_t p,
+                                            int64_t k, int64_t j, int m, int *lu_tickets, int total, int *status)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *d = reinterpret_cast<double *>(smem_raw);
+    double *rowbuf = d + 64 * kLd65;
+    double *colbuf = rowbuf + 128;
+    double *sb = colbuf + 128;
+    __shared__ int s_last;
+    __syncthreads(); // every thread is done with the FP32 working set
+    for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
+    {
+        const int r = i >> 6, c = i & 63;
+        d[r * kLd65 + c] = (r < m && c < m) ? (double)gd[r * m + c] : double(r == c);
+    }
+    __syncthreads();
+    // second round of the pivot's tickets: the last CTA to re-read the block stores it
+    if (threadIdx.x == 0)
+        s_last = atomicAdd(lu_tickets + p, 1) == 2 * total - 1;
+    lu64_shared(d, rowbuf, colbuf, (int *)nullptr, (int)k);
+    const int64_t blk = S.diag_pos[k] + 1 + j;
+    const int cc = blk < S.row_ptr[k + 1] ? S.size[S.cols[blk]] : 0;
+    const int col0 = 64 * (int)blockIdx.y;
+    const int w = min(64, cc - col0);
+    for (int h0 = 0; h0 < w; h0 += 32) // block-uniform
+    {
+        const int wh = min(32, w - h0);
+        float *gb = slab + S.blk_off[blk] + col0 + h0;
+        for (int i = threadIdx.x; i < m * wh; i += blockDim.x)
+            sb[(i / wh) * kLd33 + i % wh] = (double)gb[(i / wh) * cc + i % wh];
+        __syncthreads();
+        lu_solve_strip_warp(d, kLd65, sb, kLd33, m, wh);
+        __syncthreads();
+        for (int i = threadIdx.x; i < m * wh; i += blockDim.x)
+            gb[(i / wh) * cc + i % wh] = (float)sb[(i / wh) * kLd33 + i % wh];
+        __syncthreads();
+    }
+    if (s_last)
+    {
+        for (int i = threadIdx.x; i < m * m; i += blockDim.x)
+            gd[i] = (float)d[(i / m) * kLd65 + i % m];
+        if (threadIdx.x == 0)
+            lu_tickets[p] = 0;
+    }
+    if (status != nullptr && threadIdx.x == 0)
+        atomicAdd(status + ST_GROWTH_FP64, 1);
+}
+
 // One CTA per upper block (grid.y: its 64-column strips) of the level's pivots of at most
 // 64 rows; every CTA factors its pivot's diagonal block in shared memory (the last of them
 // to read it writes it back) and then solves its strip. A pivot without upper blocks gets
 // one CTA for the LU alone: the grid is the level's work units with empty pivots counted
 // once (lu_pref).
+//
+// Mixed form (T = float, growth_limit > 0): every CTA of a pivot computes the same FP32 LU
+// and so the same growth max|U_d| / max|D|. Past the limit, no CTA writes the FP32 factors:
+// each re-reads the original block, factors it in FP64 in its own shared memory (the FP32
+// working set reinterpreted), solves its strip in FP64 in two 32-column halves, and takes
+// a second ticket of the pivot; the last to take it stores the FP64 LU rounded to FP32.
 template <typename T, bool kPad>
 __global__ void __launch_bounds__(kThreads, 1)
     k_lu_trsm64(DevSym S, T *__restrict__ slab, int64_t p0, int64_t p1, const int64_t *__restrict__ unit_pref,
-                int *__restrict__ lu_tickets, int *status)
+                int *__restrict__ lu_tickets, int *status, float growth_limit)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *d = reinterpret_cast<T *>(smem_raw);
@@ -521,22 +722,35 @@ __global__ void __launch_bounds__(kThreads, 1)
     const bool owner = j == 0 && blockIdx.y == 0; // reports zero and non-finite pivots
     T *gd = slab + S.blk_off[S.diag_pos[k]];
     __shared__ int s_writer;
+    const bool check = std::is_same_v<T, float> && growth_limit > 0;
+    T amax = T(0);
     // an m x m diagonal block (m <= 64) is factored as [D 0; 0 I]: the padding only meets
     // zeros, so D's factors are exactly those of D alone
     for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
     {
         const int r = i >> 6, c = i & 63;
-        d[r * kLd65 + c] = (!kPad || (r < m && c < m)) ? gd[r * m + c] : T(r == c);
+        const T v = (!kPad || (r < m && c < m)) ? gd[r * m + c] : T(r == c);
+        d[r * kLd65 + c] = v;
+        if (!kPad || (r < m && c < m))
+            amax = fmax(amax, fabs(v));
     }
     __syncthreads();
     // Every CTA of the pivot reads the unfactored block; the one that takes the pivot's last
     // ticket -- after all the others have read it -- writes the factors back.
+    const int total = (int)(unit_pref[p + 1] - unit_pref[p]) * (int)gridDim.y;
     if (threadIdx.x == 0)
-    {
-        const int total = (int)(unit_pref[p + 1] - unit_pref[p]) * (int)gridDim.y;
         s_writer = atomicAdd(lu_tickets + p, 1) == total - 1;
-    }
     lu64_shared(d, rowbuf, colbuf, owner ? status : nullptr, (int)k);
+    if (check)
+    {
+        amax = cta_max(amax);
+        if (lu_growth(d, m, kLd65, amax) > (T)growth_limit)
+        {
+            if constexpr (std::is_same_v<T, float>)
+                lu_trsm64_fp64(S, slab, gd, p, k, j, m, lu_tickets, total, owner ? status : nullptr);
+            return;
+        }
+    }
     if (s_writer)
     {
         for (int i = threadIdx.x; i < m * m; i += blockDim.x)

@@ -253,6 +253,17 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
+// dst[i][r] = (B)(src[i][r] * dscale[i]): the conversions around a substitution with
+// factors of the scaled matrix S A S (dscale: S's diagonal, one value per unknown).
+template <typename A, typename B>
+__global__ void k_convert_scaled(const A *__restrict__ src, B *__restrict__ dst, const double *__restrict__ dscale,
+                                 int64_t rows, int nrhs)
+{
+    const int64_t n = rows * nrhs;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = (B)((double)src[i] * dscale[i / nrhs]);
+}
+
 // y[i][r] -= coef[r] * x[i][r] (the coefficients stay on the device between launches).
 __global__ void k_sub_scaled(double *__restrict__ y, const double *__restrict__ x, const double *__restrict__ coef,
                              int64_t rows, int nrhs)

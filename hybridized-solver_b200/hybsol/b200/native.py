@@ -34,6 +34,8 @@ OPTION_WITHHOLD_ROW = 4
 OPTION_REFINEMENT = 5  # 0 auto (refinement, then FGMRES when it stalls), 1 refinement only, 2 FGMRES
 OPTION_FP64_REFINEMENT = 6
 OPTION_KRYLOV_RESTART = 7
+OPTION_GROWTH_LIMIT = 8
+OPTION_BLOCK_SCALING = 9
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _i64p = ctypes.POINTER(ctypes.c_int64)
@@ -49,6 +51,8 @@ class DecomposeInfo(ctypes.Structure):
         ("zero_pivots", ctypes.c_uint64),
         ("non_finite", ctypes.c_uint64),
         ("first_bad_pivot", ctypes.c_int64),
+        ("growth_fp64", ctypes.c_uint64),
+        ("growth_kept", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:

@@ -81,6 +81,10 @@ typedef struct
     uint64_t zero_pivots;      /* diagonal pivots that were exactly zero */
     uint64_t non_finite;       /* diagonal pivots that came out inf/nan */
     int64_t first_bad_pivot;   /* lowest block row with a bad pivot, -1 if none */
+    uint64_t growth_fp64;      /* mixed form: pivots whose FP32 LU grew past HYB_OPTION_GROWTH_LIMIT and were
+                                  refactored (LU and row solve) in FP64 */
+    uint64_t growth_kept;      /* mixed form: pivots past the limit whose size has no FP64 path (more than 64
+                                  rows, or too large for shared memory), kept in FP32 */
 } hyb_decompose_info;
 
 typedef struct
@@ -184,7 +188,19 @@ typedef enum
      * whose plain FP64 solve misses the tolerance; 0 (default): the drop-in plain solve. */
     HYB_OPTION_FP64_REFINEMENT = 6,
     /* FGMRES restart length (Krylov vectors kept, 1..200, default 30). */
-    HYB_OPTION_KRYLOV_RESTART = 7
+    HYB_OPTION_KRYLOV_RESTART = 7,
+    /* Mixed form: growth limit of a diagonal pivot block, max|U_d| / max|D| of its FP32 LU
+     * (default 1024; 0 turns the check off). A pivot above it is refactored in FP64 -- its
+     * LU and the solves of its row's upper blocks, stored back in FP32 -- so the elimination
+     * steps that amplify rounding most are the ones kept in FP64. Pivots of at most 32 rows
+     * and of 33-64 rows have this path; larger ones are counted in growth_kept. */
+    HYB_OPTION_GROWTH_LIMIT = 8,
+    /* Mixed form: 1 factors the block-diagonally scaled S A S, s_k = 1 / sqrt(max |A_kk|)
+     * for every unknown of block row k, so each diagonal block enters the FP32 / BF16-split
+     * factorization with entries of order one; the solves apply S on both sides and the
+     * refinement's residual stays that of the unscaled FP64 A. hyb_get_block then returns
+     * the scaled factors. 0 (default): unscaled. */
+    HYB_OPTION_BLOCK_SCALING = 9
 } hyb_option;
 
 /* Sets a schedule option of the handle (takes effect at the next decomposition). */

@@ -31,7 +31,10 @@ def _run(extra_env=None, *args):
 
 
 def test_reference_arm_line():
-    out = _run(None, "--impl", "reference", "--steps", "1", "--warmup", "0", "--mesh", "12", "--cpu-sample-mesh", "6")
+    # one reference thread: its multi-threaded decompose can hang on tiny systems (a data
+    # race in its scheduler; bench.py runs it in a child process with a time limit)
+    out = _run(None, "--impl", "reference", "--steps", "1", "--warmup", "0", "--mesh", "12", "--cpu-sample-mesh", "6",
+               "--ref-threads", "1")
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [ln for ln in out.stdout.splitlines() if ln.strip()]
     assert len(lines) == 1
@@ -58,7 +61,7 @@ def test_reference_arm_loads_no_repo_library():
     own factored pattern: neither libhybsol_b200.so nor the hybsol._mod extension loads."""
     code = (
         "import sys, runpy; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0', "
-        "'--mesh', '12', '--cpu-sample-mesh', '4']\n"
+        "'--mesh', '12', '--cpu-sample-mesh', '4', '--ref-threads', '1']\n"
         "try:\n    runpy.run_path('bench.py', run_name='__main__')\nexcept SystemExit:\n    pass\n"
         "maps = open('/proc/self/maps').read()\n"
         "print('LOADED', 'libhybsol_b200' in maps, 'hybsol/_mod' in maps)\n"
@@ -66,6 +69,19 @@ def test_reference_arm_loads_no_repo_library():
     out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     assert "LOADED False False" in out.stdout, out.stdout[-500:]
+
+
+def test_reference_leg_runs_in_a_child_process():
+    """The reference's decompose runs in a child process under a time limit (its
+    multi-threaded scheduler can hang); the parent gets its times, residual, solution and
+    the flops counted from its factored pattern."""
+    import numpy as np
+
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    times, res, x, flops = bench.reference_sample(4, 8, 2, 0, 1)
+    assert len(times) == 2 and res < 1e-12 and flops > 0 and np.isfinite(x).all()
 
 
 def test_reference_arm_other_ranks_are_silent():

@@ -152,3 +152,65 @@ def test_non_finite_solution_is_never_reported_converged(gpu, mode):
     assert not info["converged"]
     assert not (info["relative_residual"] <= 1e-12)
     assert not np.isfinite(x).all()
+
+
+def test_growth_check_leaves_well_conditioned_factors_alone(gpu):
+    """On the dominant set no pivot grows past the default limit: the check changes no bit."""
+    ns, pm, bn = _system(gpu, 8, 8, seed=5)
+    d1 = ns.decompose(gpu.MIXED)
+    assert d1["growth_fp64"] == 0 and d1["growth_kept"] == 0
+    x1, _ = ns.solve(bn)
+    ns.set_option(gpu.OPTION_GROWTH_LIMIT, 0)  # check off
+    ns.decompose(gpu.MIXED)
+    x0, _ = ns.solve(bn)
+    assert np.array_equal(x0, x1)
+
+
+@pytest.mark.parametrize(("n", "p", "reduced"), [(8, 8, True), (16, 4, True), (6, "rand", False)])
+def test_growth_fallback_refactors_in_fp64(gpu, n, p, reduced):
+    """A limit of 1 flags most pivots, so every path runs: the fused 64-row FP64 redo, the
+    FP64 LU and row solves of pivots of at most 32 rows, and pivots over 64 rows (orders
+    9 and 10) counted as kept in FP32. The mixed solve still reaches the tolerance."""
+    from hybsol.b200 import meshgen
+
+    pp = meshgen.random_orders(n, 2, 10, seed=8) if p == "rand" else p
+    alpha = meshgen.reduced_shift(n, p) if reduced else 1.0
+    ns, pm, bn = _system(gpu, n, pp, shift=alpha)
+    ns.set_option(gpu.OPTION_GROWTH_LIMIT, 1)
+    d = ns.decompose(gpu.MIXED)
+    assert d["growth_fp64"] > 0, d
+    if p == "rand":
+        assert d["growth_kept"] > 0, d  # pivots of 81 and 100 rows have no FP64 path
+    x, info = ns.solve(bn, max_iter=60)
+    assert info["converged"] and info["relative_residual"] <= 1e-12, info
+    xo, ro = _oracle_refined(pm, bn)
+    kappa = meshgen.exact_kappa1(pm)
+    assert rel_err(x, xo) <= max(1e-11, 10 * kappa * (info["relative_residual"] + ro))
+    # the same decomposition twice gives the same bits (the second-round tickets reset)
+    ns.decompose(gpu.MIXED)
+    x2, _ = ns.solve(bn, max_iter=60)
+    assert np.array_equal(x, x2)
+
+
+def test_block_scaling(gpu):
+    """Scaled factors are those of S A S: the unit-lower part of a diagonal block's LU is
+    unchanged and its upper part is scaled by s_k^2 = 1 / max|A_kk|; the scaled mixed solve
+    reaches the tolerance and agrees with the unscaled one."""
+    ns, pm, bn = _system(gpu, 8, 8, seed=2)
+    ns.decompose(gpu.MIXED)
+    x0, i0 = ns.solve(bn)
+    k = pm.n_blocks - 1
+    m = int(pm.sizes[k])
+    lu0 = ns.get_block(k, k, (m, m))
+    ns.set_option(gpu.OPTION_BLOCK_SCALING, 1)
+    ns.decompose(gpu.MIXED)
+    x1, i1 = ns.solve(bn)
+    assert i0["converged"] and i1["converged"]
+    assert rel_err(x1, x0) < 1e-11
+    lu1 = ns.get_block(k, k, (m, m))
+    j = int(np.searchsorted(pm.cols[pm.row_ptr[k] : pm.row_ptr[k + 1]], k))
+    akk = pm.vals[pm.val_ptr[pm.row_ptr[k] + j] : pm.val_ptr[pm.row_ptr[k] + j + 1]]
+    s2 = 1.0 / np.abs(akk).max()
+    up = np.triu(np.ones((m, m), dtype=bool))
+    assert np.allclose(lu1[up], s2 * lu0[up], rtol=1e-4, atol=0)
+    assert np.allclose(lu1[~up], lu0[~up], rtol=1e-4, atol=1e-6)
