@@ -876,6 +876,37 @@ int check_handle(const hyb_system *h)
     return h ? HYB_SUCCESS : HYB_INVALID_ARGUMENT;
 }
 
+// Device workspace of the dense block entry points, one per device: grown to the largest
+// request and kept until the process exits, so repeated calls allocate nothing. Callers hold
+// g_ws_mutex while they use it.
+constexpr int kWsDevices = 64;
+std::mutex g_ws_mutex;
+char *g_ws[kWsDevices] = {};
+size_t g_ws_bytes[kWsDevices] = {};
+
+int workspace(size_t bytes, char **out)
+{
+    int dev = 0;
+    HYB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kWsDevices)
+        return HYB_INVALID_ARGUMENT;
+    if (g_ws_bytes[dev] < bytes)
+    {
+        if (g_ws[dev])
+        {
+            HYB_CUDA(cudaDeviceSynchronize()); // earlier users of the old buffer are done
+            cudaFree(g_ws[dev]);
+            g_ws[dev] = nullptr;
+            g_ws_bytes[dev] = 0;
+        }
+        const size_t grow = std::max<size_t>(bytes, 1 << 20);
+        HYB_CUDA(cudaMalloc(&g_ws[dev], grow));
+        g_ws_bytes[dev] = grow;
+    }
+    *out = g_ws[dev];
+    return HYB_SUCCESS;
+}
+
 // A device allocation released when it goes out of scope, so early returns do not leak.
 struct DevBuf
 {
@@ -2302,21 +2333,24 @@ HYB_API int hyb_block_lu(uint64_t m, double *a, int memory)
     if (!hyb_device_available())
         return HYB_NO_DEVICE;
     const size_t bytes = m * m * sizeof(double);
-    DevBuf dbuf, st;
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    char *ws = nullptr;
+    int rc = workspace(bytes + 256, &ws);
+    if (rc != HYB_SUCCESS)
+        return rc;
+    int *st = reinterpret_cast<int *>(ws);
     double *d = a;
     if (memory != HYB_MEMORY_DEVICE)
     {
-        HYB_CUDA(cudaMalloc(&dbuf.p, bytes));
-        d = static_cast<double *>(dbuf.p);
+        d = reinterpret_cast<double *>(ws + 256);
         HYB_CUDA(cudaMemcpy(d, a, bytes, cudaMemcpyHostToDevice));
     }
-    HYB_CUDA(cudaMalloc(&st.p, hyb::ST_WORDS * sizeof(int)));
-    k_status_init<<<1, 32>>>(static_cast<int *>(st.p));
+    k_status_init<<<1, 32>>>(st);
     HYB_CUDA(allow_smem(hyb::k_dense_lu, smem_optin()));
     if ((int)bytes <= smem_optin())
-        hyb::k_dense_lu<<<1, hyb::kThreads, bytes>>>(d, (int)m, static_cast<int *>(st.p));
+        hyb::k_dense_lu<<<1, hyb::kThreads, bytes>>>(d, (int)m, st);
     else
-        hyb::k_dense_lu_global<<<1, hyb::kThreads>>>(d, (int)m, static_cast<int *>(st.p));
+        hyb::k_dense_lu_global<<<1, hyb::kThreads>>>(d, (int)m, st);
     HYB_CUDA(cudaGetLastError());
     if (memory != HYB_MEMORY_DEVICE)
         HYB_CUDA(cudaMemcpy(a, d, bytes, cudaMemcpyDeviceToHost));
@@ -2329,30 +2363,60 @@ HYB_API int hyb_block_lu_solve(uint64_t m, const double *lu, uint64_t ncols, con
 {
     if (!lu || !b || !out || m == 0 || ncols == 0 || m > 4096)
         return HYB_INVALID_ARGUMENT;
+    if (memory == HYB_MEMORY_DEVICE && b != out)
+        HYB_CUDA(cudaMemcpy(out, b, m * ncols * sizeof(double), cudaMemcpyDeviceToDevice));
+    if (memory != HYB_MEMORY_DEVICE && b != out)
+        std::memcpy(out, b, m * ncols * sizeof(double));
+    double *const bs[1] = {out};
+    return hyb_block_lu_solve_batched(m, lu, 1, &ncols, bs, memory);
+}
+
+HYB_API int hyb_block_lu_solve_batched(uint64_t m, const double *lu, uint64_t count, const uint64_t *n,
+                                       double *const *b, int memory)
+{
+    if (!lu || m == 0 || m > 4096 || (count && (!n || !b)))
+        return HYB_INVALID_ARGUMENT;
+    for (uint64_t i = 0; i < count; ++i)
+        if (!b[i] || n[i] == 0 || n[i] > (1u << 20))
+            return HYB_INVALID_ARGUMENT;
     if (!hyb_device_available())
         return HYB_NO_DEVICE;
-    const size_t lu_bytes = m * m * sizeof(double), b_bytes = m * ncols * sizeof(double);
-    DevBuf lu_buf, b_buf;
+    if (count == 0)
+        return HYB_SUCCESS;
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    const size_t lu_bytes = m * m * sizeof(double);
+    std::vector<size_t> off(count + 1, 0);
+    for (uint64_t i = 0; i < count; ++i)
+        off[i + 1] = off[i] + (m * n[i] * sizeof(double) + 255) / 256 * 256;
     const double *dlu = lu;
-    double *db = out;
+    char *ws = nullptr;
     if (memory != HYB_MEMORY_DEVICE)
     {
-        HYB_CUDA(cudaMalloc(&lu_buf.p, lu_bytes));
-        HYB_CUDA(cudaMalloc(&b_buf.p, b_bytes));
-        HYB_CUDA(cudaMemcpy(lu_buf.p, lu, lu_bytes, cudaMemcpyHostToDevice));
-        HYB_CUDA(cudaMemcpy(b_buf.p, b, b_bytes, cudaMemcpyHostToDevice));
-        dlu = static_cast<const double *>(lu_buf.p);
-        db = static_cast<double *>(b_buf.p);
+        int rc = workspace((lu_bytes + 255) / 256 * 256 + off[count], &ws);
+        if (rc != HYB_SUCCESS)
+            return rc;
+        // one staging buffer on the host, one copy in and one out
+        std::vector<char> host((lu_bytes + 255) / 256 * 256 + off[count]);
+        std::memcpy(host.data(), lu, lu_bytes);
+        char *hb = host.data() + (lu_bytes + 255) / 256 * 256;
+        for (uint64_t i = 0; i < count; ++i)
+            std::memcpy(hb + off[i], b[i], m * n[i] * sizeof(double));
+        HYB_CUDA(cudaMemcpy(ws, host.data(), host.size(), cudaMemcpyHostToDevice));
+        dlu = reinterpret_cast<const double *>(ws);
+        char *db = ws + (lu_bytes + 255) / 256 * 256;
+        for (uint64_t i = 0; i < count; ++i)
+            hyb::k_dense_lu_solve<<<(unsigned)((n[i] + hyb::kTile - 1) / hyb::kTile), hyb::kThreads>>>(
+                dlu, (int)m, reinterpret_cast<double *>(db + off[i]), (int)n[i]);
+        HYB_CUDA(cudaGetLastError());
+        HYB_CUDA(cudaMemcpy(hb, db, off[count], cudaMemcpyDeviceToHost));
+        for (uint64_t i = 0; i < count; ++i)
+            std::memcpy(b[i], hb + off[i], m * n[i] * sizeof(double));
+        return HYB_SUCCESS;
     }
-    else if (b != out)
-    {
-        HYB_CUDA(cudaMemcpy(db, b, b_bytes, cudaMemcpyDeviceToDevice));
-    }
-    hyb::k_dense_lu_solve<<<(unsigned)((ncols + hyb::kTile - 1) / hyb::kTile), hyb::kThreads>>>(dlu, (int)m, db,
-                                                                                               (int)ncols);
+    for (uint64_t i = 0; i < count; ++i)
+        hyb::k_dense_lu_solve<<<(unsigned)((n[i] + hyb::kTile - 1) / hyb::kTile), hyb::kThreads>>>(dlu, (int)m, b[i],
+                                                                                                 (int)n[i]);
     HYB_CUDA(cudaGetLastError());
-    if (memory != HYB_MEMORY_DEVICE)
-        HYB_CUDA(cudaMemcpy(out, db, b_bytes, cudaMemcpyDeviceToHost));
     HYB_CUDA(cudaDeviceSynchronize());
     return HYB_SUCCESS;
 }
@@ -2360,33 +2424,130 @@ HYB_API int hyb_block_lu_solve(uint64_t m, const double *lu, uint64_t ncols, con
 HYB_API int hyb_block_gemm(uint64_t m, uint64_t k, uint64_t n, const double *a, const double *b, double *c,
                            int subtract, int memory)
 {
-    if (!a || !b || !c || m == 0 || n == 0 || m > (1u << 20) || n > (1u << 20) || k > (1u << 20))
+    if (!b || !c)
         return HYB_INVALID_ARGUMENT;
+    const double *const bs[1] = {b};
+    double *const cs[1] = {c};
+    return hyb_block_gemm_batched(1, m, k, &n, a, bs, cs, subtract, memory);
+}
+
+HYB_API int hyb_block_gemm_batched(uint64_t count, uint64_t m, uint64_t k, const uint64_t *n, const double *a,
+                                   const double *const *b, double *const *c, int subtract, int memory)
+{
+    if (!a || m == 0 || m > (1u << 20) || k > (1u << 20) || (count && (!n || !b || !c)))
+        return HYB_INVALID_ARGUMENT;
+    for (uint64_t i = 0; i < count; ++i)
+        if (!b[i] || !c[i] || n[i] == 0 || n[i] > (1u << 20))
+            return HYB_INVALID_ARGUMENT;
     if (!hyb_device_available())
         return HYB_NO_DEVICE;
-    const size_t ab = m * k * sizeof(double), bb = k * n * sizeof(double), cb = m * n * sizeof(double);
-    DevBuf a_buf, b_buf, c_buf;
-    const double *da = a, *db = b;
-    double *dc = c;
+    if (count == 0)
+        return HYB_SUCCESS;
+    auto launch = [&](const double *da, const double *db, double *dc, uint64_t ni) {
+        const dim3 grid((unsigned)((ni + hyb::kTile - 1) / hyb::kTile), (unsigned)((m + hyb::kTile - 1) / hyb::kTile));
+        hyb::k_dense_gemm<<<grid, hyb::kThreads>>>(da, db, dc, (int)m, (int)k, (int)ni, subtract);
+    };
+    if (memory == HYB_MEMORY_DEVICE)
+    {
+        for (uint64_t i = 0; i < count; ++i)
+            launch(a, b[i], c[i], n[i]);
+        HYB_CUDA(cudaGetLastError());
+        HYB_CUDA(cudaDeviceSynchronize());
+        return HYB_SUCCESS;
+    }
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    auto pad = [](size_t x) { return (x + 255) / 256 * 256; };
+    // workspace: a, then every b, then every c (each 256-byte aligned, 8 bytes of slack for
+    // the tile loader's vector reads past a row's end)
+    const size_t a_bytes = pad(m * k * sizeof(double) + 8);
+    std::vector<size_t> boff(count + 1, 0), coff(count + 1, 0);
+    for (uint64_t i = 0; i < count; ++i)
+    {
+        boff[i + 1] = boff[i] + pad(k * n[i] * sizeof(double) + 8);
+        coff[i + 1] = coff[i] + pad(m * n[i] * sizeof(double));
+    }
+    const size_t in_bytes = a_bytes + boff[count] + (subtract ? coff[count] : 0);
+    char *ws = nullptr;
+    int rc = workspace(a_bytes + boff[count] + coff[count], &ws);
+    if (rc != HYB_SUCCESS)
+        return rc;
+    std::vector<char> host(a_bytes + boff[count] + coff[count], 0);
+    std::memcpy(host.data(), a, m * k * sizeof(double));
+    for (uint64_t i = 0; i < count; ++i)
+    {
+        std::memcpy(host.data() + a_bytes + boff[i], b[i], k * n[i] * sizeof(double));
+        if (subtract)
+            std::memcpy(host.data() + a_bytes + boff[count] + coff[i], c[i], m * n[i] * sizeof(double));
+    }
+    HYB_CUDA(cudaMemcpy(ws, host.data(), in_bytes, cudaMemcpyHostToDevice));
+    char *dc = ws + a_bytes + boff[count];
+    for (uint64_t i = 0; i < count; ++i)
+        launch(reinterpret_cast<const double *>(ws), reinterpret_cast<const double *>(ws + a_bytes + boff[i]),
+               reinterpret_cast<double *>(dc + coff[i]), n[i]);
+    HYB_CUDA(cudaGetLastError());
+    HYB_CUDA(cudaMemcpy(host.data(), dc, coff[count], cudaMemcpyDeviceToHost));
+    for (uint64_t i = 0; i < count; ++i)
+        std::memcpy(c[i], host.data() + coff[i], m * n[i] * sizeof(double));
+    return HYB_SUCCESS;
+}
+
+HYB_API int hyb_system_add_blocks(hyb_system *h, uint64_t count, const uint64_t *rows, const uint64_t *cols,
+                                  const double *values, int memory)
+{
+    if (check_handle(h) || (count && (!rows || !cols || !values)))
+        return HYB_INVALID_ARGUMENT;
+    if (count == 0)
+        return HYB_SUCCESS;
+    const Symbolic &S = h->S;
+    // every input block's original-pattern index, checked before anything is added
+    std::vector<int64_t> tgt_of(count), in_off(count + 1, 0);
+    for (uint64_t i = 0; i < count; ++i)
+    {
+        if (rows[i] >= (uint64_t)S.n || cols[i] >= (uint64_t)S.n)
+            return HYB_INVALID_ARGUMENT;
+        const int32_t *b = S.a_cols.data() + S.a_row_ptr[rows[i]];
+        const int32_t *e = S.a_cols.data() + S.a_row_ptr[rows[i] + 1];
+        const int32_t *q = std::lower_bound(b, e, (int32_t)cols[i]);
+        if (q == e || *q != (int32_t)cols[i])
+            return HYB_BLOCK_NOT_IN_SYSTEM;
+        tgt_of[i] = q - S.a_cols.data();
+        in_off[i + 1] = in_off[i] + (int64_t)S.size[rows[i]] * S.size[cols[i]];
+    }
+    // input blocks grouped by target, each group in input order
+    std::vector<int64_t> order(count);
+    for (uint64_t i = 0; i < count; ++i)
+        order[i] = (int64_t)i;
+    std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) { return tgt_of[x] < tgt_of[y]; });
+    std::vector<int64_t> tgt, grp{0};
+    for (uint64_t q = 0; q < count; ++q)
+        if (q + 1 == count || tgt_of[order[q + 1]] != tgt_of[order[q]])
+        {
+            tgt.push_back(tgt_of[order[q]]);
+            grp.push_back((int64_t)q + 1);
+        }
+    const size_t idx_bytes = (in_off.size() + order.size() + tgt.size() + grp.size()) * sizeof(int64_t);
+    const size_t val_bytes = memory == HYB_MEMORY_DEVICE ? 0 : (size_t)in_off[count] * sizeof(double);
+    DevBuf buf;
+    HYB_CUDA(cudaMalloc(&buf.p, idx_bytes + val_bytes));
+    int64_t *d_in = static_cast<int64_t *>(buf.p), *d_order = d_in + in_off.size(), *d_tgt = d_order + order.size(),
+            *d_grp = d_tgt + tgt.size();
+    std::vector<int64_t> packed;
+    packed.reserve(idx_bytes / sizeof(int64_t));
+    for (const auto *v : {&in_off, &order, &tgt, &grp})
+        packed.insert(packed.end(), v->begin(), v->end());
+    HYB_CUDA(cudaMemcpyAsync(d_in, packed.data(), idx_bytes, cudaMemcpyHostToDevice, h->stream));
+    const double *vin = values;
     if (memory != HYB_MEMORY_DEVICE)
     {
-        HYB_CUDA(cudaMalloc(&a_buf.p, ab + 8));
-        HYB_CUDA(cudaMalloc(&b_buf.p, bb + 8));
-        HYB_CUDA(cudaMalloc(&c_buf.p, cb));
-        HYB_CUDA(cudaMemcpy(a_buf.p, a, ab, cudaMemcpyHostToDevice));
-        HYB_CUDA(cudaMemcpy(b_buf.p, b, bb, cudaMemcpyHostToDevice));
-        if (subtract)
-            HYB_CUDA(cudaMemcpy(c_buf.p, c, cb, cudaMemcpyHostToDevice));
-        da = static_cast<const double *>(a_buf.p);
-        db = static_cast<const double *>(b_buf.p);
-        dc = static_cast<double *>(c_buf.p);
+        double *dv = reinterpret_cast<double *>(reinterpret_cast<char *>(buf.p) + idx_bytes);
+        HYB_CUDA(cudaMemcpyAsync(dv, values, val_bytes, cudaMemcpyHostToDevice, h->stream));
+        vin = dv;
     }
-    const dim3 grid((unsigned)((n + hyb::kTile - 1) / hyb::kTile), (unsigned)((m + hyb::kTile - 1) / hyb::kTile));
-    hyb::k_dense_gemm<<<grid, hyb::kThreads>>>(da, db, dc, (int)m, (int)k, (int)n, subtract);
+    hyb::k_add_blocks<<<(unsigned)tgt.size(), hyb::kThreads, 0, h->stream>>>(h->ds, h->d_a, vin, d_in, d_order, d_tgt,
+                                                                             d_grp);
     HYB_CUDA(cudaGetLastError());
-    if (memory != HYB_MEMORY_DEVICE)
-        HYB_CUDA(cudaMemcpy(c, dc, cb, cudaMemcpyDeviceToHost));
-    HYB_CUDA(cudaDeviceSynchronize());
+    HYB_CUDA(cudaStreamSynchronize(h->stream)); // the staging buffer is freed on return
+    h->factored = -1;
     return HYB_SUCCESS;
 }
 

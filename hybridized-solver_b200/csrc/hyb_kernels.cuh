@@ -2289,6 +2289,24 @@ __global__ void __launch_bounds__(kThreads) k_dense_gemm(const double *a, const 
     tile_store(acc, c + (int64_t)r0 * n + c0, n, m - r0, n - c0);
 }
 
+// Bulk assembly: one CTA per target block of the original pattern; the group's input
+// blocks (positions order[grp[g]] .. order[grp[g+1]-1], in input order) are added to it one
+// after the other, as repeated add_block calls would.
+__global__ void __launch_bounds__(kThreads)
+    k_add_blocks(DevSym S, double *__restrict__ a, const double *__restrict__ vin, const int64_t *__restrict__ in_off,
+                 const int64_t *__restrict__ order, const int64_t *__restrict__ tgt, const int64_t *__restrict__ grp)
+{
+    const int64_t g = blockIdx.x, j = tgt[g];
+    const int64_t base = S.a_val_off[j], cnt = S.a_val_off[j + 1] - base;
+    for (int64_t e = threadIdx.x; e < cnt; e += blockDim.x)
+    {
+        double acc = a[base + e];
+        for (int64_t q = grp[g]; q < grp[g + 1]; ++q)
+            acc += vin[in_off[order[q]] + e];
+        a[base + e] = acc;
+    }
+}
+
 // One strip of 64 columns per CTA.
 __global__ void k_dense_lu_solve(const double *lu, int m, double *b, int ncols)
 {

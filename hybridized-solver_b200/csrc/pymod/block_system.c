@@ -946,6 +946,15 @@ static PyObject *bs_eliminate_row(PyObject *self, PyTypeObject *cls, PyObject *c
     }
     uint64_t a = rt->count, b = rs->count, k = rt->count + extra;
     int st = HYB_SUCCESS;
+    /* Merge the columns first (existing target blocks or zeroed fill blocks), collecting the
+     * products; then one batched device call applies them all. */
+    const uint64_t nprod = rs->count - ps;
+    const double **bsrc = (const double **)PyMem_RawMalloc((nprod ? nprod : 1) * sizeof(double *));
+    double **cdst = (double **)PyMem_RawMalloc((nprod ? nprod : 1) * sizeof(double *));
+    uint64_t *ncol = (uint64_t *)PyMem_RawMalloc((nprod ? nprod : 1) * sizeof(uint64_t));
+    uint64_t np = 0;
+    if (!bsrc || !cdst || !ncol)
+        st = HYB_FAILED_ALLOC;
     while (b > ps && st == HYB_SUCCESS)
     {
         const entry_t *es = rs->e + (b - 1);
@@ -958,9 +967,6 @@ static PyObject *bs_eliminate_row(PyObject *self, PyTypeObject *cls, PyObject *c
         if (a > pt && rt->e[a - 1].col == es->col)
         {
             entry_t e = rt->e[--a];
-            Py_BEGIN_ALLOW_THREADS;
-            st = hyb_block_gemm(mt, ms, nc, mult, es->vals, e.vals, 1, HYB_MEMORY_HOST);
-            Py_END_ALLOW_THREADS;
             rt->e[--k] = e;
         }
         else
@@ -971,14 +977,24 @@ static PyObject *bs_eliminate_row(PyObject *self, PyTypeObject *cls, PyObject *c
                 st = HYB_FAILED_ALLOC;
                 break;
             }
-            Py_BEGIN_ALLOW_THREADS;
-            st = hyb_block_gemm(mt, ms, nc, mult, es->vals, fill, 1, HYB_MEMORY_HOST);
-            Py_END_ALLOW_THREADS;
             rt->e[--k].col = es->col;
             rt->e[k].vals = fill;
         }
+        bsrc[np] = es->vals;
+        cdst[np] = rt->e[k].vals;
+        ncol[np] = nc;
+        ++np;
         --b;
     }
+    if (st == HYB_SUCCESS && np > 0)
+    {
+        Py_BEGIN_ALLOW_THREADS;
+        st = hyb_block_gemm_batched(np, mt, ms, ncol, mult, bsrc, cdst, 1, HYB_MEMORY_HOST);
+        Py_END_ALLOW_THREADS;
+    }
+    PyMem_RawFree((void *)bsrc);
+    PyMem_RawFree(cdst);
+    PyMem_RawFree(ncol);
     Py_DECREF(arr);
     if (st != HYB_SUCCESS)
     {
@@ -1124,15 +1140,30 @@ static PyObject *bs_row_apply_decomposition(PyObject *self, PyTypeObject *cls, P
         PyErr_Format(PyExc_ValueError, "Row %zd has no diagonal entry.", r);
         return NULL;
     }
-    /* Blocks right of the diagonal become D^{-1} B (src/block_system.c:1083-1130). */
+    /* Blocks right of the diagonal become D^{-1} B (src/block_system.c:1083-1130), all in one
+     * batched device call. */
     const uint64_t m = bsize(s, r);
     int st = HYB_SUCCESS;
-    for (uint64_t j = p + 1; j < row->count && st == HYB_SUCCESS; ++j)
+    const uint64_t nb = row->count - p - 1;
+    if (nb > 0)
     {
-        const uint64_t nc = bsize(s, row->e[j].col);
-        Py_BEGIN_ALLOW_THREADS;
-        st = hyb_block_lu_solve(m, row->e[p].vals, nc, row->e[j].vals, row->e[j].vals, HYB_MEMORY_HOST);
-        Py_END_ALLOW_THREADS;
+        double **bs = (double **)PyMem_RawMalloc(nb * sizeof(double *));
+        uint64_t *nc = (uint64_t *)PyMem_RawMalloc(nb * sizeof(uint64_t));
+        if (!bs || !nc)
+            st = HYB_FAILED_ALLOC;
+        for (uint64_t j = 0; st == HYB_SUCCESS && j < nb; ++j)
+        {
+            bs[j] = row->e[p + 1 + j].vals;
+            nc[j] = bsize(s, row->e[p + 1 + j].col);
+        }
+        if (st == HYB_SUCCESS)
+        {
+            Py_BEGIN_ALLOW_THREADS;
+            st = hyb_block_lu_solve_batched(m, row->e[p].vals, nb, nc, bs, HYB_MEMORY_HOST);
+            Py_END_ALLOW_THREADS;
+        }
+        PyMem_RawFree(bs);
+        PyMem_RawFree(nc);
     }
     if (st)
         return raise_status(st, "row_apply_decomposition"), NULL;

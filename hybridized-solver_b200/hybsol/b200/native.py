@@ -168,6 +168,28 @@ EXPORTS = {
     ),
     "hyb_condition_estimate": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Condition)]),
     "hyb_system_set_segments": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _u64p]),
+    "hyb_system_add_blocks": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_uint64, _u64p, _u64p, ctypes.c_void_p, ctypes.c_int],
+    ),
+    "hyb_block_gemm_batched": (
+        ctypes.c_int,
+        [
+            ctypes.c_uint64,
+            ctypes.c_uint64,
+            ctypes.c_uint64,
+            _u64p,
+            ctypes.c_void_p,
+            ctypes.POINTER(ctypes.c_void_p),
+            ctypes.POINTER(ctypes.c_void_p),
+            ctypes.c_int,
+            ctypes.c_int,
+        ],
+    ),
+    "hyb_block_lu_solve_batched": (
+        ctypes.c_int,
+        [ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64, _u64p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int],
+    ),
     "hyb_segment_results": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), _f64p]),
     "hyb_row_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _u64p]),
     "hyb_row_cols": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _u64p]),
@@ -385,6 +407,22 @@ class NativeSystem:
         c = Condition()
         _check(lib().hyb_condition_estimate(self._h, ctypes.byref(c)), "hyb_condition_estimate")
         return c.as_dict()
+
+    def add_blocks(self, rows, cols, values, device: bool = False):
+        """Bulk assembly on the device: block i at (rows[i], cols[i]) gets its row-major
+        values from ``values`` (blocks concatenated in input order) added; repeats sum in
+        input order. ``values`` is a host array, or a device tensor with ``device=True``."""
+        r = np.ascontiguousarray(rows, dtype=np.uint64)
+        c = np.ascontiguousarray(cols, dtype=np.uint64)
+        if not device:
+            values = np.ascontiguousarray(values, dtype=np.float64)
+        st = lib().hyb_system_add_blocks(
+            self._h, len(r), r.ctypes.data_as(_u64p), c.ctypes.data_as(_u64p), _ptr(values),
+            MEMORY_DEVICE if device else MEMORY_HOST,
+        )
+        if st == 1:
+            raise KeyError("a block is not in the system's pattern")
+        _check(st, "hyb_system_add_blocks")
 
     def set_segments(self, offsets):
         """Independent systems stacked in this handle: segment s holds the unknowns

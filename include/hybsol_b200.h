@@ -339,6 +339,30 @@ HYB_API int hyb_block_lu_solve(uint64_t m, const double *lu, uint64_t ncols, con
 HYB_API int hyb_block_gemm(uint64_t m, uint64_t k, uint64_t n, const double *a, const double *b, double *c,
                            int subtract, int memory);
 
+/* The products of one row elimination (block_system_eliminate_row, src/blocks.c:557-727)
+ * in one call: c[i] = a * b[i] or c[i] -= a * b[i] for i < count, a m x k, b[i] k x n[i],
+ * c[i] m x n[i], all row-major; every c[i] distinct from a and the b's. With host memory
+ * the operands travel in one copy each way. */
+HYB_API int hyb_block_gemm_batched(uint64_t count, uint64_t m, uint64_t k, const uint64_t *n, const double *a,
+                                   const double *const *b, double *const *c, int subtract, int memory);
+/* The solves of one row's upper blocks with its factored diagonal block
+ * (block_system_apply_diagonal_inverse, src/blocks.c:516-539): b[i] <- LU^{-1} b[i] in place,
+ * b[i] m x n[i]. */
+HYB_API int hyb_block_lu_solve_batched(uint64_t m, const double *lu, uint64_t count, const uint64_t *n,
+                                       double *const *b, int memory);
+/* The hyb_block_* calls above stage host operands in a device workspace of the current
+ * device that is grown to the largest request and kept until the process exits, so
+ * repeated calls allocate nothing; calls from several host threads take turns on it. */
+
+/* Bulk assembly on the device: adds `count` blocks to the handle's values, block i at
+ * (rows[i], cols[i]) with its row-major values next in `values` (blocks concatenated in
+ * input order; `values` host or device memory). Blocks repeated in the input are summed in
+ * input order, as repeated add_block calls (src/blocks.c:36-45) would. Every block must be
+ * in the handle's pattern (HYB_BLOCK_NOT_IN_SYSTEM otherwise, and nothing is added). Clears
+ * any decomposition, as hyb_system_set_values does. */
+HYB_API int hyb_system_add_blocks(hyb_system *sys, uint64_t count, const uint64_t *rows, const uint64_t *cols,
+                                  const double *values, int memory);
+
 #ifdef __cplusplus
 }
 #endif
