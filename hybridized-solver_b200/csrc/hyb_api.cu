@@ -142,7 +142,7 @@ struct hyb_system
     bool fp64_refine = false;             // HYB_OPTION_FP64_REFINEMENT
     int krylov_restart = 30;              // HYB_OPTION_KRYLOV_RESTART
     float growth_limit = 1024.0f;         // HYB_OPTION_GROWTH_LIMIT (mixed form)
-    bool block_scaling = false;           // HYB_OPTION_BLOCK_SCALING (mixed form)
+    bool block_scaling = true;            // HYB_OPTION_BLOCK_SCALING (mixed form)
     bool factors_scaled = false;          // the current mixed factors are those of S A S
     double *d_bscale = nullptr;           // s_k per block row
     double *d_dscale = nullptr;           // s_k per unknown

@@ -195,11 +195,11 @@ typedef enum
      * steps that amplify rounding most are the ones kept in FP64. Pivots of at most 32 rows
      * and of 33-64 rows have this path; larger ones are counted in growth_kept. */
     HYB_OPTION_GROWTH_LIMIT = 8,
-    /* Mixed form: 1 factors the block-diagonally scaled S A S, s_k = 1 / sqrt(max |A_kk|)
-     * for every unknown of block row k, so each diagonal block enters the FP32 / BF16-split
-     * factorization with entries of order one; the solves apply S on both sides and the
-     * refinement's residual stays that of the unscaled FP64 A. hyb_get_block then returns
-     * the scaled factors. 0 (default): unscaled. */
+    /* Mixed form: 1 (default) factors the block-diagonally scaled S A S, s_k = 1 /
+     * sqrt(max |A_kk|) for every unknown of block row k, so each diagonal block enters the
+     * FP32 / BF16-split factorization with entries of order one; the solves apply S on both
+     * sides and the refinement's residual stays that of the unscaled FP64 A. hyb_get_block
+     * then returns the scaled factors. 0: the factors of A itself. */
     HYB_OPTION_BLOCK_SCALING = 9
 } hyb_option;
 

@@ -271,6 +271,7 @@ def test_tensor_core_mixed_matches_cuda_core_mixed(gpu, n):
     x64, _ = ns.solve(bn)
     f64 = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
     ns.set_values(pm.vals)
+    ns.set_option(gpu.OPTION_BLOCK_SCALING, 0)  # the factors of A itself, to compare with FP64's
     ns.decompose(gpu.MIXED)
     ftc = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
     xtc, itc = ns.solve(bn)

@@ -197,6 +197,7 @@ def test_block_scaling(gpu):
     unchanged and its upper part is scaled by s_k^2 = 1 / max|A_kk|; the scaled mixed solve
     reaches the tolerance and agrees with the unscaled one."""
     ns, pm, bn = _system(gpu, 8, 8, seed=2)
+    ns.set_option(gpu.OPTION_BLOCK_SCALING, 0)
     ns.decompose(gpu.MIXED)
     x0, i0 = ns.solve(bn)
     k = pm.n_blocks - 1
