@@ -219,6 +219,8 @@ def test_every_batched_system_converges_on_its_own_residual(gpu):
     per = info["systems"]
     assert all(s["iterations"] is not None for s in per)
     assert per[2]["iterations"] > max(per[0]["iterations"], per[1]["iterations"])
+    # the device's residuals against a host recomputation: forming b - A x rounds at about
+    # u ||A|| ||x|| / ||b||, a few 1e-15 here, so they agree to that
     for s, r in zip(per, res):
-        assert s["relative_residual"] == pytest.approx(r, rel=1e-3, abs=1e-15)
+        assert s["relative_residual"] == pytest.approx(r, rel=1e-3, abs=2e-14)
     bs.close()
