@@ -145,6 +145,27 @@ def device_bytes(system, precision: int = native.FP64, strategy: str = "first") 
     return slab + 8 * len(system.vals) + 64 * int(system.dof) + inv
 
 
+def pattern_bytes(sizes, row_ptr, cols, precision: int = native.FP64, strategy: str = "first") -> int:
+    """``device_bytes`` from the block pattern alone (no values needed)."""
+    sizes = np.asarray(sizes, dtype=np.int64)
+    row_ptr = np.asarray(row_ptr, dtype=np.int64)
+    cols = np.asarray(cols, dtype=np.int64)
+    order = native.compute_ordering(row_ptr, cols, strategy).astype(np.int64)
+    n = len(sizes)
+    inv = np.empty(n, dtype=np.int64)
+    inv[order] = np.arange(n)
+    new_sizes = sizes[inv]
+    counts = np.diff(row_ptr)[inv]
+    new_ptr = np.concatenate([[0], np.cumsum(counts)])
+    new_cols = np.concatenate([np.sort(order[cols[row_ptr[r] : row_ptr[r + 1]]]) for r in inv])
+    a = native.analyze(new_sizes, new_ptr, new_cols)
+    slab = int(a["slab_bytes_fp64"]) // (2 if precision == native.MIXED else 1)
+    inv_bytes = 16384 * int(np.count_nonzero(sizes == 64)) if precision == native.MIXED else 0
+    rows = np.repeat(np.arange(n), np.diff(row_ptr))
+    nvals = int(np.sum(sizes[rows] * sizes[cols]))
+    return slab + 8 * nvals + 64 * int(sizes.sum()) + inv_bytes
+
+
 def plan_waves(weights, budget: int) -> list:
     """Indices of systems per wave: largest first, each into the first wave with room
     (first-fit decreasing); a system larger than the budget gets a wave of its own.

@@ -218,6 +218,20 @@ def mesh_system(n: int, p, seed: int = 0, nrhs: int = 1, shift: float = 1.0):
     return mat, rhs
 
 
+def mesh_pattern(n: int, p):
+    """The block pattern of ``mesh_system(n, p)`` without its values: ``(sizes, row_ptr,
+    cols)`` in the same (element-first) numbering, columns ascending in every row."""
+    sizes, elem_edges = mesh_layout(n, p)
+    ne = n * n
+    rows = np.concatenate([np.repeat(np.arange(ne), 4), elem_edges.ravel(), np.arange(len(sizes))])
+    cols = np.concatenate([elem_edges.ravel(), np.repeat(np.arange(ne), 4), np.arange(len(sizes))])
+    order = np.lexsort((cols, rows))
+    rows, cols = rows[order], cols[order]
+    row_ptr = np.zeros(len(sizes) + 1, dtype=np.int64)
+    np.add.at(row_ptr, rows + 1, 1)
+    return sizes.astype(np.int64), np.cumsum(row_ptr), cols.astype(np.int64)
+
+
 def random_orders(n: int, pmin: int, pmax: int, seed: int = 0) -> np.ndarray:
     """Per-element orders drawn uniformly from ``{pmin, ..., pmax}``."""
     return np.random.default_rng(seed).integers(pmin, pmax + 1, n * n)

@@ -224,3 +224,16 @@ def test_every_batched_system_converges_on_its_own_residual(gpu):
     for s, r in zip(per, res):
         assert s["relative_residual"] == pytest.approx(r, rel=1e-3, abs=2e-14)
     bs.close()
+
+
+@pytest.mark.parametrize(("side", "p"), [(3, 2), (5, 4), (4, 6)])
+def test_pattern_bytes_from_the_pattern_alone(native, side, p):
+    """Waves of many systems are planned before their values exist: the generator's
+    pattern alone gives the same pattern and the same device bytes as the full system."""
+    from hybsol.b200 import batch, meshgen
+
+    m, _ = meshgen.mesh_system(side, p, seed=7)
+    sizes, row_ptr, cols = meshgen.mesh_pattern(side, p)
+    assert np.array_equal(sizes, m.sizes) and np.array_equal(row_ptr, m.row_ptr) and np.array_equal(cols, m.cols)
+    for prec in (native.FP64, native.MIXED):
+        assert batch.pattern_bytes(sizes, row_ptr, cols, prec) == batch.device_bytes(m, prec)
