@@ -143,6 +143,7 @@ struct hyb_system
     int krylov_restart = 30;              // HYB_OPTION_KRYLOV_RESTART
     float growth_limit = 1024.0f;         // HYB_OPTION_GROWTH_LIMIT (mixed form)
     bool block_scaling = true;            // HYB_OPTION_BLOCK_SCALING (mixed form)
+    bool alternate_walk = true;           // HYB_OPTION_ALTERNATE_WALK
     bool factors_scaled = false;          // the current mixed factors are those of S A S
     double *d_bscale = nullptr;           // s_k per block row
     double *d_dscale = nullptr;           // s_k per unknown
@@ -513,6 +514,8 @@ template <typename T> int enqueue_update(hyb_system *h, T *slab, int64_t l, cuda
     const Symbolic::LevelShape &sh = S.shape[l];
     const unsigned tiles =
         (unsigned)(((sh.max_row + hyb::kTile - 1) / hyb::kTile) * ((sh.max_col + hyb::kTile - 1) / hyb::kTile));
+    // alternate levels walk their targets backwards (the priority launch keeps its order)
+    const int reverse = h->alternate_walk && mode != 1 && (l & 1) ? 1 : 0;
     if (S.lvl_listed[l])
     {
         const int64_t q0 = S.mt_lvl_ptr[l], nq = S.mt_lvl_ptr[l + 1] - q0;
@@ -533,7 +536,7 @@ template <typename T> int enqueue_update(hyb_system *h, T *slab, int64_t l, cuda
         if (sh.uniform64)
         {
             hyb::k_update64_f64<<<(unsigned)nu, hyb::kUpd64Threads, hyb::kUpd64Smem, st>>>(
-                ds, slab, p0, p1, mode, sh.la_i0, sh.la_j0, h->d_status);
+                ds, slab, p0, p1, mode, sh.la_i0, sh.la_j0, h->d_status, reverse);
             ++launches;
             HYB_LAUNCHED("k_update64_f64", l);
             return HYB_SUCCESS;
@@ -552,7 +555,7 @@ template <typename T> int enqueue_update(hyb_system *h, T *slab, int64_t l, cuda
                 const unsigned grid = (unsigned)std::min<int64_t>(tiles, (int64_t)sm_count());
                 hyb::k_update64_tc<<<grid, hyb::kTcThreads, hyb::kTcSmem, st>>>(
                     ds, slab, level_ops(h, l), level_tgt(h, l), p0, p1, mode, sh.la_i0, sh.la_j0, tiles,
-                    h->d_status);
+                    h->d_status, reverse);
                 ++launches;
                 HYB_LAUNCHED("k_update64_tc", l);
             }
@@ -1614,6 +1617,7 @@ HYB_API int hyb_system_copy(const hyb_system *src, hyb_system **out)
     h->krylov_restart = src->krylov_restart;
     h->growth_limit = src->growth_limit;
     h->block_scaling = src->block_scaling;
+    h->alternate_walk = src->alternate_walk;
     HYB_CUDA(create_streams(h.get()));
     int rc = upload_symbolic(h.get());
     if (rc != HYB_SUCCESS)
@@ -1713,6 +1717,14 @@ HYB_API int hyb_system_set_option(hyb_system *h, int option, int64_t value)
         if (value != h->krylov_restart)
             h->free_krylov();
         h->krylov_restart = (int)value;
+        return HYB_SUCCESS;
+    case HYB_OPTION_ALTERNATE_WALK:
+        if (h->alternate_walk != (value != 0))
+        {
+            h->alternate_walk = value != 0;
+            h->g_factor[0].reset();
+            h->g_factor[1].reset();
+        }
         return HYB_SUCCESS;
     case HYB_OPTION_BLOCK_SCALING:
         h->block_scaling = value != 0;

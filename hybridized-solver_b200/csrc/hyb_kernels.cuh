@@ -883,12 +883,13 @@ struct UpdUnit
     int64_t k, li, bu; // pivot, index into lcol_*, index into cols (the upper block)
 };
 
-__device__ __forceinline__ UpdUnit update_unit(const DevSym &S, int64_t p0, int64_t p1, int mode, int i0, int j0)
+__device__ __forceinline__ UpdUnit update_unit(const DevSym &S, int64_t p0, int64_t p1, int mode, int i0, int j0,
+                                               int64_t unit)
 {
-    int64_t p = p0, local = blockIdx.x;
+    int64_t p = p0, local = unit;
     if (mode == 0)
     {
-        const int64_t u = S.upd_pref[p0] + blockIdx.x;
+        const int64_t u = S.upd_pref[p0] + unit;
         p = find_owner(S.upd_pref, p0, p1, u);
         local = u - S.upd_pref[p];
     }
@@ -932,7 +933,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 {
     __shared__ __align__(16) T sa[kTileKC * kLdA];
     __shared__ __align__(16) T sb[kTileKC * kTile];
-    const UpdUnit w = update_unit(S, p0, p1, mode, i0, j0);
+    const UpdUnit w = update_unit(S, p0, p1, mode, i0, j0, blockIdx.x);
     const int64_t k = w.k, li = w.li, bu = w.bu;
     const int32_t t = S.lcol_row[li];
     const int32_t c = S.cols[bu];
@@ -970,7 +971,7 @@ __global__ void __launch_bounds__(kSmallThreads, 8)
     constexpr int kPer = TL * KC / NT; // chunk values per thread, each of A and B
     __shared__ __align__(16) T sa[KC * LDA];
     __shared__ __align__(16) T sb[KC * TL];
-    const UpdUnit w = update_unit(S, p0, p1, mode, i0, j0);
+    const UpdUnit w = update_unit(S, p0, p1, mode, i0, j0, blockIdx.x);
     const int64_t k = w.k, li = w.li, bu = w.bu;
     const int32_t t = S.lcol_row[li];
     const int32_t c = S.cols[bu];
@@ -1143,14 +1144,16 @@ constexpr int kUpd64Smem = 2 * 64 * kLd64 * 8 + 16;
 // per DMMA). Work units as in k_update.
 __global__ void __launch_bounds__(kUpd64Threads)
     k_update64_f64(DevSym S, double *__restrict__ slab, int64_t p0, int64_t p1, int mode, int i0, int j0,
-                   int *status)
+                   int *status, int reverse)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double *sa = reinterpret_cast<double *>(smem_raw);
     double *sb = sa + 64 * kLd64;
     uint64_t *bar = reinterpret_cast<uint64_t *>(sb + 64 * kLd64);
 
-    const UpdUnit w = update_unit(S, p0, p1, mode, i0, j0);
+    // reverse: units in descending order, so the CTAs scheduled first at this level take the
+    // targets the previous level's last CTAs wrote (still in L2)
+    const UpdUnit w = update_unit(S, p0, p1, mode, i0, j0, reverse ? gridDim.x - 1 - blockIdx.x : blockIdx.x);
     const int64_t li = w.li, bu = w.bu;
     const int32_t t = S.lcol_row[li];
     const int32_t c = S.cols[bu];

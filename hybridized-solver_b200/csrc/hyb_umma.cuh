@@ -265,7 +265,7 @@ __device__ __forceinline__ TcTile tc_tile(const DevSym &S, int64_t p0, int64_t p
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_update64_tc(DevSym S, float *__restrict__ slab, const unsigned char *__restrict__ ops,
                   const int64_t *__restrict__ tgt, int64_t p0, int64_t p1, int mode, int i0, int j0, int64_t n_tiles,
-                  int *status)
+                  int *status, int reverse)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>(
@@ -290,6 +290,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int64_t t0 = n_tiles * blockIdx.x / gridDim.x, t1 = n_tiles * (blockIdx.x + 1) / gridDim.x;
+    // With `reverse` the CTA walks its range from the end: on alternate levels every CTA
+    // starts on the targets it wrote last (consecutive levels update nearly the same
+    // targets), which are still in L2; column-pair-major order, and with it the reuse of
+    // the U pair, is kept. Every target's arithmetic is the same either way.
+    auto tix = [&](int64_t t) { return reverse ? t0 + t1 - 1 - t : t; };
     if (tid == 0)
     {
         for (int i = 0; i < kTcStages; ++i)
@@ -349,7 +354,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             int64_t na = -1, nb = -1;
             if (t0 < t1)
             {
-                xn = tc_tile(S, p0, p1, mode, i0, j0, t0);
+                xn = tc_tile(S, p0, p1, mode, i0, j0, tix(t0));
                 targets(xn, na, nb);
             }
             int64_t i = 0;
@@ -359,7 +364,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 const int64_t off_a = na, off_b = nb;
                 if (t + 1 < t1)
                 {
-                    xn = tc_tile(S, p0, p1, mode, i0, j0, t + 1);
+                    xn = tc_tile(S, p0, p1, mode, i0, j0, tix(t + 1));
                     targets(xn, na, nb);
                 }
                 const int64_t k = S.piv[x.p];
@@ -435,7 +440,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             int64_t i = 0;
             for (int64_t t = t0; t < t1; ++t, ++i)
             {
-                const TcTile x = tc_tile(S, p0, p1, mode, i0, j0, t);
+                const TcTile x = tc_tile(S, p0, p1, mode, i0, j0, tix(t));
                 if (x.p != cur_p || x.ja != cur_a || x.jb != cur_b)
                 {
                     if (uloads > 0)

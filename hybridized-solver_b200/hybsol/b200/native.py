@@ -36,6 +36,7 @@ OPTION_FP64_REFINEMENT = 6
 OPTION_KRYLOV_RESTART = 7
 OPTION_GROWTH_LIMIT = 8
 OPTION_BLOCK_SCALING = 9
+OPTION_ALTERNATE_WALK = 10
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _i64p = ctypes.POINTER(ctypes.c_int64)

@@ -200,7 +200,11 @@ typedef enum
      * FP32 / BF16-split factorization with entries of order one; the solves apply S on both
      * sides and the refinement's residual stays that of the unscaled FP64 A. hyb_get_block
      * then returns the scaled factors. 0: the factors of A itself. */
-    HYB_OPTION_BLOCK_SCALING = 9
+    HYB_OPTION_BLOCK_SCALING = 9,
+    /* 1 (default): the Schur updates of 64-blocks walk their targets backwards on every
+     * other level, so each level starts on the targets the previous one wrote last (still in
+     * L2); 0: always forwards. Both give the same factors. */
+    HYB_OPTION_ALTERNATE_WALK = 10
 } hyb_option;
 
 /* Sets a schedule option of the handle (takes effect at the next decomposition). */

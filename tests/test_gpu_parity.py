@@ -233,6 +233,21 @@ def test_lookahead_schedule_matches_in_order(gpu, prec):
 
 
 @pytest.mark.parametrize("prec", [0, 1])
+def test_alternating_walk_matches_forward(gpu, prec):
+    """Walking the targets backwards on alternate levels changes only which CTA updates a
+    target when, not its arithmetic: the factors are bit-identical."""
+    mat, b = _mesh(12, 8, seed=14)
+    order, pm, ns = _native_from(gpu, mat)
+    ns.decompose(prec)
+    blocks = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
+    ns.set_option(gpu.OPTION_ALTERNATE_WALK, 0)
+    ns.set_values(pm.vals)
+    ns.decompose(prec)
+    blocks2 = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
+    assert all(np.array_equal(x, y) for x, y in zip(blocks, blocks2))
+
+
+@pytest.mark.parametrize("prec", [0, 1])
 def test_sampled_update_profile(gpu, prec):
     """Event pairs around every n-th level's update: ceil(levels / n) timed levels, the same
     level count for every stride, and factors identical to an untimed decomposition."""
