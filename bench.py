@@ -63,6 +63,7 @@ def parse_args():
         default="8",
         help="element order: an integer, or 'rand' for a per-element order drawn uniformly from 2..10 (seed 0)",
     )
+    ap.add_argument("--nrhs", type=int, default=1, help="right-hand sides per solve (configs with 4 RHS)")
     ap.add_argument("--cpu-sample-mesh", type=int, default=CPU_SAMPLE_MESH)
     ap.add_argument(
         "--ref-threads",
@@ -145,11 +146,13 @@ def workload_config(n, p, extra=None):
     else:
         p = int(p)
         blocks = f"p={p} (element blocks {p * p}x{p * p}, edge blocks {p}x{p})"
+    nrhs = int((extra or {}).pop("nrhs", 1))
     cfg = {
-        "workload": f"hybridized quad mesh {n}x{n} elements, {blocks}, 1 RHS, seed 0, reference first-fit coloring order",
+        "workload": f"hybridized quad mesh {n}x{n} elements, {blocks}, {nrhs} RHS, seed 0, reference first-fit "
+        "coloring order",
         "mesh": f"{n}x{n}",
         "p": p,
-        "nrhs": 1,
+        "nrhs": nrhs,
         "tolerance": TOL,
         "l2": "inputs larger than L2 (factor slab >> 126 MB)",
     }
@@ -174,12 +177,12 @@ def element_orders(n, p):
     return int(p)
 
 
-def build_workload(n, p, with_order=False, shift=1.0):
+def build_workload(n, p, with_order=False, shift=1.0, nrhs=1):
     import numpy as np
 
     from hybsol.b200 import batch, meshgen, native
 
-    mat, b = meshgen.mesh_system(n, element_orders(n, p), seed=0, shift=shift)
+    mat, b = meshgen.mesh_system(n, element_orders(n, p), seed=0, shift=shift, nrhs=nrhs)
     order = native.compute_ordering(mat.row_ptr, mat.cols, "first")
     pm = mat.permuted(order)
     perm = batch.dof_permutation(mat.sizes, order)  # x_new[perm] = x_old
@@ -698,7 +701,8 @@ def run_ours(args):
     fp32_peak = gemm_peak(torch.float32)
 
     t0 = time.perf_counter()
-    pm, bn = build_workload(args.mesh, args.p, shift=args.alpha)
+    pm, bn = build_workload(args.mesh, args.p, shift=args.alpha, nrhs=args.nrhs)
+    nr = args.nrhs
     gen_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     ns = native.NativeSystem(pm.sizes, pm.row_ptr, pm.cols)
@@ -722,7 +726,7 @@ def run_ours(args):
         native._check(lib.hyb_system_set_values(ns._h, native._ptr(d_vals), native.MEMORY_DEVICE), "set_values")
         ns.decompose(prec)
         launches += ns.last_launch_count()
-        info = ns.solve_device(d_b, d_x, 1, tol=TOL, max_iter=60, residual=(prec == native.MIXED or reduced))
+        info = ns.solve_device(d_b, d_x, nr, tol=TOL, max_iter=60, residual=(prec == native.MIXED or reduced))
         launches += ns.last_launch_count()
         return launches, info
 
@@ -771,7 +775,7 @@ def run_ours(args):
         native._check(lib.hyb_system_set_values(ns._h, native._ptr(h_vals), native.MEMORY_HOST), "set_values")
         ns.decompose(native.MIXED)
         st = lib.hyb_solve(
-            ns._h, native._ptr(h_b), native._ptr(h_x), 1, native.MEMORY_HOST, TOL, 60, ctypes.byref(sinfo)
+            ns._h, native._ptr(h_b), native._ptr(h_x), nr, native.MEMORY_HOST, TOL, 60, ctypes.byref(sinfo)
         )
         native._check(st, "hyb_solve")
 
@@ -881,6 +885,7 @@ def run_ours(args):
                     "factor_gflop": flops / 1e9,
                     "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                     "alpha": args.alpha,
+                    "nrhs": args.nrhs,
                 },
             ),
             "fp64_ms": fp64_ms,
