@@ -113,6 +113,31 @@ __global__ void k_status_init(int *st)
     }
 }
 
+// Size buckets of the update tuner: the pivot size and the largest target dimension of a
+// level, each rounded up to one of 8, 16, 32, 64, 128, 256 or more.
+constexpr int kSizeClasses = 7;
+constexpr int hyb_tuning_buckets()
+{
+    return kSizeClasses * kSizeClasses;
+}
+
+int size_class(int x)
+{
+    int c = 0;
+    for (int lim = 8; c < kSizeClasses - 1 && x > lim; lim *= 2)
+        ++c;
+    return c;
+}
+
+// Generic-size Schur-update kernels the tuner chooses among.
+enum UpdateKernel
+{
+    UPD_TILE32 = 0, // k_update32: 64-thread CTAs of one 32x32 output tile (targets up to 256 wide)
+    UPD_TILE64 = 1, // k_update: one 256-thread CTA per target, its 64x64 tiles in turn
+    UPD_DMMA = 2,   // k_update_dmma: FP64 tensor pipe, one CTA per 64x64 tile (pivots up to 128 rows)
+    UPD_KINDS = 3
+};
+
 struct GraphExec
 {
     cudaGraphExec_t exec = nullptr;
@@ -144,6 +169,16 @@ struct hyb_system
     float growth_limit = 1024.0f;         // HYB_OPTION_GROWTH_LIMIT (mixed form)
     bool block_scaling = true;            // HYB_OPTION_BLOCK_SCALING (mixed form)
     bool alternate_walk = true;           // HYB_OPTION_ALTERNATE_WALK
+    // generic-size Schur updates: HYB_OPTION_UPDATE_KERNEL (-1: tuned per size bucket), and
+    // the tuned choice per precision and bucket (-1: not tuned yet)
+    int update_kernel = -1;
+    int tuned[2][hyb_tuning_buckets()];
+    hyb_system()
+    {
+        for (auto &row : tuned)
+            for (int &v : row)
+                v = -1;
+    }
     bool factors_scaled = false;          // the current mixed factors are those of S A S
     double *d_bscale = nullptr;           // s_k per block row
     double *d_dscale = nullptr;           // s_k per unknown
@@ -504,6 +539,154 @@ template <typename T> int enqueue_inverses(hyb_system *h, T *slab, uint64_t &lau
     return HYB_SUCCESS;
 }
 
+// Whether a generic update kernel can run a level's shapes.
+bool generic_kernel_fits(const Symbolic::LevelShape &sh, int kind)
+{
+    if (kind == UPD_TILE32)
+        return std::max(sh.max_row, sh.max_col) <= 8 * hyb::kSmallTile;
+    if (kind == UPD_DMMA)
+        return sh.max_piv <= hyb::kDmmaMaxK;
+    return true;
+}
+
+int level_bucket(const Symbolic::LevelShape &sh)
+{
+    return size_class(sh.max_piv) * kSizeClasses + size_class(std::max(sh.max_row, sh.max_col));
+}
+
+// The generic update kernel of level l: the forced one (HYB_OPTION_UPDATE_KERNEL) where it
+// fits, else the tuned choice of the level's size bucket, else the fixed rule (32x32 tiles
+// for targets up to 256 wide, 64x64 tiles beyond).
+template <typename T> int generic_kernel(const hyb_system *h, int64_t l)
+{
+    const Symbolic::LevelShape &sh = h->S.shape[l];
+    if (h->update_kernel >= 0 && generic_kernel_fits(sh, h->update_kernel))
+        return h->update_kernel;
+    const int tuned = h->tuned[std::is_same_v<T, float> ? 1 : 0][level_bucket(sh)];
+    if (tuned >= 0 && generic_kernel_fits(sh, tuned))
+        return tuned;
+    return generic_kernel_fits(sh, UPD_TILE32) ? UPD_TILE32 : UPD_TILE64;
+}
+
+template <typename T>
+int enqueue_generic_update(hyb_system *h, T *slab, int64_t l, cudaStream_t st, int mode, int64_t nu, int kind,
+                           uint64_t &launches)
+{
+    const Symbolic &S = h->S;
+    const DevSym &ds = h->ds;
+    const int64_t p0 = S.lvl_ptr[l], p1 = S.lvl_ptr[l + 1];
+    const Symbolic::LevelShape &sh = S.shape[l];
+    if (kind == UPD_TILE32)
+    {
+        // 64-thread CTAs of one 32x32 tile each (grid.y: the tiles of the largest target)
+        const unsigned t32 = (unsigned)(((sh.max_row + hyb::kSmallTile - 1) / hyb::kSmallTile) *
+                                        ((sh.max_col + hyb::kSmallTile - 1) / hyb::kSmallTile));
+        hyb::k_update32<T><<<dim3((unsigned)nu, t32), hyb::kSmallThreads, 0, st>>>(ds, slab, p0, p1, mode, sh.la_i0,
+                                                                                  sh.la_j0);
+        ++launches;
+        HYB_LAUNCHED("k_update32", l);
+        return HYB_SUCCESS;
+    }
+    if (kind == UPD_DMMA)
+    {
+        const unsigned t64 = (unsigned)(((sh.max_row + 63) / 64) * ((sh.max_col + 63) / 64));
+        hyb::k_update_dmma<T><<<dim3((unsigned)nu, t64), hyb::kDmmaThreads, hyb::dmma_smem_bytes(sh.max_piv), st>>>(
+            ds, slab, p0, p1, mode, sh.la_i0, sh.la_j0);
+        ++launches;
+        HYB_LAUNCHED("k_update_dmma", l);
+        return HYB_SUCCESS;
+    }
+    // one CTA per target block, looping over its 64x64 tiles
+    hyb::k_update<T><<<(unsigned)nu, hyb::kThreads, 0, st>>>(ds, slab, p0, p1, mode, sh.la_i0, sh.la_j0);
+    ++launches;
+    HYB_LAUNCHED("k_update", l);
+    return HYB_SUCCESS;
+}
+
+// Tunes the generic update kernel of every size bucket the factorization meets (T's
+// precision): on the bucket's level with the most update units, each kernel that fits is
+// run once to warm up and then three times under CUDA events; the fastest is kept. It runs
+// on the zeroed slab before the values are scattered (products of zeros: nothing changes).
+template <typename T> int tune_updates(hyb_system *h, T *slab)
+{
+    const Symbolic &S = h->S;
+    const int prec = std::is_same_v<T, float> ? 1 : 0;
+    std::vector<int64_t> rep(hyb_tuning_buckets(), -1);
+    for (int64_t l = 0; l < S.n_levels; ++l)
+    {
+        const Symbolic::LevelShape &sh = S.shape[l];
+        const int64_t p0 = S.lvl_ptr[l], p1 = S.lvl_ptr[l + 1];
+        const int64_t nu = S.upd_pref[p1] - S.upd_pref[p0];
+        if (S.lvl_listed[l] || nu == 0 || (std::is_same_v<T, double> && sh.uniform64) || tc_level<T>(h, l))
+            continue;
+        const int b = level_bucket(sh);
+        if (h->tuned[prec][b] >= 0)
+            continue;
+        if (rep[b] < 0 || nu > S.upd_pref[S.lvl_ptr[rep[b] + 1]] - S.upd_pref[S.lvl_ptr[rep[b]]])
+            rep[b] = l;
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    HYB_CUDA(cudaEventCreate(&e0));
+    HYB_CUDA(cudaEventCreate(&e1));
+    int rc = HYB_SUCCESS;
+    for (int b = 0; b < hyb_tuning_buckets() && rc == HYB_SUCCESS; ++b)
+    {
+        const int64_t l = rep[b];
+        if (l < 0)
+            continue;
+        const Symbolic::LevelShape &sh = S.shape[l];
+        const int64_t p0 = S.lvl_ptr[l], p1 = S.lvl_ptr[l + 1];
+        const int64_t nu = S.upd_pref[p1] - S.upd_pref[p0];
+        float best = INFINITY;
+        int best_kind = -1;
+        for (int kind = 0; kind < UPD_KINDS && rc == HYB_SUCCESS; ++kind)
+        {
+            if (!generic_kernel_fits(sh, kind))
+                continue;
+            uint64_t dummy = 0;
+            if ((rc = enqueue_generic_update<T>(h, slab, l, h->stream, 0, nu, kind, dummy)) != HYB_SUCCESS)
+                break;
+            cudaEventRecord(e0, h->stream);
+            for (int r = 0; r < 3 && rc == HYB_SUCCESS; ++r)
+                rc = enqueue_generic_update<T>(h, slab, l, h->stream, 0, nu, kind, dummy);
+            cudaEventRecord(e1, h->stream);
+            const cudaError_t e = cudaEventSynchronize(e1);
+            float ms = 0;
+            if (e == cudaSuccess)
+                cudaEventElapsedTime(&ms, e0, e1);
+            else
+                rc = cuda_fail(e, "tuning the update kernels");
+            if (rc == HYB_SUCCESS && ms < best)
+            {
+                best = ms;
+                best_kind = kind;
+            }
+        }
+        h->tuned[prec][b] = best_kind;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
+
+// Whether some level of the factorization in T's precision uses a generic update kernel
+// whose size bucket has not been tuned yet.
+template <typename T> bool needs_tuning(const hyb_system *h)
+{
+    const Symbolic &S = h->S;
+    const int prec = std::is_same_v<T, float> ? 1 : 0;
+    for (int64_t l = 0; l < S.n_levels; ++l)
+    {
+        const int64_t p0 = S.lvl_ptr[l], p1 = S.lvl_ptr[l + 1];
+        if (S.lvl_listed[l] || S.upd_pref[p1] == S.upd_pref[p0] || (std::is_same_v<T, double> && S.shape[l].uniform64) ||
+            tc_level<T>(h, l))
+            continue;
+        if (h->tuned[prec][level_bucket(S.shape[l])] < 0)
+            return true;
+    }
+    return false;
+}
+
 // Schur-complement updates of level l: mode 0 all of them, 1 / 2 the lookahead split.
 template <typename T> int enqueue_update(hyb_system *h, T *slab, int64_t l, cudaStream_t st, int mode,
                                          uint64_t &launches)
@@ -562,22 +745,7 @@ template <typename T> int enqueue_update(hyb_system *h, T *slab, int64_t l, cuda
             return HYB_SUCCESS;
         }
     }
-    if (std::max(sh.max_row, sh.max_col) <= 8 * hyb::kSmallTile)
-    {
-        // 64-thread CTAs of one 32x32 tile each (grid.y: the tiles of the largest target)
-        const unsigned t32 = (unsigned)(((sh.max_row + hyb::kSmallTile - 1) / hyb::kSmallTile) *
-                                        ((sh.max_col + hyb::kSmallTile - 1) / hyb::kSmallTile));
-        hyb::k_update32<T><<<dim3((unsigned)nu, t32), hyb::kSmallThreads, 0, st>>>(ds, slab, p0, p1, mode, sh.la_i0,
-                                                                                  sh.la_j0);
-        ++launches;
-        HYB_LAUNCHED("k_update32", l);
-        return HYB_SUCCESS;
-    }
-    // one CTA per target block, looping over its 64x64 tiles
-    hyb::k_update<T><<<(unsigned)nu, hyb::kThreads, 0, st>>>(ds, slab, p0, p1, mode, sh.la_i0, sh.la_j0);
-    ++launches;
-    HYB_LAUNCHED("k_update", l);
-    return HYB_SUCCESS;
+    return enqueue_generic_update<T>(h, slab, l, st, mode, nu, generic_kernel<T>(h, l), launches);
 }
 
 // Issues the whole factorization (used under graph capture). Levels run in order on the
@@ -878,6 +1046,7 @@ int check_handle(const hyb_system *h)
 {
     return h ? HYB_SUCCESS : HYB_INVALID_ARGUMENT;
 }
+
 
 // Device workspace of the dense block entry points, one per device: grown to the largest
 // request and kept until the process exits, so repeated calls allocate nothing. Callers hold
@@ -1618,6 +1787,8 @@ HYB_API int hyb_system_copy(const hyb_system *src, hyb_system **out)
     h->growth_limit = src->growth_limit;
     h->block_scaling = src->block_scaling;
     h->alternate_walk = src->alternate_walk;
+    h->update_kernel = src->update_kernel;
+    std::memcpy(h->tuned, src->tuned, sizeof(h->tuned));
     HYB_CUDA(create_streams(h.get()));
     int rc = upload_symbolic(h.get());
     if (rc != HYB_SUCCESS)
@@ -1718,6 +1889,16 @@ HYB_API int hyb_system_set_option(hyb_system *h, int option, int64_t value)
             h->free_krylov();
         h->krylov_restart = (int)value;
         return HYB_SUCCESS;
+    case HYB_OPTION_UPDATE_KERNEL:
+        if (value < -1 || value >= UPD_KINDS)
+            return HYB_INVALID_ARGUMENT;
+        if (value != h->update_kernel)
+        {
+            h->update_kernel = (int)value;
+            h->g_factor[0].reset();
+            h->g_factor[1].reset();
+        }
+        return HYB_SUCCESS;
     case HYB_OPTION_ALTERNATE_WALK:
         if (h->alternate_walk != (value != 0))
         {
@@ -1782,6 +1963,16 @@ HYB_API int hyb_system_set_segments(hyb_system *h, uint64_t nseg, const uint64_t
     return HYB_SUCCESS;
 }
 
+HYB_API int hyb_tuned_kernels(const hyb_system *h, int precision, int32_t kinds[49])
+{
+    if (check_handle(h) || !kinds || (precision != HYB_PRECISION_FP64 && precision != HYB_PRECISION_MIXED))
+        return HYB_INVALID_ARGUMENT;
+    static_assert(hyb_tuning_buckets() == 49, "the header declares 49 buckets");
+    for (int b = 0; b < hyb_tuning_buckets(); ++b)
+        kinds[b] = h->tuned[precision][b];
+    return HYB_SUCCESS;
+}
+
 HYB_API int hyb_segment_results(const hyb_system *h, uint32_t *iterations, double *relative_residual)
 {
     if (check_handle(h) || h->seg_off.empty())
@@ -1838,6 +2029,8 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
             allow_smem(hyb::k_update<float>, 0),
             allow_smem(hyb::k_update32<double>, 0),
             allow_smem(hyb::k_update32<float>, 0),
+            allow_smem(hyb::k_update_dmma<double>, hyb::dmma_smem_bytes(hyb::kDmmaMaxK)),
+            allow_smem(hyb::k_update_dmma<float>, hyb::dmma_smem_bytes(hyb::kDmmaMaxK)),
         };
         for (cudaError_t e : errs)
             if (e != cudaSuccess)
@@ -1866,6 +2059,14 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
             h->g_solve.clear();
         }
         HYB_CUDA(cudaMemsetAsync(h->d_f64, 0, slab * sizeof(double), h->stream));
+        if (h->update_kernel < 0 && needs_tuning<double>(h))
+        {
+            const int rc = tune_updates<double>(h, h->d_f64);
+            if (rc != HYB_SUCCESS)
+                return rc;
+            h->g_factor[0].reset(); // recaptured with the chosen kernels
+            HYB_CUDA(cudaMemsetAsync(h->d_f64, 0, slab * sizeof(double), h->stream));
+        }
         hyb::k_scatter<double><<<sgrid, hyb::kThreads, 0, h->stream>>>(h->ds, h->d_a, h->d_f64, S.nnz_a(), nullptr);
         h->last_launches += 1;
         const int rc = run_graph(h, h->g_factor[0], [&](uint64_t &count) {
@@ -1919,6 +2120,14 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
             h->g_factor[1].reset();
         }
         HYB_CUDA(cudaMemsetAsync(h->d_f32, 0, slab * sizeof(float), h->stream));
+        if (h->update_kernel < 0 && needs_tuning<float>(h))
+        {
+            const int rc = tune_updates<float>(h, h->d_f32);
+            if (rc != HYB_SUCCESS)
+                return rc;
+            h->g_factor[1].reset();
+            HYB_CUDA(cudaMemsetAsync(h->d_f32, 0, slab * sizeof(float), h->stream));
+        }
         h->factors_scaled = false;
         if (h->block_scaling)
         {

@@ -1233,6 +1233,102 @@ __global__ void __launch_bounds__(kUpd64Threads)
                 make_double2(acc[mi][ni][0], acc[mi][ni][1]);
 }
 
+// Generic-size Schur update on the FP64 tensor pipe (DMMA m8n8k4), for levels whose blocks
+// are not all 64 wide (uneven orders): one CTA per 64x64 tile of a target block (grid.y:
+// the tiles of the level's largest target; CTAs past a target's last tile return),
+// C(t,c)[tile] -= A(t,k) B(k,c) with A m x K and B K x n of any size, K <= kDmmaMaxK. The
+// operands are staged in shared memory as FP64, zero-padded to 64 rows/columns and to K
+// rounded up to 4 (padding adds exact zeros), C is held in DMMA accumulator fragments with
+// masked loads and stores; eight warps of 16x32 as in k_update64_f64. With T = float (the
+// mixed form's FP32 factors) the products are still formed in FP64 and rounded once.
+constexpr int kDmmaMaxK = 128;
+constexpr int kDmmaThreads = 256;
+
+__host__ __device__ constexpr int dmma_lda(int kp)
+{
+    return (kp + 15) / 16 * 16 + 4; // 64 + 4 for K = 64: the conflict-free stride of k_update64_f64
+}
+
+__host__ __device__ constexpr int dmma_smem_bytes(int k)
+{
+    return (64 * dmma_lda((k + 3) / 4 * 4) + (k + 3) / 4 * 4 * kLd64) * 8;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kDmmaThreads)
+    k_update_dmma(DevSym S, T *__restrict__ slab, int64_t p0, int64_t p1, int mode, int i0, int j0)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const UpdUnit w = update_unit(S, p0, p1, mode, i0, j0, blockIdx.x);
+    const int32_t t = S.lcol_row[w.li];
+    const int32_t c = S.cols[w.bu];
+    const int M = S.size[t], N = S.size[c], K = S.size[w.k];
+    const int tn = (N + 63) / 64, tm = (M + 63) / 64;
+    if ((int)blockIdx.y >= tm * tn)
+        return;
+    const int r0 = (blockIdx.y / tn) * 64, c0 = (blockIdx.y % tn) * 64;
+    const int mt = min(64, M - r0), nt = min(64, N - c0);
+    const int Kp = (K + 3) & ~3, lda = dmma_lda(Kp);
+    double *sa = reinterpret_cast<double *>(smem_raw); // 64 x lda: A rows r0.., K columns
+    double *sb = sa + 64 * lda;                        // Kp x kLd64: B rows, columns c0..
+    const int64_t tgt = warp_find_col(S.cols, S.row_ptr[t], S.row_ptr[t + 1], c);
+    const T *ga = slab + S.blk_off[S.lcol_blk[w.li]] + (int64_t)r0 * K;
+    const T *gb = slab + S.blk_off[w.bu] + c0;
+    T *gc = slab + S.blk_off[tgt] + (int64_t)r0 * N + c0;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < 64 * Kp; i += kDmmaThreads)
+    {
+        const int r = i / Kp, q = i - r * Kp;
+        sa[r * lda + q] = (r < mt && q < K) ? -(double)ga[(int64_t)r * K + q] : 0.0;
+    }
+    for (int i = tid; i < Kp * 64; i += kDmmaThreads)
+    {
+        const int q = i >> 6, cc = i & 63;
+        sb[q * kLd64 + cc] = (q < K && cc < nt) ? (double)gb[(int64_t)q * N + cc] : 0.0;
+    }
+    const int g = lane >> 2, qq = lane & 3;
+    const int wm = (warp >> 1) * 16, wn = (warp & 1) * 32;
+    double acc[2][4][2];
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int e = 0; e < 2; ++e)
+            {
+                const int r = wm + mi * 8 + g, cc = wn + ni * 8 + 2 * qq + e;
+                acc[mi][ni][e] = (r < mt && cc < nt) ? (double)gc[(int64_t)r * N + cc] : 0.0;
+            }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < Kp; kk += 4)
+    {
+        double av[2], bv[4];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+            av[mi] = sa[(wm + mi * 8 + g) * lda + kk + qq];
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+            bv[ni] = sb[(kk + qq) * kLd64 + wn + ni * 8 + g];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+                dmma_8x8x4(acc[mi][ni][0], acc[mi][ni][1], av[mi], bv[ni]);
+    }
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int e = 0; e < 2; ++e)
+            {
+                const int r = wm + mi * 8 + g, cc = wn + ni * 8 + 2 * qq + e;
+                if (r < mt && cc < nt)
+                    gc[(int64_t)r * N + cc] = (T)acc[mi][ni][e];
+            }
+}
+
 // Update of a level whose pivots share target rows: one CTA per listed target, its
 // sources applied in ascending pivot order.
 template <typename T>

@@ -37,6 +37,7 @@ OPTION_KRYLOV_RESTART = 7
 OPTION_GROWTH_LIMIT = 8
 OPTION_BLOCK_SCALING = 9
 OPTION_ALTERNATE_WALK = 10
+OPTION_UPDATE_KERNEL = 11  # -1 tuned, 0 32x32 SIMT, 1 64x64 SIMT, 2 DMMA
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _i64p = ctypes.POINTER(ctypes.c_int64)
@@ -169,6 +170,7 @@ EXPORTS = {
     ),
     "hyb_condition_estimate": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Condition)]),
     "hyb_system_set_segments": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _u64p]),
+    "hyb_tuned_kernels": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int32)]),
     "hyb_system_add_blocks": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_uint64, _u64p, _u64p, ctypes.c_void_p, ctypes.c_int],
@@ -424,6 +426,13 @@ class NativeSystem:
         if st == 1:
             raise KeyError("a block is not in the system's pattern")
         _check(st, "hyb_system_add_blocks")
+
+    def tuned_kernels(self, precision: int) -> np.ndarray:
+        """Tuned generic update kernel per size bucket (7 x 7: pivot class, target class), -1 untuned."""
+        out = np.empty(49, dtype=np.int32)
+        _check(lib().hyb_tuned_kernels(self._h, precision, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))),
+               "hyb_tuned_kernels")
+        return out.reshape(7, 7)
 
     def set_segments(self, offsets):
         """Independent systems stacked in this handle: segment s holds the unknowns

@@ -204,11 +204,24 @@ typedef enum
     /* 1 (default): the Schur updates of 64-blocks walk their targets backwards on every
      * other level, so each level starts on the targets the previous one wrote last (still in
      * L2); 0: always forwards. Both give the same factors. */
-    HYB_OPTION_ALTERNATE_WALK = 10
+    HYB_OPTION_ALTERNATE_WALK = 10,
+    /* Schur updates of levels whose blocks are not all 64 wide (uneven orders): -1
+     * (default) tunes the kernel per size bucket (pivot size and largest target dimension,
+     * each rounded up to 8, 16, ..., 256) at the first factorization that meets the bucket,
+     * timing every kernel that fits on the bucket's largest level, and keeps the fastest;
+     * 0: 32x32 SIMT tiles; 1: 64x64 SIMT tiles; 2: the FP64 tensor pipe (DMMA, pivots up
+     * to 128 rows, FP64 products also for FP32 factors). A kernel that does not fit a level
+     * falls back to the tuned or default choice. */
+    HYB_OPTION_UPDATE_KERNEL = 11
 } hyb_option;
 
 /* Sets a schedule option of the handle (takes effect at the next decomposition). */
 HYB_API int hyb_system_set_option(hyb_system *sys, int option, int64_t value);
+
+/* The tuned generic update kernel per size bucket (HYB_OPTION_UPDATE_KERNEL) of the given
+ * precision: `kinds[bucket]` for the 49 buckets (pivot class x 7 + target class, classes
+ * 8, 16, 32, 64, 128, 256, larger), -1 where no level of that bucket was tuned. */
+HYB_API int hyb_tuned_kernels(const hyb_system *sys, int precision, int32_t kinds[49]);
 
 /* Declares the system to be `nseg` independent systems stacked block-diagonally, segment s
  * holding the unknowns [offsets[s], offsets[s+1]) (offsets[0] = 0, ascending, offsets[nseg]

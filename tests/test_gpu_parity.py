@@ -401,3 +401,32 @@ def test_uneven_orders_large_pivot_grids(gpu, prec):
     ns.decompose(prec)
     x, info = ns.solve(bn)
     assert info["relative_residual"] < (1e-13 if prec == 0 else 1e-12)
+
+
+@pytest.mark.parametrize("kind", [-1, 0, 1, 2])
+def test_generic_update_kernels_match_oracle(gpu, kind):
+    """Uneven orders 2..10: every generic Schur-update kernel -- 32x32 and 64x64 SIMT tiles,
+    the FP64 tensor pipe (DMMA, operands zero-padded) and the tuned choice per size bucket --
+    gives the oracle's FP64 factors within 1e-12 per block; the mixed form (FP64 products
+    into FP32 factors on the DMMA path) refines to the FP64 solution."""
+    from hybsol.b200 import meshgen
+
+    pp = meshgen.random_orders(7, 2, 10, seed=19)
+    mat, b = _mesh(7, pp, seed=8, nrhs=2)
+    order, pm, ns = _native_from(gpu, mat)
+    bn = reorder_rhs(mat.sizes, order, b)
+    ns.set_option(gpu.OPTION_UPDATE_KERNEL, kind)
+    osys = O.OracleSystem.from_csr(pm.sizes, pm.row_ptr, pm.cols, pm.vals)
+    osys.decompose()
+    ns.decompose(gpu.FP64)
+    _check_factors(ns, osys, pm)
+    x, _ = ns.solve(bn)
+    xo = osys.solve(bn)
+    assert rel_err(x, xo) < TOL_X
+    if kind == -1:
+        tuned = ns.tuned_kernels(gpu.FP64)
+        assert (tuned >= 0).any() and set(np.unique(tuned[tuned >= 0])) <= {0, 1, 2}
+    ns.set_values(pm.vals)
+    ns.decompose(gpu.MIXED)
+    xm, im = ns.solve(bn)
+    assert im["converged"] and rel_err(xm, xo) < TOL_X_MIXED
