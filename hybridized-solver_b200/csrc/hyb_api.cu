@@ -187,6 +187,11 @@ struct hyb_system
     int *d_hg = nullptr;
     double *d_piv64 = nullptr;
     int64_t *d_g64_off = nullptr;
+    // FP64 LUs of high-growth 64-row pivots between k_lu64_once and k_trsm64_strips: two
+    // level-parity halves of fused_half slots of 64 x 64 doubles
+    double *d_piv64f = nullptr;
+    int64_t fused_half = 0;
+    bool lu_once = true; // HYB_OPTION_PIVOT_LU_ONCE
     // independent systems stacked in one handle (hyb_system_set_segments): unknown offsets,
     // their device copy, norms per segment and column, and the last solve's results
     std::vector<int64_t> seg_off;
@@ -277,6 +282,7 @@ struct hyb_system
         cudaFree(d_seg_off);
         cudaFree(d_seg_norm);
         cudaFree(d_hg);
+        cudaFree(d_piv64f);
         cudaFree(d_bscale);
         cudaFree(d_dscale);
         cudaFree(d_piv64);
@@ -470,6 +476,12 @@ template <typename T> int enqueue_split(hyb_system *h, T *slab, int64_t l, cudaS
     return HYB_SUCCESS;
 }
 
+// Whether a level's pivots take the 64-row kernels (33-64 rows, upper blocks up to 128 wide).
+bool fused_pivots(const Symbolic::LevelShape &sh)
+{
+    return sh.max_piv > 32 && sh.max_piv <= 64 && sh.max_up <= 128;
+}
+
 template <typename T> int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cudaStream_t st, uint64_t &launches)
 {
     const Symbolic &S = h->S;
@@ -479,10 +491,38 @@ template <typename T> int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cuda
     const Symbolic::LevelShape &sh = S.shape[l];
     // growth check and FP64 fallback of the mixed form (0: off, and always for FP64 factors)
     const float glim = std::is_same_v<T, float> && h->d_hg ? h->growth_limit : 0.0f;
-    if (sh.max_piv > 32 && sh.max_piv <= 64 && sh.max_up <= 128)
+    if (fused_pivots(sh))
     {
         // fused: diagonal LU (padded to 64x64) and the solves of the pivot rows' upper blocks;
         // pivots of up to 32 rows stay on the generic kernels, whose serial steps are short
+        if (h->lu_once)
+        {
+            // each pivot factored once, then the strips from the stored factors
+            int *hg = glim > 0 ? h->d_hg : nullptr;
+            double *f64 = glim > 0 ? h->d_piv64f + (l & 1) * h->fused_half * 4096 : nullptr;
+            if (sh.piv64)
+                hyb::k_lu64_once<T, false><<<(unsigned)(p1 - p0), hyb::kThreads, hyb::lu64_once_smem<T>(), st>>>(
+                    ds, slab, p0, h->d_status, glim, hg, f64);
+            else
+                hyb::k_lu64_once<T, true><<<(unsigned)(p1 - p0), hyb::kThreads, hyb::lu64_once_smem<T>(), st>>>(
+                    ds, slab, p0, h->d_status, glim, hg, f64);
+            ++launches;
+            HYB_LAUNCHED("k_lu64_once", l);
+            const int64_t n_trsm = S.trsm_pref[p1] - S.trsm_pref[p0];
+            if (n_trsm > 0)
+            {
+                const dim3 grid((unsigned)n_trsm, sh.max_up > 64 ? 2u : 1u);
+                if (sh.piv64)
+                    hyb::k_trsm64_strips<T, false><<<grid, hyb::kThreads, hyb::lu_trsm64_smem<T>(), st>>>(
+                        ds, slab, p0, p1, hg, f64);
+                else
+                    hyb::k_trsm64_strips<T, true><<<grid, hyb::kThreads, hyb::lu_trsm64_smem<T>(), st>>>(
+                        ds, slab, p0, p1, hg, f64);
+                ++launches;
+                HYB_LAUNCHED("k_trsm64_strips", l);
+            }
+            return enqueue_split<T>(h, slab, l, st, launches);
+        }
         const int64_t units = S.lu_pref[p1] - S.lu_pref[p0];
         const dim3 grid((unsigned)units, sh.max_up > 64 ? 2u : 1u);
         if (sh.piv64) // every pivot and upper block exactly 64: no padding
@@ -1788,6 +1828,7 @@ HYB_API int hyb_system_copy(const hyb_system *src, hyb_system **out)
     h->block_scaling = src->block_scaling;
     h->alternate_walk = src->alternate_walk;
     h->update_kernel = src->update_kernel;
+    h->lu_once = src->lu_once;
     std::memcpy(h->tuned, src->tuned, sizeof(h->tuned));
     HYB_CUDA(create_streams(h.get()));
     int rc = upload_symbolic(h.get());
@@ -1888,6 +1929,14 @@ HYB_API int hyb_system_set_option(hyb_system *h, int option, int64_t value)
         if (value != h->krylov_restart)
             h->free_krylov();
         h->krylov_restart = (int)value;
+        return HYB_SUCCESS;
+    case HYB_OPTION_PIVOT_LU_ONCE:
+        if (h->lu_once != (value != 0))
+        {
+            h->lu_once = value != 0;
+            h->g_factor[0].reset();
+            h->g_factor[1].reset();
+        }
         return HYB_SUCCESS;
     case HYB_OPTION_UPDATE_KERNEL:
         if (value < -1 || value >= UPD_KINDS)
@@ -2030,6 +2079,14 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
             allow_smem(hyb::k_update32<double>, 0),
             allow_smem(hyb::k_update32<float>, 0),
             allow_smem(hyb::k_update_dmma<double>, hyb::dmma_smem_bytes(hyb::kDmmaMaxK)),
+            allow_smem(hyb::k_lu64_once<double, false>, hyb::lu64_once_smem<double>()),
+            allow_smem(hyb::k_lu64_once<double, true>, hyb::lu64_once_smem<double>()),
+            allow_smem(hyb::k_lu64_once<float, false>, hyb::lu64_once_smem<float>()),
+            allow_smem(hyb::k_lu64_once<float, true>, hyb::lu64_once_smem<float>()),
+            allow_smem(hyb::k_trsm64_strips<double, false>, hyb::lu_trsm64_smem<double>()),
+            allow_smem(hyb::k_trsm64_strips<double, true>, hyb::lu_trsm64_smem<double>()),
+            allow_smem(hyb::k_trsm64_strips<float, false>, hyb::lu_trsm64_smem<float>()),
+            allow_smem(hyb::k_trsm64_strips<float, true>, hyb::lu_trsm64_smem<float>()),
             allow_smem(hyb::k_update_dmma<float>, hyb::dmma_smem_bytes(hyb::kDmmaMaxK)),
         };
         for (cudaError_t e : errs)
@@ -2109,6 +2166,16 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
             HYB_CUDA(cudaMalloc(&h->d_piv64, std::max<int64_t>(1, total) * sizeof(double)));
             HYB_CUDA(cudaMalloc(&h->d_g64_off, S.n * sizeof(int64_t)));
             HYB_CUDA(cudaMemcpy(h->d_g64_off, off.data(), S.n * sizeof(int64_t), cudaMemcpyHostToDevice));
+            // slots for the FP64 LUs of high-growth pivots of the fused 33-64-row levels
+            int64_t most = 0;
+            for (int64_t l = 0; l < S.n_levels; ++l)
+            {
+                const Symbolic::LevelShape &sh = S.shape[l];
+                if (fused_pivots(sh))
+                    most = std::max(most, S.lvl_ptr[l + 1] - S.lvl_ptr[l]);
+            }
+            h->fused_half = std::max<int64_t>(1, most);
+            HYB_CUDA(cudaMalloc(&h->d_piv64f, 2 * h->fused_half * 4096 * sizeof(double)));
             h->g_factor[1].reset();
         }
         if (h->umma && !h->d_ops && S.max_split_blocks > 0)

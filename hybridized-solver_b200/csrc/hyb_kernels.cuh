@@ -778,6 +778,143 @@ __global__ void __launch_bounds__(kThreads, 1)
     trsm64_columns<T, kPad>(dtl, dtu, diag, slab + S.blk_off[blk] + col0, cc, m, min(64, cc - col0));
 }
 
+// The same pivots in two launches, without the redundant factorizations: k_lu64_once
+// factors each pivot of the level once (one CTA per pivot) and k_trsm64_strips solves the
+// strips (one CTA per upper block and 64-column strip) from the stored factors, with the
+// same arithmetic as k_lu_trsm64 -- the factors are bit-identical. Mixed form: a pivot past
+// the growth limit is refactored in FP64 by its LU CTA, which stores the FP64 LU (64 x 64)
+// in `piv64` at the pivot's index in the level and sets hg[k]; its strips are then solved
+// in FP64 with that LU.
+template <typename T> constexpr int lu64_once_smem()
+{
+    return std::is_same_v<T, float> ? (64 * kLd65 + 256) * 8 : (64 * kLd65 + 256) * (int)sizeof(T);
+}
+
+template <typename T, bool kPad>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_lu64_once(DevSym S, T *__restrict__ slab, int64_t p0, int *status, float growth_limit, int *__restrict__ hg,
+                double *__restrict__ piv64)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *d = reinterpret_cast<T *>(smem_raw);
+    T *rowbuf = d + 64 * kLd65;
+    T *colbuf = rowbuf + 128;
+    const int64_t k = S.piv[p0 + blockIdx.x];
+    const int m = kPad ? S.size[k] : 64;
+    T *gd = slab + S.blk_off[S.diag_pos[k]];
+    const bool check = std::is_same_v<T, float> && growth_limit > 0;
+    T amax = T(0);
+    for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
+    {
+        const int r = i >> 6, c = i & 63;
+        const T v = (!kPad || (r < m && c < m)) ? gd[r * m + c] : T(r == c);
+        d[r * kLd65 + c] = v;
+        if (!kPad || (r < m && c < m))
+            amax = fmax(amax, fabs(v));
+    }
+    __syncthreads();
+    lu64_shared(d, rowbuf, colbuf, status, (int)k);
+    if (check)
+    {
+        amax = cta_max(amax);
+        if (lu_growth(d, m, kLd65, amax) > (T)growth_limit)
+        {
+            // refactor from the original values (still in the slab) in FP64, in the same
+            // shared memory reinterpreted
+            double *d64 = reinterpret_cast<double *>(smem_raw);
+            double *rb = d64 + 64 * kLd65, *cb = rb + 128;
+            __syncthreads();
+            for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
+            {
+                const int r = i >> 6, c = i & 63;
+                d64[r * kLd65 + c] = (r < m && c < m) ? (double)gd[r * m + c] : double(r == c);
+            }
+            __syncthreads();
+            lu64_shared(d64, rb, cb, (int *)nullptr, (int)k);
+            double *slot = piv64 + (int64_t)blockIdx.x * 4096;
+            for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
+                slot[i] = d64[(i >> 6) * kLd65 + (i & 63)];
+            for (int i = threadIdx.x; i < m * m; i += blockDim.x)
+                gd[i] = (T)d64[(i / m) * kLd65 + i % m];
+            if (threadIdx.x == 0)
+            {
+                hg[k] = 1;
+                atomicAdd(status + ST_GROWTH_FP64, 1);
+            }
+            return;
+        }
+    }
+    for (int i = threadIdx.x; i < m * m; i += blockDim.x)
+        gd[i] = kPad ? d[(i / m) * kLd65 + i % m] : d[(i >> 6) * kLd65 + (i & 63)];
+}
+
+template <typename T, bool kPad>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_trsm64_strips(DevSym S, T *__restrict__ slab, int64_t p0, int64_t p1, const int *__restrict__ hg,
+                    const double *__restrict__ piv64)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int64_t u = S.trsm_pref[p0] + blockIdx.x;
+    const int64_t p = find_owner(S.trsm_pref, p0, p1, u);
+    const int64_t k = S.piv[p];
+    const int64_t blk = S.diag_pos[k] + 1 + (u - S.trsm_pref[p]);
+    const int m = kPad ? S.size[k] : 64;
+    const int cc = kPad ? S.size[S.cols[blk]] : 64;
+    const int col0 = 64 * (int)blockIdx.y;
+    if (col0 >= cc)
+        return;
+    const int w = min(64, cc - col0);
+    const T *gd = slab + S.blk_off[S.diag_pos[k]];
+    if constexpr (std::is_same_v<T, float>)
+    {
+        if (hg && hg[k])
+        {
+            // FP64 row solve with the pivot's FP64 LU, the strip in two 32-column halves
+            double *d = reinterpret_cast<double *>(smem_raw);
+            double *sb = d + 64 * kLd65 + 256;
+            const double *slot = piv64 + (p - p0) * 4096;
+            for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
+                d[(i >> 6) * kLd65 + (i & 63)] = slot[i];
+            for (int h0 = 0; h0 < w; h0 += 32)
+            {
+                const int wh = min(32, w - h0);
+                float *gb = slab + S.blk_off[blk] + col0 + h0;
+                __syncthreads();
+                for (int i = threadIdx.x; i < m * wh; i += blockDim.x)
+                    sb[(i / wh) * kLd33 + i % wh] = (double)gb[(i / wh) * cc + i % wh];
+                __syncthreads();
+                lu_solve_strip_warp(d, kLd65, sb, kLd33, m, wh);
+                __syncthreads();
+                for (int i = threadIdx.x; i < m * wh; i += blockDim.x)
+                    gb[(i / wh) * cc + i % wh] = (float)sb[(i / wh) * kLd33 + i % wh];
+            }
+            return;
+        }
+    }
+    T *d = reinterpret_cast<T *>(smem_raw);
+    T *dtl = d + 64 * kLd65;
+    T *dtu = dtl + 64 * kLdT;
+    T *diag = dtu + 64 * kLdT;
+    // the factored block, padded with the identity as k_lu_trsm64 holds it
+    for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
+    {
+        const int r = i >> 6, c = i & 63;
+        d[r * kLd65 + c] = (!kPad || (r < m && c < m)) ? gd[r * m + c] : T(r == c);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
+    {
+        const int c = i >> 6, r = i & 63;
+        const T v = d[r * kLd65 + c];
+        dtl[dt_idx(c, r)] = r > c ? v : T(0);
+        dtu[dt_idx(c, r)] = r < c ? v : T(0);
+        if (r == c)
+            diag[c] = v;
+    }
+    __syncthreads();
+    trsm64_columns<T, kPad>(dtl, dtu, diag, slab + S.blk_off[blk] + col0, cc, m, w);
+}
+
 // ----------------------------------------------------------------------------------
 // Generic tiled update of one 64x64 output tile: acc -= A * B with A (M x K, lda) and
 // B (K x N, ldb), both row-major; 256 threads, 4x4 outputs each.

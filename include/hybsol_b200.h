@@ -212,7 +212,12 @@ typedef enum
      * 0: 32x32 SIMT tiles; 1: 64x64 SIMT tiles; 2: the FP64 tensor pipe (DMMA, pivots up
      * to 128 rows, FP64 products also for FP32 factors). A kernel that does not fit a level
      * falls back to the tuned or default choice. */
-    HYB_OPTION_UPDATE_KERNEL = 11
+    HYB_OPTION_UPDATE_KERNEL = 11,
+    /* Pivots of 33-64 rows: 1 (default) factors each diagonal block once and then solves
+     * its row's upper blocks from the stored factors (two launches); 0: one fused launch in
+     * which every CTA of a pivot factors the block itself before its strip. Both give the
+     * same factors. */
+    HYB_OPTION_PIVOT_LU_ONCE = 12
 } hyb_option;
 
 /* Sets a schedule option of the handle (takes effect at the next decomposition). */

@@ -248,6 +248,25 @@ def test_alternating_walk_matches_forward(gpu, prec):
 
 
 @pytest.mark.parametrize("prec", [0, 1])
+@pytest.mark.parametrize("p", [8, "rand"])
+def test_pivot_lu_once_matches_fused(gpu, prec, p):
+    """Factoring each 33-64-row pivot once and solving its strips from the stored factors
+    gives the fused kernel's factors bit for bit (padded pivots of uneven orders included)."""
+    from hybsol.b200 import meshgen
+
+    pp = meshgen.random_orders(8, 2, 10, seed=31) if p == "rand" else p
+    mat, b = _mesh(8, pp, seed=15)
+    order, pm, ns = _native_from(gpu, mat)
+    ns.decompose(prec)
+    blocks = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
+    ns.set_option(gpu.OPTION_PIVOT_LU_ONCE, 0)
+    ns.set_values(pm.vals)
+    ns.decompose(prec)
+    blocks2 = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
+    assert all(np.array_equal(x, y) for x, y in zip(blocks, blocks2))
+
+
+@pytest.mark.parametrize("prec", [0, 1])
 def test_sampled_update_profile(gpu, prec):
     """Event pairs around every n-th level's update: ceil(levels / n) timed levels, the same
     level count for every stride, and factors identical to an untimed decomposition."""
