@@ -191,7 +191,7 @@ struct hyb_system
     // level-parity halves of fused_half slots of 64 x 64 doubles
     double *d_piv64f = nullptr;
     int64_t fused_half = 0;
-    bool lu_once = true; // HYB_OPTION_PIVOT_LU_ONCE
+    int lu_once = -1; // HYB_OPTION_PIVOT_LU_ONCE: -1 per precision (FP64 once, mixed fused)
     // independent systems stacked in one handle (hyb_system_set_segments): unknown offsets,
     // their device copy, norms per segment and column, and the last solve's results
     std::vector<int64_t> seg_off;
@@ -495,7 +495,10 @@ template <typename T> int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cuda
     {
         // fused: diagonal LU (padded to 64x64) and the solves of the pivot rows' upper blocks;
         // pivots of up to 32 rows stay on the generic kernels, whose serial steps are short
-        if (h->lu_once)
+        // measured at 128x128 p=8: FP64 6,369 ms once against 6,770 fused (the redundant FP64
+        // LUs take SM time from the DMMA update); mixed 1,794 against 1,766 (its FP32 LU is
+        // cheap, and the extra launch lands on the pivot chain)
+        if (h->lu_once < 0 ? std::is_same_v<T, double> : h->lu_once != 0)
         {
             // each pivot factored once, then the strips from the stored factors
             int *hg = glim > 0 ? h->d_hg : nullptr;
@@ -1931,9 +1934,11 @@ HYB_API int hyb_system_set_option(hyb_system *h, int option, int64_t value)
         h->krylov_restart = (int)value;
         return HYB_SUCCESS;
     case HYB_OPTION_PIVOT_LU_ONCE:
-        if (h->lu_once != (value != 0))
+        if (value < -1 || value > 1)
+            return HYB_INVALID_ARGUMENT;
+        if (h->lu_once != (int)value)
         {
-            h->lu_once = value != 0;
+            h->lu_once = (int)value;
             h->g_factor[0].reset();
             h->g_factor[1].reset();
         }

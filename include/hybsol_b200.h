@@ -213,10 +213,12 @@ typedef enum
      * to 128 rows, FP64 products also for FP32 factors). A kernel that does not fit a level
      * falls back to the tuned or default choice. */
     HYB_OPTION_UPDATE_KERNEL = 11,
-    /* Pivots of 33-64 rows: 1 (default) factors each diagonal block once and then solves
-     * its row's upper blocks from the stored factors (two launches); 0: one fused launch in
-     * which every CTA of a pivot factors the block itself before its strip. Both give the
-     * same factors. */
+    /* Pivots of 33-64 rows: 1 factors each diagonal block once and then solves its row's
+     * upper blocks from the stored factors (two launches); 0: one fused launch in which every
+     * CTA of a pivot factors the block itself before its strip; -1 (default): 1 for the FP64
+     * form (its LU is costly and the redundant copies slow the concurrent update), 0 for the
+     * mixed form (its FP32 LU is cheap and the extra launch lengthens the pivot chain). All
+     * give the same factors. */
     HYB_OPTION_PIVOT_LU_ONCE = 12
 } hyb_option;
 

@@ -257,6 +257,7 @@ def test_pivot_lu_once_matches_fused(gpu, prec, p):
     pp = meshgen.random_orders(8, 2, 10, seed=31) if p == "rand" else p
     mat, b = _mesh(8, pp, seed=15)
     order, pm, ns = _native_from(gpu, mat)
+    ns.set_option(gpu.OPTION_PIVOT_LU_ONCE, 1)
     ns.decompose(prec)
     blocks = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
     ns.set_option(gpu.OPTION_PIVOT_LU_ONCE, 0)
