@@ -192,6 +192,7 @@ struct hyb_system
     double *d_piv64f = nullptr;
     int64_t fused_half = 0;
     int lu_once = -1; // HYB_OPTION_PIVOT_LU_ONCE: -1 per precision (FP64 once, mixed fused)
+    int fp64_shape = 0; // HYB_OPTION_FP64_MMA_SHAPE
     // independent systems stacked in one handle (hyb_system_set_segments): unknown offsets,
     // their device copy, norms per segment and column, and the last solve's results
     std::vector<int64_t> seg_off;
@@ -761,8 +762,17 @@ template <typename T> int enqueue_update(hyb_system *h, T *slab, int64_t l, cuda
     {
         if (sh.uniform64)
         {
-            hyb::k_update64_f64<<<(unsigned)nu, hyb::kUpd64Threads, hyb::kUpd64Smem, st>>>(
-                ds, slab, p0, p1, mode, sh.la_i0, sh.la_j0, h->d_status, reverse);
+            // FP64 MMA instruction shape (HYB_OPTION_FP64_MMA_SHAPE); every shape applies the
+            // same products, only the grouping of the K sums inside an instruction differs
+            if (h->fp64_shape == 2)
+                hyb::k_update64_f64<2><<<(unsigned)nu, hyb::kUpd64Threads, hyb::kUpd64Smem, st>>>(
+                    ds, slab, p0, p1, mode, sh.la_i0, sh.la_j0, h->d_status, reverse);
+            else if (h->fp64_shape == 1)
+                hyb::k_update64_f64<1><<<(unsigned)nu, hyb::kUpd64Threads, hyb::kUpd64Smem, st>>>(
+                    ds, slab, p0, p1, mode, sh.la_i0, sh.la_j0, h->d_status, reverse);
+            else
+                hyb::k_update64_f64<0><<<(unsigned)nu, hyb::kUpd64Threads, hyb::kUpd64Smem, st>>>(
+                    ds, slab, p0, p1, mode, sh.la_i0, sh.la_j0, h->d_status, reverse);
             ++launches;
             HYB_LAUNCHED("k_update64_f64", l);
             return HYB_SUCCESS;
@@ -1832,6 +1842,7 @@ HYB_API int hyb_system_copy(const hyb_system *src, hyb_system **out)
     h->alternate_walk = src->alternate_walk;
     h->update_kernel = src->update_kernel;
     h->lu_once = src->lu_once;
+    h->fp64_shape = src->fp64_shape;
     std::memcpy(h->tuned, src->tuned, sizeof(h->tuned));
     HYB_CUDA(create_streams(h.get()));
     int rc = upload_symbolic(h.get());
@@ -1932,6 +1943,15 @@ HYB_API int hyb_system_set_option(hyb_system *h, int option, int64_t value)
         if (value != h->krylov_restart)
             h->free_krylov();
         h->krylov_restart = (int)value;
+        return HYB_SUCCESS;
+    case HYB_OPTION_FP64_MMA_SHAPE:
+        if (value < 0 || value > 2)
+            return HYB_INVALID_ARGUMENT;
+        if (h->fp64_shape != (int)value)
+        {
+            h->fp64_shape = (int)value;
+            h->g_factor[0].reset();
+        }
         return HYB_SUCCESS;
     case HYB_OPTION_PIVOT_LU_ONCE:
         if (value < -1 || value > 1)
@@ -2072,7 +2092,9 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
             allow_smem(hyb::k_trsm<float, true>, optin),
             allow_smem(hyb::k_fwd_stage<double, double>, optin),
             allow_smem(hyb::k_fwd_stage<float, float>, optin),
-            allow_smem(hyb::k_update64_f64, hyb::kUpd64Smem),
+            allow_smem(hyb::k_update64_f64<0>, hyb::kUpd64Smem),
+            allow_smem(hyb::k_update64_f64<1>, hyb::kUpd64Smem),
+            allow_smem(hyb::k_update64_f64<2>, hyb::kUpd64Smem),
             allow_smem(hyb::k_lu_trsm64<double, false>, hyb::lu_trsm64_smem<double>()),
             allow_smem(hyb::k_lu_trsm64<float, false>, hyb::lu_trsm64_smem<float>()),
             allow_smem(hyb::k_lu_trsm64<double, true>, hyb::lu_trsm64_smem<double>()),

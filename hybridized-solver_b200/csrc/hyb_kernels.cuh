@@ -1268,6 +1268,29 @@ __device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, dou
                  : "d"(a), "d"(b));
 }
 
+// The larger FP64 shapes (sm_90 and later): D(16x8) += A(16xK) B(Kx8) for K = 8 and 16.
+// Lane l (g = l / 4, t = l % 4) holds A at rows g and g + 8 and columns t + 4j, B at rows
+// t + 4j and column g, and D at rows g and g + 8, columns 2t and 2t + 1 -- so D's registers
+// are those of two m8n8k4 tiles stacked at rows g and g + 8.
+__device__ __forceinline__ void dmma_16x8x8(double &d0, double &d1, double &d2, double &d3, const double (&a)[4],
+                                            double b0, double b1)
+{
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};"
+                 : "+d"(d0), "+d"(d1), "+d"(d2), "+d"(d3)
+                 : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b0), "d"(b1));
+}
+
+__device__ __forceinline__ void dmma_16x8x16(double &d0, double &d1, double &d2, double &d3, const double (&a)[8],
+                                             const double (&b)[4])
+{
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+                 "{%12,%13,%14,%15}, {%0,%1,%2,%3};"
+                 : "+d"(d0), "+d"(d1), "+d"(d2), "+d"(d3)
+                 : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]),
+                   "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
 constexpr int kLd64 = 68; // padded shared-memory row (doubles): conflict-free fragment reads
 constexpr int kUpd64Threads = 256;
 constexpr int kUpd64Smem = 2 * 64 * kLd64 * 8 + 16;
@@ -1279,6 +1302,8 @@ constexpr int kUpd64Smem = 2 * 64 * kLd64 * 8 + 16;
 // (24 per SM at 3 CTAs) hide the shared-memory operand latency better than four (7% less
 // FP64 factorization time at 96x96) and better than sixteen (smaller tiles, more loads
 // per DMMA). Work units as in k_update.
+// kShape: 0 m8n8k4, 1 m16n8k8, 2 m16n8k16 (FP64 MMA instruction shape; same tiling).
+template <int kShape>
 __global__ void __launch_bounds__(kUpd64Threads)
     k_update64_f64(DevSym S, double *__restrict__ slab, int64_t p0, int64_t p1, int mode, int i0, int j0,
                    int *status, int reverse)
@@ -1346,21 +1371,52 @@ __global__ void __launch_bounds__(kUpd64Threads)
         }
         return;
     }
-#pragma unroll
-    for (int kk = 0; kk < 64; kk += 4)
+    if constexpr (kShape == 0)
     {
-        double av[2], bv[4];
 #pragma unroll
-        for (int mi = 0; mi < 2; ++mi)
-            av[mi] = -sa[(wm + mi * 8 + g) * kLd64 + kk + q];
+        for (int kk = 0; kk < 64; kk += 4)
+        {
+            double av[2], bv[4];
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni)
-            bv[ni] = sb[(kk + q) * kLd64 + wn + ni * 8 + g];
-#pragma unroll
-        for (int mi = 0; mi < 2; ++mi)
+            for (int mi = 0; mi < 2; ++mi)
+                av[mi] = -sa[(wm + mi * 8 + g) * kLd64 + kk + q];
 #pragma unroll
             for (int ni = 0; ni < 4; ++ni)
-                dmma_8x8x4(acc[mi][ni][0], acc[mi][ni][1], av[mi], bv[ni]);
+                bv[ni] = sb[(kk + q) * kLd64 + wn + ni * 8 + g];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+                    dmma_8x8x4(acc[mi][ni][0], acc[mi][ni][1], av[mi], bv[ni]);
+        }
+    }
+    else
+    {
+        constexpr int KS = kShape == 1 ? 8 : 16; // k per instruction
+#pragma unroll
+        for (int kk = 0; kk < 64; kk += KS)
+        {
+            double av[KS / 2], bv[4][KS / 4];
+#pragma unroll
+            for (int j = 0; j < KS / 4; ++j)
+            {
+                av[2 * j] = -sa[(wm + g) * kLd64 + kk + 4 * j + q];
+                av[2 * j + 1] = -sa[(wm + 8 + g) * kLd64 + kk + 4 * j + q];
+            }
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int j = 0; j < KS / 4; ++j)
+                    bv[ni][j] = sb[(kk + 4 * j + q) * kLd64 + wn + ni * 8 + g];
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+            {
+                if constexpr (kShape == 1)
+                    dmma_16x8x8(acc[0][ni][0], acc[0][ni][1], acc[1][ni][0], acc[1][ni][1], av, bv[ni][0], bv[ni][1]);
+                else
+                    dmma_16x8x16(acc[0][ni][0], acc[0][ni][1], acc[1][ni][0], acc[1][ni][1], av, bv[ni]);
+            }
+        }
     }
 #pragma unroll
     for (int mi = 0; mi < 2; ++mi)

@@ -39,6 +39,7 @@ OPTION_BLOCK_SCALING = 9
 OPTION_ALTERNATE_WALK = 10
 OPTION_UPDATE_KERNEL = 11  # -1 tuned, 0 32x32 SIMT, 1 64x64 SIMT, 2 DMMA
 OPTION_PIVOT_LU_ONCE = 12
+OPTION_FP64_MMA_SHAPE = 13
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _i64p = ctypes.POINTER(ctypes.c_int64)

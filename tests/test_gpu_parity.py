@@ -450,3 +450,18 @@ def test_generic_update_kernels_match_oracle(gpu, kind):
     ns.decompose(gpu.MIXED)
     xm, im = ns.solve(bn)
     assert im["converged"] and rel_err(xm, xo) < TOL_X_MIXED
+
+
+@pytest.mark.parametrize("shape", [0, 1, 2])
+def test_fp64_update_mma_shapes_match_oracle(gpu, shape):
+    """The FP64 64-block update with each FP64 MMA instruction shape (m8n8k4, m16n8k8,
+    m16n8k16) gives the oracle's factors within 1e-12 per block."""
+    mat, b = _mesh(8, 8, seed=27)
+    order, pm, ns = _native_from(gpu, mat)
+    ns.set_option(gpu.OPTION_FP64_MMA_SHAPE, shape)
+    osys = O.OracleSystem.from_csr(pm.sizes, pm.row_ptr, pm.cols, pm.vals)
+    osys.decompose()
+    ns.decompose(gpu.FP64)
+    _check_factors(ns, osys, pm)
+    bn = reorder_rhs(mat.sizes, order, b)
+    assert rel_err(ns.solve(bn)[0], osys.solve(bn)) < TOL_X
