@@ -220,8 +220,8 @@ typedef enum
      * mixed form (its FP32 LU is cheap and the extra launch lengthens the pivot chain). All
      * give the same factors. */
     HYB_OPTION_PIVOT_LU_ONCE = 12,
-    /* FP64 MMA instruction shape of the FP64 form's 64-block Schur update: 0 (default)
-     * m8n8k4, 1 m16n8k8, 2 m16n8k16. The same products, summed in different groups inside
+    /* FP64 MMA instruction shape of the FP64 form's 64-block Schur update: 0 m8n8k4,
+     * 1 (default) m16n8k8, 2 m16n8k16. The same products, summed in different groups inside
      * an instruction (FP64 factors agree to rounding). */
     HYB_OPTION_FP64_MMA_SHAPE = 13
 } hyb_option;
