@@ -788,12 +788,13 @@ def run_ours(args):
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps)
 
     def roofline(prof, bound, peak, unit, elem_bytes, peak_note, step_ms, kernel, traffic_per_block=None):
-        """One level's Schur update (both lookahead launches, timed with events on the
-        handle's stream, every profile-stride-th level of the timed steps) against its bound;
-        algorithmic work per level from the pattern: 2 m k n flops per target block, and the
+        """One update pass -- one level, or in the mixed form a pair of levels applied in one
+        two-pivot pass -- (both lookahead launches, timed with events on the handle's stream,
+        every profile-stride-th pass of the timed steps) against its bound; algorithmic work
+        per pass from the pattern: 2 m k n flops per target block and source pivot, and the
         FP32/FP64 bytes of reading and writing every target once plus reading the
         lower-column and upper-row operands once. The share of the step scales the sampled
-        mean to every level with an update."""
+        mean to every pass with an update."""
         if prof is None:
             return None
         avg_ms = prof.total_ms / prof.launches
@@ -814,9 +815,13 @@ def run_ours(args):
             "traffic": traffic,
             "kernel": kernel,
             "avg_launch_ms": avg_ms,
-            "share_of_step": avg_ms * prof.levels / step_ms,
-            "levels_timed": prof.launches,
+            "share_of_step": avg_ms * prof.passes / step_ms,
+            "passes_timed": prof.launches,
+            "passes_with_update": prof.passes,
             "levels_with_update": prof.levels,
+            "pivots_per_pass": prof.pivots_timed / prof.launches,
+            "ms_per_pivot": avg_ms * prof.launches / prof.pivots_timed,
+            "pivot_work_ms_per_pivot": (prof.pivot_ms / prof.pivot_levels) if prof.pivot_levels else None,
             "peak_source": peak_note,
             "algorithmic_per_launch": per_launch,
             "algorithmic_unit": "flop" if bound == "tensor" else "byte",
@@ -835,6 +840,11 @@ def run_ours(args):
         "k_update64_tc (tcgen05 split-BF16, persistent, bulk-copy C ring)",
         traffic_per_block=TC_DRAM_BYTES_PER_TARGET_BLOCK,
     )
+    if rmix is not None and rmix["pivots_per_pass"] > 1.5:
+        rmix["kernel"] = (
+            "k_update64_tc2 (tcgen05 split-BF16, two pivots per pass: K = 128, targets staged in registers, "
+            "persistent)"
+        )
     if rf64 is not None:
         rf64["traffic_note"] = (
             "null: the FP64 update's DRAM bytes were captured only at 32x32 (profiles/k_update64_f64_mesh32_p8.md), "

@@ -4,6 +4,7 @@
 #include "hyb_internal.h"
 #include "hyb_kernels.cuh"
 #include "hyb_krylov.cuh"
+#include "hyb_pivot.cuh"
 #include "hyb_umma.cuh"
 
 #include "hybsol_b200.h"
@@ -157,7 +158,8 @@ struct hyb_system
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr; // lookahead pivots (joined into `stream` inside graphs)
-    cudaEvent_t ev_prio = nullptr, ev_piv = nullptr, ev_join = nullptr;
+    cudaStream_t stream3 = nullptr; // operand splits beside a pivot launch (forked and joined per level)
+    cudaEvent_t ev_prio = nullptr, ev_piv = nullptr, ev_join = nullptr, ev_fork3 = nullptr, ev_join3 = nullptr;
     bool lookahead = true;
     bool umma = true; // mixed-form updates of 64-blocks on the tcgen05 tensor cores
     bool flow = true; // dataflow substitution (enqueue_solve_flow) in hyb_solve
@@ -169,6 +171,8 @@ struct hyb_system
     float growth_limit = 1024.0f;         // HYB_OPTION_GROWTH_LIMIT (mixed form)
     bool block_scaling = true;            // HYB_OPTION_BLOCK_SCALING (mixed form)
     bool alternate_walk = true;           // HYB_OPTION_ALTERNATE_WALK
+    bool pair_passes = false;             // HYB_OPTION_PAIR_PASSES (mixed form)
+    int row_pivots = -1;                  // HYB_OPTION_ROW_PIVOTS: -1 per precision (mixed 2, FP64 0)
     // generic-size Schur updates: HYB_OPTION_UPDATE_KERNEL (-1: tuned per size bucket), and
     // the tuned choice per precision and bucket (-1: not tuned yet)
     int update_kernel = -1;
@@ -220,10 +224,11 @@ struct hyb_system
     double *d_f64 = nullptr;
     float *d_f32 = nullptr;
     float *d_dinv = nullptr; // FP32 inverses of the 64-row diagonal blocks (mixed form), n_inv x 4096
-    // BF16 operand splits of tensor-core levels, two level-parity halves of split_half bytes
+    // BF16 operand splits of tensor-core levels, a ring of level slots of split_half bytes
+    // each, then one all-zero split block
     unsigned char *d_ops = nullptr;
     size_t split_half = 0;
-    // target-block offsets of tensor-core levels, two level-parity halves of tgt_half entries
+    // target-block offsets of tensor-core levels, a ring of level slots of tgt_half entries
     int64_t *d_tgt = nullptr;
     size_t tgt_half = 0;
     // solve buffers, sized for buf_nrhs right-hand sides
@@ -254,8 +259,14 @@ struct hyb_system
     // that has an update (0: off)
     int profile = 0;
     std::vector<cudaEvent_t> prof_ev;
-    std::vector<int64_t> prof_levels; // level of each event pair
-    int64_t prof_update_levels = 0;   // levels with an update in the captured schedule
+    std::vector<int64_t> prof_levels; // first level of the unit of each event pair
+    std::vector<uint8_t> prof_pair;   // whether that unit is a two-pivot pass
+    int64_t prof_update_levels = 0;   // update passes in the captured schedule (a pair counts once)
+    int64_t prof_update_pivots = 0;   // levels with an update in the captured schedule
+    // the same for the pivot work of every profile-th unit (on whichever stream runs it)
+    std::vector<cudaEvent_t> prof_piv_ev;
+    std::vector<uint8_t> prof_piv_levels; // levels of each timed unit
+    int64_t prof_piv_units = 0;
     int prof_precision = -1;
 
     ~hyb_system()
@@ -292,9 +303,11 @@ struct hyb_system
         cudaFree(d_tscr);
         cudaFree(d_colsum);
         free_solve_buffers();
-        for (cudaEvent_t e : {ev_prio, ev_piv, ev_join})
+        for (cudaEvent_t e : {ev_prio, ev_piv, ev_join, ev_fork3, ev_join3})
             if (e)
                 cudaEventDestroy(e);
+        if (stream3)
+            cudaStreamDestroy(stream3);
         if (stream2)
             cudaStreamDestroy(stream2);
         if (stream)
@@ -307,7 +320,14 @@ struct hyb_system
             cudaEventDestroy(e);
         prof_ev.clear();
         prof_levels.clear();
+        prof_pair.clear();
         prof_update_levels = 0;
+        prof_update_pivots = 0;
+        for (cudaEvent_t e : prof_piv_ev)
+            cudaEventDestroy(e);
+        prof_piv_ev.clear();
+        prof_piv_levels.clear();
+        prof_piv_units = 0;
     }
 
     void free_krylov()
@@ -346,7 +366,9 @@ cudaError_t create_streams(hyb_system *h)
         e = cudaStreamCreateWithPriority(&h->stream, cudaStreamNonBlocking, lo);
     if (e == cudaSuccess)
         e = cudaStreamCreateWithPriority(&h->stream2, cudaStreamNonBlocking, hi);
-    for (cudaEvent_t *ev : {&h->ev_prio, &h->ev_piv, &h->ev_join})
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithPriority(&h->stream3, cudaStreamNonBlocking, hi);
+    for (cudaEvent_t *ev : {&h->ev_prio, &h->ev_piv, &h->ev_join, &h->ev_fork3, &h->ev_join3})
         if (e == cudaSuccess)
             e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
     return e;
@@ -401,6 +423,7 @@ int upload_symbolic(hyb_system *h)
         {S.a_cols.data(), S.a_cols.size() * 4, (const void **)&d.a_cols},
         {S.a_val_off.data(), S.a_val_off.size() * 8, (const void **)&d.a_val_off},
         {S.a_to_f.data(), S.a_to_f.size() * 4, (const void **)&d.a_to_f},
+        {S.pair_map.data(), S.pair_map.size() * 4, (const void **)&d.pair_map},
     };
     size_t total = 0;
     for (const Item &it : items)
@@ -446,14 +469,24 @@ template <typename T> bool tc_level(const hyb_system *h, int64_t l)
            h->S.shape[l].uniform64;
 }
 
+// Operand splits and target tables live in a ring of kOpsSlots level slots: a two-pivot pass
+// reads the slots of its two levels while the next pair's pivots write the next two.
+constexpr int kOpsSlots = 4;
+
 unsigned char *level_ops(hyb_system *h, int64_t l)
 {
-    return h->d_ops + (size_t)(l & 1) * h->split_half;
+    return h->d_ops + (size_t)(l % kOpsSlots) * h->split_half;
 }
 
 int64_t *level_tgt(hyb_system *h, int64_t l)
 {
-    return h->d_tgt + (size_t)(l & 1) * h->tgt_half;
+    return h->d_tgt + (size_t)(l % kOpsSlots) * h->tgt_half;
+}
+
+// One all-zero BF16 split block after the ring (a column a pair's first pivot does not reach).
+const unsigned char *zero_split(const hyb_system *h)
+{
+    return h->d_ops + (size_t)kOpsSlots * h->split_half;
 }
 
 // BF16 split of a tensor-core level's operands, once its pivots are factored.
@@ -469,7 +502,7 @@ template <typename T> int enqueue_split(hyb_system *h, T *slab, int64_t l, cudaS
         if (blocks > 0)
         {
             hyb::k_split64<<<(unsigned)blocks, hyb::kSplitThreads, 0, st>>>(h->ds, slab, level_ops(h, l),
-                                                                           level_tgt(h, l), p0, p1);
+                                                                           level_tgt(h, l), p0, p1, 0);
             ++launches;
             HYB_LAUNCHED("k_split64", l);
         }
@@ -492,6 +525,79 @@ template <typename T> int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cuda
     const Symbolic::LevelShape &sh = S.shape[l];
     // growth check and FP64 fallback of the mixed form (0: off, and always for FP64 factors)
     const float glim = std::is_same_v<T, float> && h->d_hg ? h->growth_limit : 0.0f;
+    // 64-row pivots (HYB_OPTION_ROW_PIVOTS): the mixed form by default factors each pivot
+    // once and takes its upper blocks as products with the inverse (2); 1 is the blocked
+    // substitution kernel (bit-identical to the 256-thread kernels); the FP64 form keeps the
+    // 256-thread kernels by default, since the blocked kernel's 115 KB of FP64 shared
+    // memory displaces update CTAs (measured at 96x96 p=8: 2,229 against 2,138 ms)
+    const int mode64 = h->row_pivots < 0 ? (std::is_same_v<T, float> ? 2 : 0) : h->row_pivots;
+    if constexpr (std::is_same_v<T, float>)
+    {
+        if (fused_pivots(sh) && sh.piv64 && mode64 == 2 && tc_level<T>(h, l) && h->d_dinv)
+        {
+            const int64_t n_split = S.split_pref[p1] - S.split_pref[p0];
+            const int64_t n_trsm = S.trsm_pref[p1] - S.trsm_pref[p0];
+            double *inv64 = h->d_piv64f + (l & 1) * h->fused_half * 4096;
+            HYB_CUDA(cudaEventRecord(h->ev_fork3, st));
+            HYB_CUDA(cudaStreamWaitEvent(h->stream3, h->ev_fork3, 0));
+            if (n_split > 0) // the lower blocks' splits beside the pivot work
+            {
+                hyb::k_split64<<<(unsigned)n_split, hyb::kSplitThreads, 0, h->stream3>>>(
+                    ds, slab, level_ops(h, l), level_tgt(h, l), p0, p1, 1);
+                ++launches;
+                HYB_LAUNCHED("k_split64", l);
+            }
+            HYB_CUDA(cudaEventRecord(h->ev_join3, h->stream3));
+            hyb::k_piv64_inv<<<(unsigned)(p1 - p0), hyb::kPivThreads, hyb::kInvSmem, st>>>(
+                ds, slab, p0, h->d_status, glim, h->d_dinv, inv64, h->d_hg);
+            ++launches;
+            HYB_LAUNCHED("k_piv64_inv", l);
+            if (n_trsm > 0)
+            {
+                hyb::k_strips64_inv<<<(unsigned)n_trsm, hyb::kPivThreads, 0, st>>>(
+                    ds, slab, p0, p1, h->d_dinv, inv64, glim > 0 ? h->d_hg : nullptr, level_ops(h, l));
+                ++launches;
+                HYB_LAUNCHED("k_strips64_inv", l);
+            }
+            HYB_CUDA(cudaStreamWaitEvent(st, h->ev_join3, 0));
+            return HYB_SUCCESS;
+        }
+    }
+    if (fused_pivots(sh) && sh.piv64 && mode64 >= 1)
+    {
+        // blocked LU and row solves per upper block; on a tensor-core level the lower-column
+        // splits run beside it on a third stream and the upper blocks' splits are written by
+        // the row solves
+        const int64_t n_lu = S.lu_pref[p1] - S.lu_pref[p0];
+        if (tc_level<T>(h, l))
+        {
+            if constexpr (std::is_same_v<T, float>)
+            {
+                const int64_t n_split = S.split_pref[p1] - S.split_pref[p0];
+                HYB_CUDA(cudaEventRecord(h->ev_fork3, st));
+                HYB_CUDA(cudaStreamWaitEvent(h->stream3, h->ev_fork3, 0));
+                if (n_split > 0) // the last pivots have no lower or upper blocks
+                {
+                    hyb::k_split64<<<(unsigned)n_split, hyb::kSplitThreads, 0, h->stream3>>>(
+                        ds, slab, level_ops(h, l), level_tgt(h, l), p0, p1, 1);
+                    ++launches;
+                    HYB_LAUNCHED("k_split64", l);
+                }
+                HYB_CUDA(cudaEventRecord(h->ev_join3, h->stream3));
+                hyb::k_piv64<float, true><<<(unsigned)n_lu, hyb::kPivThreads, hyb::piv64_smem<float>(), st>>>(
+                    ds, slab, p0, p1, h->d_lu_tickets, h->d_status, glim, level_ops(h, l));
+                ++launches;
+                HYB_LAUNCHED("k_piv64", l);
+                HYB_CUDA(cudaStreamWaitEvent(st, h->ev_join3, 0));
+                return HYB_SUCCESS;
+            }
+        }
+        hyb::k_piv64<T, false><<<(unsigned)n_lu, hyb::kPivThreads, hyb::piv64_smem<T>(), st>>>(
+            ds, slab, p0, p1, h->d_lu_tickets, h->d_status, glim, nullptr);
+        ++launches;
+        HYB_LAUNCHED("k_piv64", l);
+        return HYB_SUCCESS;
+    }
     if (fused_pivots(sh))
     {
         // fused: diagonal LU (padded to 64x64) and the solves of the pivot rows' upper blocks;
@@ -566,6 +672,25 @@ template <typename T> int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cuda
     return enqueue_split<T>(h, slab, l, st, launches);
 }
 
+// Whether the pivot work of every level with 64-row pivots already wrote their FP32
+// inverses (the mixed form's inverse-and-products path, HYB_OPTION_ROW_PIVOTS 2).
+template <typename T> bool inverses_by_pivots(const hyb_system *h)
+{
+    const Symbolic &S = h->S;
+    const int mode64 = h->row_pivots < 0 ? (std::is_same_v<T, float> ? 2 : 0) : h->row_pivots;
+    if (!std::is_same_v<T, float> || mode64 != 2)
+        return false;
+    for (int64_t l = 0; l < S.n_levels; ++l)
+    {
+        bool has64 = false;
+        for (int64_t p = S.lvl_ptr[l]; p < S.lvl_ptr[l + 1] && !has64; ++p)
+            has64 = S.size[S.piv[p]] == 64;
+        if (has64 && !(fused_pivots(S.shape[l]) && S.shape[l].piv64 && tc_level<T>(h, l)))
+            return false;
+    }
+    return true;
+}
+
 // FP32 inverses of every 64-row diagonal block (mixed form), in one launch after the last
 // level. Only the solves read them; launched beside the stages instead, they slowed the
 // update CTAs that shared their SMs, and each level waits for its slowest update CTA.
@@ -573,7 +698,7 @@ template <typename T> int enqueue_inverses(hyb_system *h, T *slab, uint64_t &lau
 {
     if constexpr (std::is_same_v<T, float>)
     {
-        if (!h->d_dinv || h->S.n_inv == 0)
+        if (!h->d_dinv || h->S.n_inv == 0 || inverses_by_pivots<T>(h))
             return HYB_SUCCESS;
         hyb::k_diag_inv64<float>
             <<<(unsigned)h->S.n_inv, hyb::kInvThreads, 0, h->stream>>>(h->ds, slab, h->d_dinv);
@@ -801,10 +926,59 @@ template <typename T> int enqueue_update(hyb_system *h, T *slab, int64_t l, cuda
     return enqueue_generic_update<T>(h, slab, l, st, mode, nu, generic_kernel<T>(h, l), launches);
 }
 
-// Issues the whole factorization (used under graph capture). Levels run in order on the
-// handle's stream; where a level and the next each have one pivot, the next pivot's LU
-// and row solves run on the second stream as soon as the update of its own row and
-// column is done, overlapping the rest of this level's update (lookahead).
+// Whether level l starts a two-pivot pass in T's factorization: the mixed form on the
+// tensor cores, a pair of the symbolic phase (Symbolic::PairShape), option on.
+template <typename T> bool pair_unit(const hyb_system *h, int64_t l)
+{
+    return std::is_same_v<T, float> && h->pair_passes && l + 1 < h->S.n_levels && h->S.pair_first[l] &&
+           tc_level<T>(h, l) && tc_level<T>(h, l + 1);
+}
+
+// The pivot work of the unit that starts at level l. A single level: its LU, row solves and
+// split. A pair (a, b): a's, then a's update of b's row and column -- a few hundred target
+// blocks in FP32 on the CUDA cores, in CTAs small enough to run beside a tensor-core pass --
+// then b's.
+template <typename T> int enqueue_unit_pivots(hyb_system *h, T *slab, int64_t l, cudaStream_t st, uint64_t &launches)
+{
+    int rc = enqueue_pivots<T>(h, slab, l, st, launches);
+    if (rc != HYB_SUCCESS || !pair_unit<T>(h, l))
+        return rc;
+    const Symbolic::LevelShape &sh = h->S.shape[l];
+    if ((rc = enqueue_generic_update<T>(h, slab, l, st, 1, sh.la_prio_units, UPD_TILE32, launches)) != HYB_SUCCESS)
+        return rc;
+    return enqueue_pivots<T>(h, slab, l + 1, st, launches);
+}
+
+// The two-pivot pass of the pair that starts at level l: mode 0 every target of b, 1 / 2 the
+// lookahead split (the next unit's rows and columns first).
+template <typename T> int enqueue_pair_update(hyb_system *h, T *slab, int64_t l, cudaStream_t st, int mode,
+                                              uint64_t &launches)
+{
+    if constexpr (std::is_same_v<T, float>)
+    {
+        const Symbolic &S = h->S;
+        const Symbolic::PairShape &ps = S.pair[l];
+        const int64_t tiles = mode == 0 ? ps.all_tiles : (mode == 1 ? ps.prio_tiles : ps.rest_tiles);
+        if (tiles <= 0)
+            return HYB_SUCCESS;
+        const int4 pr = make_int4(ps.i0, ps.i1, ps.j0, ps.j1);
+        // alternate passes walk their targets backwards (the priority launch keeps its order)
+        const int reverse = h->alternate_walk && mode != 1 && ((l >> 1) & 1) ? 1 : 0;
+        const unsigned grid = (unsigned)std::min<int64_t>(tiles, (int64_t)sm_count());
+        hyb::k_update64_tc2<<<grid, hyb::kTc2Threads, hyb::kTc2Smem, st>>>(
+            h->ds, slab, level_ops(h, l), level_ops(h, l + 1), level_tgt(h, l + 1), zero_split(h), S.lvl_ptr[l],
+            S.lvl_ptr[l + 1], mode, pr, tiles, h->d_status, reverse);
+        ++launches;
+        HYB_LAUNCHED("k_update64_tc2", l);
+    }
+    return HYB_SUCCESS;
+}
+
+// Issues the whole factorization (used under graph capture). Units -- one level, or a pair
+// of levels applied in one two-pivot pass -- run in order on the handle's stream; where a
+// unit and the next are single pivots (or pairs of them), the next unit's pivot work runs
+// on the second stream as soon as the update of its rows and columns is done, overlapping
+// the rest of this unit's update (lookahead).
 template <typename T> int enqueue_factor(hyb_system *h, T *slab, uint64_t &launches)
 {
     const Symbolic &S = h->S;
@@ -817,19 +991,43 @@ template <typename T> int enqueue_factor(hyb_system *h, T *slab, uint64_t &launc
         HYB_CUDA(cudaMemsetAsync(h->d_hg, 0, S.n * sizeof(int), st));
     int rc = HYB_SUCCESS;
     bool next_pivots_issued = false, forked = false;
-    for (int64_t l = 0; l < S.n_levels; ++l)
+    int64_t nl = 1;
+    // the pivot work of the unit at level lu on stream s, bracketed by events on every
+    // profile-th unit
+    auto unit_pivots = [&](int64_t lu, cudaStream_t s) -> int {
+        const bool tp = h->profile > 0 && h->prof_piv_units++ % h->profile == 0;
+        if (tp)
+        {
+            cudaEvent_t e0, e1;
+            HYB_CUDA(cudaEventCreate(&e0));
+            HYB_CUDA(cudaEventCreate(&e1));
+            h->prof_piv_ev.push_back(e0);
+            h->prof_piv_ev.push_back(e1);
+            h->prof_piv_levels.push_back(pair_unit<T>(h, lu) ? 2 : 1);
+            HYB_CUDA(cudaEventRecordWithFlags(e0, s, cudaEventRecordExternal));
+        }
+        const int r = enqueue_unit_pivots<T>(h, slab, lu, s, launches);
+        if (r == HYB_SUCCESS && tp)
+            HYB_CUDA(cudaEventRecordWithFlags(h->prof_piv_ev.back(), s, cudaEventRecordExternal));
+        return r;
+    };
+    for (int64_t l = 0; l < S.n_levels; l += nl)
     {
+        const bool pair = pair_unit<T>(h, l);
+        nl = pair ? 2 : 1;
+        const int64_t next = l + nl; // first level of the next unit
         const int64_t p0 = S.lvl_ptr[l], p1 = S.lvl_ptr[l + 1];
         const Symbolic::LevelShape &sh = S.shape[l];
         if (next_pivots_issued)
             HYB_CUDA(cudaStreamWaitEvent(st, h->ev_piv, 0));
-        else if ((rc = enqueue_pivots<T>(h, slab, l, st, launches)) != HYB_SUCCESS)
+        else if ((rc = unit_pivots(l, st)) != HYB_SUCCESS)
             return rc;
         next_pivots_issued = false;
         const bool has_update =
-            S.lvl_listed[l] ? S.mt_lvl_ptr[l + 1] > S.mt_lvl_ptr[l] : S.upd_pref[p1] > S.upd_pref[p0];
+            pair || (S.lvl_listed[l] ? S.mt_lvl_ptr[l + 1] > S.mt_lvl_ptr[l] : S.upd_pref[p1] > S.upd_pref[p0]);
         const bool timed = h->profile > 0 && has_update && h->prof_update_levels % h->profile == 0;
         h->prof_update_levels += has_update ? 1 : 0;
+        h->prof_update_pivots += has_update ? nl : 0;
         if (timed)
         {
             cudaEvent_t e0, e1;
@@ -838,25 +1036,34 @@ template <typename T> int enqueue_factor(hyb_system *h, T *slab, uint64_t &launc
             h->prof_ev.push_back(e0);
             h->prof_ev.push_back(e1);
             h->prof_levels.push_back(l);
+            h->prof_pair.push_back(pair ? 1 : 0);
             // external records become event nodes of the captured graph (a plain record
             // under capture is only a dependency marker and never fires)
             HYB_CUDA(cudaEventRecordWithFlags(e0, st, cudaEventRecordExternal));
         }
-        if (sh.lookahead && h->lookahead)
+        // A single level's lookahead clears only the next pivot's row and column, so it is
+        // not taken when the next unit is a pair (whose pivot work spans two of each).
+        const bool lookahead =
+            h->lookahead && (pair ? S.pair[l].lookahead : sh.lookahead && !pair_unit<T>(h, next));
+        auto update = [&](int mode) {
+            return pair ? enqueue_pair_update<T>(h, slab, l, st, mode, launches)
+                        : enqueue_update<T>(h, slab, l, st, mode, launches);
+        };
+        if (lookahead)
         {
-            if ((rc = enqueue_update<T>(h, slab, l, st, 1, launches)) != HYB_SUCCESS)
+            if ((rc = update(1)) != HYB_SUCCESS)
                 return rc;
             HYB_CUDA(cudaEventRecord(h->ev_prio, st));
             HYB_CUDA(cudaStreamWaitEvent(st2, h->ev_prio, 0));
-            if ((rc = enqueue_pivots<T>(h, slab, l + 1, st2, launches)) != HYB_SUCCESS)
+            if ((rc = unit_pivots(next, st2)) != HYB_SUCCESS)
                 return rc;
             HYB_CUDA(cudaEventRecord(h->ev_piv, st2));
-            if ((rc = enqueue_update<T>(h, slab, l, st, 2, launches)) != HYB_SUCCESS)
+            if ((rc = update(2)) != HYB_SUCCESS)
                 return rc;
             next_pivots_issued = true;
             forked = true;
         }
-        else if ((rc = enqueue_update<T>(h, slab, l, st, 0, launches)) != HYB_SUCCESS)
+        else if ((rc = update(0)) != HYB_SUCCESS)
         {
             return rc;
         }
@@ -1840,6 +2047,8 @@ HYB_API int hyb_system_copy(const hyb_system *src, hyb_system **out)
     h->growth_limit = src->growth_limit;
     h->block_scaling = src->block_scaling;
     h->alternate_walk = src->alternate_walk;
+    h->pair_passes = src->pair_passes;
+    h->row_pivots = src->row_pivots;
     h->update_kernel = src->update_kernel;
     h->lu_once = src->lu_once;
     h->fp64_shape = src->fp64_shape;
@@ -1981,6 +2190,23 @@ HYB_API int hyb_system_set_option(hyb_system *h, int option, int64_t value)
             h->g_factor[1].reset();
         }
         return HYB_SUCCESS;
+    case HYB_OPTION_ROW_PIVOTS:
+        if (value < -1 || value > 2)
+            return HYB_INVALID_ARGUMENT;
+        if (h->row_pivots != (int)value)
+        {
+            h->row_pivots = (int)value;
+            h->g_factor[0].reset();
+            h->g_factor[1].reset();
+        }
+        return HYB_SUCCESS;
+    case HYB_OPTION_PAIR_PASSES:
+        if (h->pair_passes != (value != 0))
+        {
+            h->pair_passes = value != 0;
+            h->g_factor[1].reset();
+        }
+        return HYB_SUCCESS;
     case HYB_OPTION_BLOCK_SCALING:
         h->block_scaling = value != 0;
         return HYB_SUCCESS;
@@ -2100,6 +2326,11 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
             allow_smem(hyb::k_lu_trsm64<double, true>, hyb::lu_trsm64_smem<double>()),
             allow_smem(hyb::k_lu_trsm64<float, true>, hyb::lu_trsm64_smem<float>()),
             allow_smem(hyb::k_update64_tc, hyb::kTcSmem),
+            allow_smem(hyb::k_update64_tc2, hyb::kTc2Smem),
+            allow_smem(hyb::k_piv64<double, false>, hyb::piv64_smem<double>()),
+            allow_smem(hyb::k_piv64<float, false>, hyb::piv64_smem<float>()),
+            allow_smem(hyb::k_piv64<float, true>, hyb::piv64_smem<float>()),
+            allow_smem(hyb::k_piv64_inv, hyb::kInvSmem),
             allow_smem(hyb::k_split64, 0),
             allow_smem(hyb::k_update<double>, 0),
             allow_smem(hyb::k_update<float>, 0),
@@ -2209,8 +2440,9 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
         {
             h->split_half = (size_t)S.max_split_blocks * hyb::kSplitBytes;
             h->tgt_half = (size_t)std::max<int64_t>(1, S.max_tc_targets);
-            HYB_CUDA(cudaMalloc(&h->d_ops, 2 * h->split_half));
-            HYB_CUDA(cudaMalloc(&h->d_tgt, 2 * h->tgt_half * sizeof(int64_t)));
+            HYB_CUDA(cudaMalloc(&h->d_ops, kOpsSlots * h->split_half + hyb::kSplitBytes));
+            HYB_CUDA(cudaMemset(h->d_ops + kOpsSlots * h->split_half, 0, hyb::kSplitBytes));
+            HYB_CUDA(cudaMalloc(&h->d_tgt, kOpsSlots * h->tgt_half * sizeof(int64_t)));
             h->g_factor[1].reset();
         }
         HYB_CUDA(cudaMemsetAsync(h->d_f32, 0, slab * sizeof(float), h->stream));
@@ -2630,14 +2862,40 @@ HYB_API int hyb_profile_read(const hyb_system *h, hyb_kernel_profile *out)
             cudaGetLastError();
             return cuda_fail(e, "cudaEventElapsedTime");
         }
-        const auto &sh = h->S.shape[h->prof_levels[i]];
         out->launches += 1;
         out->total_ms += ms;
-        out->flops += sh.upd_flops;
-        out->c_elems += sh.upd_c_elems;
-        out->ab_elems += sh.upd_ab_elems;
+        if (h->prof_pair[i])
+        {
+            const auto &ps = h->S.pair[h->prof_levels[i]];
+            out->flops += ps.flops;
+            out->c_elems += ps.c_elems;
+            out->ab_elems += ps.ab_elems;
+            out->pivots_timed += 2;
+        }
+        else
+        {
+            const auto &sh = h->S.shape[h->prof_levels[i]];
+            out->flops += sh.upd_flops;
+            out->c_elems += sh.upd_c_elems;
+            out->ab_elems += sh.upd_ab_elems;
+            out->pivots_timed += 1;
+        }
     }
-    out->levels = (uint64_t)h->prof_update_levels;
+    out->levels = (uint64_t)h->prof_update_pivots;
+    out->passes = (uint64_t)h->prof_update_levels;
+    for (size_t i = 0; i < h->prof_piv_levels.size(); ++i)
+    {
+        float ms = 0;
+        const cudaError_t e = cudaEventElapsedTime(&ms, h->prof_piv_ev[2 * i], h->prof_piv_ev[2 * i + 1]);
+        if (e != cudaSuccess)
+        {
+            cudaGetLastError();
+            return cuda_fail(e, "cudaEventElapsedTime");
+        }
+        out->pivot_ms += ms;
+        out->pivot_units += 1;
+        out->pivot_levels += h->prof_piv_levels[i];
+    }
     return HYB_SUCCESS;
 }
 

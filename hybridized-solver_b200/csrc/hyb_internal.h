@@ -104,7 +104,36 @@ struct Symbolic
     };
     std::vector<LevelShape> shape;
 
-    int64_t max_split_blocks = 0;     // max over uniform-64 levels of the split_pref span
+    // Two pivots per update pass (mixed form, tensor-core levels). Levels l and l+1 form a
+    // pair when each has one pivot (a, then b), both are uniform-64 and unlisted, b lies in
+    // a's lower column and upper row, and a's other lower rows and upper columns are among
+    // b's. The pair's targets are then exactly b's (every one receives b's product, and
+    // a's where a reaches it), so one pass over b's targets applies both pivots with
+    // K = 128. a's update of b's own row and column is done first, on the pivot chain.
+    struct PairShape
+    {
+        // lookahead into the next unit (the level after the pair, and the one after that
+        // when those two form a pair too): positions of its pivots c, d in b's lower column
+        // (i0, i1) and upper row (j0, j1), ascending, -1 where absent
+        bool lookahead = false;
+        int32_t i0 = -1, i1 = -1, j0 = -1, j1 = -1;
+        int64_t all_tiles = 0;  // one target row x two columns, every target of b
+        int64_t prio_tiles = 0; // rows i0, i1 x column pairs, then columns (j0, j1) for every other row
+        int64_t rest_tiles = 0; // the other rows x column pairs of the other columns
+        double flops = 0;       // algorithmic flops of the pass (a's products on b's targets and b's)
+        double c_elems = 0;     // target scalars, each read and written once
+        double ab_elems = 0;    // operand scalars of both pivots
+    };
+    std::vector<uint8_t> pair_first; // [L] 1: levels l and l+1 form a pair
+    std::vector<PairShape> pair;     // [L] valid where pair_first
+    // For the second pivot b (slot p) of a pair, at split_pref[p] + i: the index in a's
+    // lower column of b's i-th lower row, and at split_pref[p] + n_lc(b) + j: the index in
+    // a's upper row of b's j-th upper column; -1 where a has no such block (and everywhere
+    // outside pairs).
+    std::vector<int32_t> pair_map;
+    int64_t n_pairs = 0;
+
+    int64_t max_split_blocks = 0;    // max over uniform-64 levels of the split_pref span
     int64_t max_tc_targets = 0;       // max over uniform-64 levels of the upd_pref span (target table)
     int64_t max_fwd_scratch_rows = 0; // max over levels of fwd_rows span
     int64_t max_bwd_scratch_rows = 0;

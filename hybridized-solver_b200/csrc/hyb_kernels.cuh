@@ -59,6 +59,7 @@ struct DevSym
     const int32_t *a_cols;
     const int64_t *a_val_off;
     const int32_t *a_to_f;
+    const int32_t *pair_map; // two-pivot passes: operand indices of a pair's first pivot (Symbolic::pair_map)
 };
 
 // Status words written by the factorization (host reads them after a decompose).

@@ -35,6 +35,119 @@ int64_t find_block(const Symbolic &s, int64_t r, int64_t c)
     return p - s.cols.data();
 }
 
+namespace
+{
+
+using Span = std::pair<const int32_t *, const int32_t *>; // sorted block indices
+
+// Position of v in a sorted span, -1 if absent.
+int32_t span_pos(Span s, int64_t v)
+{
+    const int32_t *q = std::lower_bound(s.first, s.second, (int32_t)v);
+    return (q != s.second && *q == v) ? (int32_t)(q - s.first) : -1;
+}
+
+// Whether every entry of a other than `skip` is in b (both sorted).
+bool span_covered(Span a, Span b, int64_t skip)
+{
+    const int32_t *q = b.first;
+    for (const int32_t *p = a.first; p != a.second; ++p)
+    {
+        if (*p == skip)
+            continue;
+        while (q != b.second && *q < *p)
+            ++q;
+        if (q == b.second || *q != *p)
+            return false;
+    }
+    return true;
+}
+
+// The present ones of two positions, ascending, then -1s.
+void order_pair(int32_t &x, int32_t &y)
+{
+    if (x < 0)
+        std::swap(x, y);
+    if (y >= 0 && y < x)
+        std::swap(x, y);
+}
+
+// Pairs consecutive single-pivot levels for two-pivot tensor-core passes (PairShape), from
+// the first level of each chain on, and records each pair's operand maps, tile counts and
+// lookahead into the next unit.
+void pair_levels(Symbolic &S)
+{
+    const int64_t L = S.n_levels;
+    S.pair_first.assign(L, 0);
+    S.pair.assign(L, {});
+    S.pair_map.assign(S.split_pref[S.n], -1);
+    S.n_pairs = 0;
+    auto single = [&](int64_t l) { return l < L && S.lvl_ptr[l + 1] - S.lvl_ptr[l] == 1; };
+    auto lower = [&](int64_t k) {
+        return Span(S.lcol_row.data() + S.lcol_ptr[k], S.lcol_row.data() + S.lcol_ptr[k + 1]);
+    };
+    auto upper = [&](int64_t k) { return Span(S.cols.data() + S.diag_pos[k] + 1, S.cols.data() + S.row_ptr[k + 1]); };
+    for (int64_t l = 0; l + 1 < L; ++l)
+    {
+        if (!single(l) || !single(l + 1) || S.lvl_listed[l] || S.lvl_listed[l + 1] || !S.shape[l].uniform64 ||
+            !S.shape[l + 1].uniform64)
+            continue;
+        const int64_t pa = S.lvl_ptr[l], pb = S.lvl_ptr[l + 1];
+        const int64_t a = S.piv[pa], b = S.piv[pb];
+        const Span ra = lower(a), ca = upper(a), rb = lower(b), cb = upper(b);
+        if (rb.first == rb.second || cb.first == cb.second || span_pos(ra, b) < 0 || span_pos(ca, b) < 0 ||
+            !span_covered(ra, rb, b) || !span_covered(ca, cb, b))
+            continue;
+        S.pair_first[l] = 1;
+        ++S.n_pairs;
+        const int64_t n_lc = rb.second - rb.first, n_up = cb.second - cb.first;
+        int64_t rows_a = 0, cols_a = 0;
+        for (int64_t i = 0; i < n_lc; ++i)
+        {
+            const int32_t x = span_pos(ra, rb.first[i]);
+            S.pair_map[S.split_pref[pb] + i] = x;
+            rows_a += x >= 0;
+        }
+        for (int64_t j = 0; j < n_up; ++j)
+        {
+            const int32_t x = span_pos(ca, cb.first[j]);
+            S.pair_map[S.split_pref[pb] + n_lc + j] = x;
+            cols_a += x >= 0;
+        }
+        Symbolic::PairShape &ps = S.pair[l];
+        ps.all_tiles = n_lc * ((n_up + 1) / 2);
+        ps.flops = 2.0 * 64 * 64 * 64 * (double)(n_lc * n_up + rows_a * cols_a);
+        ps.c_elems = 4096.0 * (double)(n_lc * n_up);
+        ps.ab_elems = 4096.0 * (double)((ra.second - ra.first) + (ca.second - ca.first) + n_lc + n_up);
+        ++l; // b's level belongs to the pair
+    }
+    for (int64_t l = 0; l + 1 < L; ++l)
+    {
+        if (!S.pair_first[l])
+            continue;
+        Symbolic::PairShape &ps = S.pair[l];
+        const int64_t m = l + 2;
+        if (!single(m))
+            continue;
+        const int64_t b = S.piv[S.lvl_ptr[l + 1]];
+        const Span rb = lower(b), cb = upper(b);
+        const int64_t n_lc = rb.second - rb.first, n_up = cb.second - cb.first;
+        const int64_t c = S.piv[S.lvl_ptr[m]], d = S.pair_first[m] ? S.piv[S.lvl_ptr[m + 1]] : -1;
+        ps.lookahead = true;
+        ps.i0 = span_pos(rb, c);
+        ps.i1 = d >= 0 ? span_pos(rb, d) : -1;
+        ps.j0 = span_pos(cb, c);
+        ps.j1 = d >= 0 ? span_pos(cb, d) : -1;
+        order_pair(ps.i0, ps.i1);
+        order_pair(ps.j0, ps.j1);
+        const int64_t nri = (ps.i0 >= 0) + (ps.i1 >= 0), ncj = (ps.j0 >= 0) + (ps.j1 >= 0);
+        ps.prio_tiles = nri * ((n_up + 1) / 2) + (ncj > 0 ? n_lc - nri : 0);
+        ps.rest_tiles = (n_lc - nri) * ((n_up - ncj + 1) / 2);
+    }
+}
+
+} // namespace
+
 int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, const uint64_t *cols, Symbolic &S,
                    std::string &err)
 {
@@ -425,6 +538,7 @@ int symbolic_build(int64_t n, const uint64_t *sizes, const uint64_t *row_ptr, co
         sh.la_prio_tiles = (i0 >= 0 ? (n_up + 1) / 2 : 0) + (j0 >= 0 ? n_lc - (i0 >= 0) : 0);
         sh.la_rest_tiles = (n_lc - (i0 >= 0)) * ((n_up - (j0 >= 0) + 1) / 2);
     }
+    pair_levels(S);
     return HYB_SUCCESS;
 }
 

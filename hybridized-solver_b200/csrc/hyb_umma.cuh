@@ -98,12 +98,13 @@ __device__ __forceinline__ void split8(const float (&x)[8], uint4 &hi, uint4 &lo
 // stored transposed (rows = its columns n, K = k contiguous). The CTA of lower block i
 // also writes the slab offsets of the targets (t_i, c_j) of its row for every upper
 // column j into `tgt` (per pivot n_lc x n_up, at upd_pref[p] - upd_pref[p0]), so the
-// update kernel finds a tile's C blocks with one load.
+// update kernel finds a tile's C blocks with one load. With lower_only, only the lower
+// blocks (and the target table) are written.
 constexpr int kSplitThreads = 128;
 
 __global__ void __launch_bounds__(kSplitThreads)
     k_split64(DevSym S, const float *__restrict__ slab, unsigned char *__restrict__ ops, int64_t *__restrict__ tgt,
-              int64_t p0, int64_t p1)
+              int64_t p0, int64_t p1, int lower_only)
 {
     __shared__ float tr[64 * 65];
     const int64_t u = S.split_pref[p0] + blockIdx.x;
@@ -138,6 +139,8 @@ __global__ void __launch_bounds__(kSplitThreads)
         }
         return;
     }
+    if (lower_only) // the upper blocks' splits are written by the pivot kernel's row solves
+        return;
     const float *src = slab + S.blk_off[S.diag_pos[k] + 1 + (local - n_lc)];
     for (int i = tid; i < 64 * 16; i += kSplitThreads)
     {
@@ -539,6 +542,406 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
         if (tid == 0)
             asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); // stores complete before exit
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (tid == 0 && s_fail)
+        atomicOr(status + ST_TIMEOUT, 1);
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128));
+}
+
+// ----------------------------------------------------------------------------------
+// Two pivots per pass (a pair of consecutive single-pivot levels, Symbolic::PairShape):
+// C(t,c) -= L(t,a) U(a,c) + L(t,b) U(b,c) over b's targets, with a's product only where a
+// reaches the target. The tile is that of k_update64_tc (one target row t x two upper
+// columns, M = 128, N = 64) with K = 128: a's three BF16 products, then b's, accumulate
+// into one FP32 tensor-memory accumulator, and the target is read and written once for
+// both pivots -- half the target traffic of two single-pivot passes.
+//
+// Shared memory holds both pivots' U pairs (64 KB; a column a does not reach is a zero
+// block) and a four-entry ring of L blocks (one source each); the targets do not pass
+// through shared memory: each epilogue thread loads its 32 values of the next tile into
+// registers while the current tile's products run, and the producer lane prefetches the
+// targets of tiles further ahead into L2. At ~130 KB of shared memory and <= 128 registers
+// per thread the CTA leaves room on its SM for the next pivots' LU / row-solve CTAs.
+constexpr int kTc2Threads = 320;
+constexpr int kTc2LStages = 4;  // L(t, .) ring entries
+constexpr int kTc2Prefetch = 2; // tiles ahead of the producer whose targets go to L2
+constexpr int kTc2Smem = 4 * kSplitBytes + kTc2LStages * kSplitBytes + 256 + 1024;
+
+struct Tc2Tile
+{
+    int32_t row; // index in b's lower column
+    int32_t ja;  // index in b's upper row of the first column block
+    int32_t jb;  // second column block, -1 if the tile has one
+};
+
+// Index x of a sequence with the positions s0 < s1 (-1: absent, present ones first) removed.
+__host__ __device__ __forceinline__ int32_t skip_two(int32_t x, int32_t s0, int32_t s1)
+{
+    if (s0 >= 0 && x >= s0)
+        ++x;
+    if (s1 >= 0 && x >= s1)
+        ++x;
+    return x;
+}
+
+// Tile t of a pair pass. mode 0: every target, column pair major; mode 1: the priority rows
+// pr.x, pr.y x every column pair, then the priority columns (pr.z, pr.w) of every other
+// row in one tile; mode 2: the other rows x pairs of the other columns, column pair major.
+__host__ __device__ __forceinline__ Tc2Tile tc2_tile(int32_t n_lc, int32_t n_up, int mode, int4 pr, int64_t t)
+{
+    Tc2Tile x;
+    if (mode == 0)
+    {
+        const int32_t cp = (int32_t)(t / n_lc);
+        x.row = (int32_t)(t - (int64_t)cp * n_lc);
+        x.ja = 2 * cp;
+        x.jb = x.ja + 1 < n_up ? x.ja + 1 : -1;
+        return x;
+    }
+    const int32_t nri = (pr.x >= 0) + (pr.y >= 0), ncj = (pr.z >= 0) + (pr.w >= 0);
+    if (mode == 1)
+    {
+        const int32_t ncp = (n_up + 1) / 2;
+        const int64_t np = (int64_t)nri * ncp;
+        if (t < np)
+        {
+            const int32_t r = (int32_t)(t / ncp), cp = (int32_t)(t - (int64_t)r * ncp);
+            x.row = r == 0 ? pr.x : pr.y;
+            x.ja = 2 * cp;
+            x.jb = x.ja + 1 < n_up ? x.ja + 1 : -1;
+        }
+        else
+        {
+            x.row = skip_two((int32_t)(t - np), pr.x, pr.y);
+            x.ja = pr.z;
+            x.jb = pr.w;
+        }
+        return x;
+    }
+    const int32_t nr = n_lc - nri, nc = n_up - ncj;
+    const int32_t cp = (int32_t)(t / nr);
+    x.row = skip_two((int32_t)(t - (int64_t)cp * nr), pr.x, pr.y);
+    const int32_t a = 2 * cp, b = a + 1;
+    x.ja = skip_two(a, pr.z, pr.w);
+    x.jb = b < nc ? skip_two(b, pr.z, pr.w) : -1;
+    return x;
+}
+
+__device__ __forceinline__ void tmem_load16(uint32_t addr, uint32_t (&v)[16])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                 "[%16];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                   "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                   "=r"(v[15])
+                 : "r"(addr));
+}
+
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// ops_a / ops_b: the BF16 splits of the levels of a (slot pa) and b (slot pb), each its
+// lower-column blocks then its upper-row blocks; tgt: b's target-offset table (k_split64);
+// zero_split: one all-zero split block. Every wait is bounded; on expiry the CTA sets
+// ST_TIMEOUT, lets its copies and MMAs finish and returns.
+__global__ void __launch_bounds__(kTc2Threads, 1)
+    k_update64_tc2(DevSym S, float *__restrict__ slab, const unsigned char *__restrict__ ops_a,
+                   const unsigned char *__restrict__ ops_b, const int64_t *__restrict__ tgt,
+                   const unsigned char *__restrict__ zero_split, int64_t pa, int64_t pb, int mode, int4 pr,
+                   int64_t n_tiles, int *status, int reverse)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned char *base = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    unsigned char *ua = base;                   // U(a, [ja jb]): hi (ja, jb) then lo (ja, jb)
+    unsigned char *ub = base + 2 * kSplitBytes; // U(b, [ja jb])
+    unsigned char *ring = base + 4 * kSplitBytes;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(ring + kTc2LStages * kSplitBytes);
+    uint64_t *full = bars;                 // [kTc2LStages] L block landed
+    uint64_t *empty = full + kTc2LStages;  // [kTc2LStages] L block consumed by the MMAs
+    uint64_t *ufull = empty + kTc2LStages; // U pairs landed
+    uint64_t *uempty = ufull + 1;          // MMAs on the previous U pairs done
+    uint64_t *tfull = ufull + 2;           // [2] accumulator ready
+    uint64_t *tempty = ufull + 4;          // [2] accumulator drained (one arrival per epilogue warp)
+    uint64_t *done = ufull + 6;            // all MMAs of the CTA done
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(ufull + 7);
+    __shared__ int s_fail;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t ka = S.piv[pa], kb = S.piv[pb];
+    const int32_t n_lc_a = (int32_t)(S.lcol_ptr[ka + 1] - S.lcol_ptr[ka]);
+    const int32_t n_lc = (int32_t)(S.lcol_ptr[kb + 1] - S.lcol_ptr[kb]);
+    const int32_t n_up = (int32_t)(S.row_ptr[kb + 1] - S.diag_pos[kb] - 1);
+    const int32_t *rmap = S.pair_map + S.split_pref[pb]; // b's lower row i -> a's, or -1
+    const int32_t *cmap = rmap + n_lc;                    // b's upper column j -> a's, or -1
+    const int64_t t0 = n_tiles * blockIdx.x / gridDim.x, t1 = n_tiles * (blockIdx.x + 1) / gridDim.x;
+    auto tix = [&](int64_t t) { return reverse ? t0 + t1 - 1 - t : t; };
+    auto tile = [&](int64_t t) { return tc2_tile(n_lc, n_up, mode, pr, tix(t)); };
+    // whether a reaches any column of a tile's pair, and a given row
+    auto a_cols = [&](const Tc2Tile &x) { return cmap[x.ja] >= 0 || (x.jb >= 0 && cmap[x.jb] >= 0); };
+    if (tid == 0)
+    {
+        for (int i = 0; i < kTc2LStages; ++i)
+        {
+            mbar_init(full + i, 1);
+            mbar_init(empty + i, 1);
+        }
+        mbar_init(ufull, 1);
+        mbar_init(uempty, 1);
+        mbar_init(tfull, 1);
+        mbar_init(tfull + 1, 1);
+        mbar_init(tempty, kTcEpiWarps);
+        mbar_init(tempty + 1, kTcEpiWarps);
+        mbar_init(done, 1);
+        s_fail = schedule_aborted(status);
+    }
+    if (warp == 0)
+    {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(128));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const bool run = s_fail == 0; // read by every thread before any role can change it
+    __syncthreads();
+
+    if (!run)
+    {
+    }
+    else if (warp == kTcEpiWarps)
+    {
+        // ---- producer: both U pairs on change, one L block per source and tile, and the
+        // targets of a tile kTc2Prefetch ahead into L2
+        if (lane == 0)
+        {
+            int32_t cur_a = -2, cur_b = -2;
+            bool cols_a = false;
+            uint32_t uloads = 0;
+            int64_t e = 0;
+            bool ok = true;
+            for (int64_t t = t0; t < t1 && ok; ++t)
+            {
+                const Tc2Tile x = tile(t);
+                if (x.ja != cur_a || x.jb != cur_b)
+                {
+                    if (uloads > 0 && !mbar_wait(uempty, (uloads - 1) & 1))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    cols_a = a_cols(x);
+                    const int halves = x.jb >= 0 ? 2 : 1;
+                    mbar_expect_tx(ufull, (uint32_t)(halves * (cols_a ? 2 : 1) * kSplitBytes));
+                    for (int hsel = 0; hsel < halves; ++hsel)
+                    {
+                        const int32_t j = hsel ? x.jb : x.ja;
+                        const unsigned char *sb = ops_b + (int64_t)(n_lc + j) * kSplitBytes;
+                        bulk_g2s(ub + hsel * kSplitHalf, sb, kSplitHalf, ufull);
+                        bulk_g2s(ub + kSplitBytes + hsel * kSplitHalf, sb + kSplitHalf, kSplitHalf, ufull);
+                        if (cols_a)
+                        {
+                            const int32_t ja = cmap[j];
+                            const unsigned char *sa =
+                                ja >= 0 ? ops_a + (int64_t)(n_lc_a + ja) * kSplitBytes : zero_split;
+                            bulk_g2s(ua + hsel * kSplitHalf, sa, kSplitHalf, ufull);
+                            bulk_g2s(ua + kSplitBytes + hsel * kSplitHalf, sa + kSplitHalf, kSplitHalf, ufull);
+                        }
+                    }
+                    ++uloads;
+                    cur_a = x.ja;
+                    cur_b = x.jb;
+                }
+                const int32_t ra = cols_a ? rmap[x.row] : -1;
+                for (int src = ra >= 0 ? 0 : 1; src < 2; ++src)
+                {
+                    const int s = (int)(e % kTc2LStages);
+                    if (e >= kTc2LStages && !mbar_wait(empty + s, (uint32_t)((e / kTc2LStages - 1) & 1)))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    mbar_expect_tx(full + s, kSplitBytes);
+                    const unsigned char *sl =
+                        src == 0 ? ops_a + (int64_t)ra * kSplitBytes : ops_b + (int64_t)x.row * kSplitBytes;
+                    bulk_g2s(ring + s * kSplitBytes, sl, kSplitBytes, full + s);
+                    ++e;
+                }
+                if (ok && t + kTc2Prefetch < t1)
+                {
+                    const Tc2Tile y = tile(t + kTc2Prefetch);
+                    const int64_t *row_tgt = tgt + (int64_t)y.row * n_up;
+                    prefetch_l2(slab + row_tgt[y.ja], 16384);
+                    if (y.jb >= 0)
+                        prefetch_l2(slab + row_tgt[y.jb], 16384);
+                }
+            }
+            if (!ok)
+                s_fail = 1;
+            // drain: every copy issued lands before the CTA can leave
+            for (int64_t j = e > kTc2LStages ? e - kTc2LStages : 0; j < e; ++j)
+                if (!mbar_wait(full + (j % kTc2LStages), (uint32_t)((j / kTc2LStages) & 1)))
+                    s_fail = 1;
+            if (uloads > 0 && !mbar_wait(ufull, (uloads - 1) & 1))
+                s_fail = 1;
+        }
+    }
+    else if (warp == kTcEpiWarps + 1)
+    {
+        // ---- MMA issuer: per tile a's products (where a reaches it), then b's
+        if (lane == 0)
+        {
+            constexpr uint32_t idesc = umma_idesc_bf16(128, 64);
+            int32_t cur_a = -2, cur_b = -2;
+            bool cols_a = false;
+            uint32_t uloads = 0;
+            int64_t e = 0, i = 0;
+            bool ok = true;
+            for (int64_t t = t0; t < t1 && ok; ++t, ++i)
+            {
+                const Tc2Tile x = tile(t);
+                if (x.ja != cur_a || x.jb != cur_b)
+                {
+                    if (uloads > 0)
+                        umma_commit(uempty);
+                    if (!mbar_wait(ufull, uloads & 1))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    ++uloads;
+                    cols_a = a_cols(x);
+                    cur_a = x.ja;
+                    cur_b = x.jb;
+                }
+                const int acc_i = (int)(i & 1);
+                if (i >= 2 && !mbar_wait(tempty + acc_i, (uint32_t)(((i >> 1) - 1) & 1)))
+                {
+                    ok = false;
+                    break;
+                }
+                const uint32_t acc = tmem + (uint32_t)(acc_i * 64);
+                const bool use_a = cols_a && rmap[x.row] >= 0;
+                for (int src = use_a ? 0 : 1; src < 2; ++src)
+                {
+                    const int s = (int)(e % kTc2LStages);
+                    if (!mbar_wait(full + s, (uint32_t)((e / kTc2LStages) & 1)))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t uh = smem_u32(src == 0 ? ua : ub);
+                    const uint64_t duh = umma_smem_desc(uh), dul = umma_smem_desc(uh + kSplitBytes);
+                    const uint32_t lh = smem_u32(ring + s * kSplitBytes);
+                    const uint64_t dlh = umma_smem_desc(lh), dll = umma_smem_desc(lh + kSplitHalf);
+                    const bool first = src == (use_a ? 0 : 1);
+#pragma unroll
+                    for (int ks = 0; ks < 4; ++ks)
+                    {
+                        const uint64_t off = (uint64_t)((ks * 32) >> 4); // 16 BF16 = 32 bytes along K
+                        umma_bf16(acc, duh + off, dlh + off, idesc, (first && ks == 0) ? 0u : 1u);
+                        umma_bf16(acc, duh + off, dll + off, idesc, 1);
+                        umma_bf16(acc, dul + off, dlh + off, idesc, 1);
+                    }
+                    umma_commit(empty + s);
+                    ++e;
+                }
+                if (ok)
+                    umma_commit(tfull + acc_i);
+            }
+            if (!ok)
+                s_fail = 1;
+            umma_commit(done);
+            if (!mbar_wait(done, 0))
+                s_fail = 1;
+        }
+    }
+    else
+    {
+        // ---- epilogue warps 0-7: lane i of warp w is column (w & 1) * 32 + i of block
+        // ((w & 3) < 2 ? ja : jb), rows 32 (w >> 2) .. + 31 of the tile. The target values of
+        // the next tile are loaded into registers before this tile's accumulator is awaited.
+        const int q = warp & 3, h = warp >> 2;
+        const int cb_idx = q >> 1;
+        const int col = (q & 1) * 32 + lane;
+        const int64_t rowoff = (int64_t)(h * 32) * 64 + col;
+        auto target = [&](int64_t t) -> int64_t {
+            const Tc2Tile x = tile(t);
+            const int32_t j = cb_idx ? x.jb : x.ja;
+            return j < 0 ? -1 : tgt[(int64_t)x.row * n_up + j];
+        };
+        float cn[32];
+        int64_t on = t0 < t1 ? target(t0) : -1;
+        if (on >= 0)
+        {
+            const float *src = slab + on + rowoff;
+#pragma unroll
+            for (int r = 0; r < 32; ++r)
+                cn[r] = src[r * 64];
+        }
+        bool failed = false; // warp-uniform
+        int64_t i = 0;
+        for (int64_t t = t0; t < t1; ++t, ++i)
+        {
+            float cc[32];
+#pragma unroll
+            for (int r = 0; r < 32; ++r)
+                cc[r] = cn[r];
+            const int64_t oc = on;
+            on = -1;
+            if (!failed && t + 1 < t1)
+            {
+                on = target(t + 1);
+                if (on >= 0)
+                {
+                    const float *src = slab + on + rowoff;
+#pragma unroll
+                    for (int r = 0; r < 32; ++r)
+                        cn[r] = src[r * 64];
+                }
+            }
+            const int acc_i = (int)(i & 1);
+            if (!failed && !__all_sync(0xffffffffu, mbar_wait(tfull + acc_i, (uint32_t)((i >> 1) & 1))))
+            {
+                s_fail = 1;
+                failed = true;
+            }
+            if (failed)
+                continue;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            // the accumulator in two halves of 16 rows, so only 16 of its values are live
+            const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc_i * 64 + h * 32);
+            float *dst = slab + oc + rowoff;
+            uint32_t v[16];
+            tmem_load16(ta, v);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (oc >= 0)
+            {
+#pragma unroll
+                for (int r = 0; r < 16; ++r)
+                    dst[r * 64] = cc[r] - __uint_as_float(v[r]);
+            }
+            tmem_load16(ta + 16, v);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+                mbar_arrive(tempty + acc_i);
+            if (oc >= 0)
+            {
+#pragma unroll
+                for (int r = 0; r < 16; ++r)
+                    dst[(r + 16) * 64] = cc[r + 16] - __uint_as_float(v[r]);
+            }
+        }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();

@@ -40,6 +40,8 @@ OPTION_ALTERNATE_WALK = 10
 OPTION_UPDATE_KERNEL = 11  # -1 tuned, 0 32x32 SIMT, 1 64x64 SIMT, 2 DMMA
 OPTION_PIVOT_LU_ONCE = 12
 OPTION_FP64_MMA_SHAPE = 13
+OPTION_PAIR_PASSES = 14  # mixed form: two consecutive pivots per tensor-core pass
+OPTION_ROW_PIVOTS = 15  # 64-row pivots: LU by rows, row solves by columns (64-thread CTAs)
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _i64p = ctypes.POINTER(ctypes.c_int64)
@@ -112,6 +114,11 @@ class KernelProfile(ctypes.Structure):
         ("c_elems", ctypes.c_double),
         ("ab_elems", ctypes.c_double),
         ("levels", ctypes.c_uint64),
+        ("passes", ctypes.c_uint64),
+        ("pivots_timed", ctypes.c_uint64),
+        ("pivot_ms", ctypes.c_double),
+        ("pivot_units", ctypes.c_uint64),
+        ("pivot_levels", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:

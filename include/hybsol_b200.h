@@ -223,7 +223,27 @@ typedef enum
     /* FP64 MMA instruction shape of the FP64 form's 64-block Schur update: 0 m8n8k4,
      * 1 (default) m16n8k8, 2 m16n8k16. The same products, summed in different groups inside
      * an instruction (FP64 factors agree to rounding). */
-    HYB_OPTION_FP64_MMA_SHAPE = 13
+    HYB_OPTION_FP64_MMA_SHAPE = 13,
+    /* Mixed form: 1 applies consecutive single pivots in pairs where the pattern allows
+     * (the second pivot lies in the first one's lower column and upper row, and the first
+     * one's other lower rows and upper columns are among the second one's): the first
+     * pivot's update of the second one's row and column runs on the pivot chain, and one
+     * tensor-core pass then applies both pivots to the second one's targets (K = 128), so
+     * each target is read and written once for two pivots. 0 (default): one pass per pivot
+     * (while the two pivots' chain is longer than the update it saves). The factors differ
+     * only by FP32 rounding (the two products are summed in the accumulator before they are
+     * subtracted). */
+    HYB_OPTION_PAIR_PASSES = 14,
+    /* Levels whose pivots and upper blocks are all 64x64: 1 factors each diagonal block
+     * with a blocked LU (eight-column panels by one warp, rank-8 updates by the CTA) and
+     * solves the upper blocks in 8x8 blocks, writing the mixed form's operand splits beside
+     * it (the same operations in the same order as 0: the same factors); 0: the 256-thread
+     * unblocked kernels (HYB_OPTION_PIVOT_LU_ONCE); 2 (mixed form, tensor-core levels):
+     * each pivot is factored once and inverted (blocked triangular inverses), and its
+     * upper blocks are taken as products with the inverse, so the pivot's critical path
+     * holds no substitution (FP32 factors that differ from 0 and 1 by rounding); -1
+     * (default): 2 for the mixed form, 0 for the FP64 form. */
+    HYB_OPTION_ROW_PIVOTS = 15
 } hyb_option;
 
 /* Sets a schedule option of the handle (takes effect at the next decomposition). */
@@ -336,12 +356,20 @@ HYB_API uint64_t hyb_last_launch_count(const hyb_system *sys);
 
 typedef struct
 {
-    uint64_t launches; /* levels whose Schur-update kernels were timed */
+    uint64_t launches; /* update passes whose Schur-update kernels were timed (one level, or a
+                          pair of levels applied in one two-pivot pass, HYB_OPTION_PAIR_PASSES) */
     double total_ms;   /* sum of their device durations (CUDA events on the handle's stream) */
     double flops;      /* algorithmic flops they performed */
     double c_elems;    /* target scalars each read and written once */
     double ab_elems;   /* operand scalars (lower-column and upper-row blocks) */
     uint64_t levels;   /* levels of the decomposition that have a Schur update, timed or not */
+    uint64_t passes;   /* update passes of the decomposition, timed or not (a pair counts once) */
+    uint64_t pivots_timed; /* levels covered by the timed passes */
+    double pivot_ms;       /* device time of the timed units' pivot work: LU, row solves, operand
+                              splits and, for a pair, the first pivot's update of the second one's
+                              row and column (CUDA events on the stream that runs it) */
+    uint64_t pivot_units;  /* units whose pivot work was timed */
+    uint64_t pivot_levels; /* levels they cover */
 } hyb_kernel_profile;
 
 /* With stride n >= 1, later decompositions record CUDA events around the Schur-update

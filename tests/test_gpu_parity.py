@@ -257,6 +257,7 @@ def test_pivot_lu_once_matches_fused(gpu, prec, p):
     pp = meshgen.random_orders(8, 2, 10, seed=31) if p == "rand" else p
     mat, b = _mesh(8, pp, seed=15)
     order, pm, ns = _native_from(gpu, mat)
+    ns.set_option(gpu.OPTION_ROW_PIVOTS, 0)  # the 256-thread kernels
     ns.set_option(gpu.OPTION_PIVOT_LU_ONCE, 1)
     ns.decompose(prec)
     blocks = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
@@ -267,6 +268,49 @@ def test_pivot_lu_once_matches_fused(gpu, prec, p):
     assert all(np.array_equal(x, y) for x, y in zip(blocks, blocks2))
 
 
+@pytest.mark.parametrize(("prec", "pairs"), [(0, 1), (1, 1), (1, 0)])
+def test_row_pivots_match_256_thread_kernels(gpu, prec, pairs):
+    """The 64-thread pivot kernel (LU by rows, row solves by columns, splits in the same
+    launch) gives the factors of the 256-thread kernels bit for bit, in both forms."""
+    mat, b = _mesh(12, 8, seed=21)
+    order, pm, ns = _native_from(gpu, mat)
+    ns.set_option(gpu.OPTION_PAIR_PASSES, pairs)
+    ns.set_option(gpu.OPTION_ROW_PIVOTS, 1)
+    ns.decompose(prec)
+    blocks = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
+    ns.set_option(gpu.OPTION_ROW_PIVOTS, 0)
+    ns.set_values(pm.vals)
+    ns.decompose(prec)
+    blocks2 = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
+    assert all(np.array_equal(x, y) for x, y in zip(blocks, blocks2))
+
+
+@pytest.mark.parametrize("pairs", [0, 1])
+def test_inverse_pivots_match_substitution(gpu, pairs):
+    """Mixed form: each 64-row pivot factored once and its upper blocks taken as products
+    with its inverse (the default) against the blocked substitution: the FP32 factors agree
+    to rounding, both refine to 1e-12 and agree with the oracle; the inverses written for
+    the inner solves are those the factorization used."""
+    mat, b = _mesh(12, 8, seed=27)
+    order, pm, ns = _native_from(gpu, mat)
+    bn = reorder_rhs(mat.sizes, order, b)
+    osys = O.OracleSystem.from_csr(pm.sizes, pm.row_ptr, pm.cols, pm.vals)
+    osys.decompose()
+    xo = osys.solve(bn)
+    ns.set_option(gpu.OPTION_PAIR_PASSES, pairs)
+    out = {}
+    for mode in (2, 1):
+        ns.set_option(gpu.OPTION_ROW_PIVOTS, mode)
+        ns.set_values(pm.vals)
+        ns.decompose(gpu.MIXED)
+        out[mode] = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
+        x, info = ns.solve(bn)
+        assert info["converged"] and info["relative_residual"] <= 1e-12, (mode, info)
+        assert rel_err(x, xo) < TOL_X_MIXED
+    worst = max(rel_err(a, b) for a, b in zip(out[2], out[1]))
+    assert 0 < worst < 1e-3, worst
+
+
 @pytest.mark.parametrize("prec", [0, 1])
 def test_sampled_update_profile(gpu, prec):
     """Event pairs around every n-th level's update: ceil(levels / n) timed levels, the same
@@ -275,6 +319,7 @@ def test_sampled_update_profile(gpu, prec):
 
     mat, b = _mesh(10, 8, seed=23)
     order, pm, ns = _native_from(gpu, mat)
+    ns.set_option(gpu.OPTION_PAIR_PASSES, 1)  # the mixed form then counts pairs as one pass
     lib = gpu.lib()
     ns.decompose(prec)
     ref = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
@@ -285,14 +330,51 @@ def test_sampled_update_profile(gpu, prec):
         ns.decompose(prec)
         prof = gpu.KernelProfile()
         assert lib.hyb_profile_read(ns._h, ctypes.byref(prof)) == 0
-        counts[stride] = (prof.launches, prof.levels)
+        counts[stride] = (prof.launches, prof.passes, prof.levels, prof.pivots_timed)
         assert prof.total_ms > 0 and prof.c_elems > 0
         blocks = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
         assert all(np.array_equal(x, y) for x, y in zip(ref, blocks))
-    levels = counts[1][1]
-    assert levels > 4 and counts[1] == (levels, levels) and counts[4] == ((levels + 3) // 4, levels)
+    passes, levels = counts[1][1], counts[1][2]
+    assert passes > 4 and counts[1] == (passes, passes, levels, levels)
+    assert counts[4][:3] == ((passes + 3) // 4, passes, levels)
+    # the FP64 form takes one pass per level; the mixed form applies most pivots in pairs
+    assert passes == levels if prec == 0 else levels // 2 < passes < levels
     assert lib.hyb_profile_enable(ns._h, -1) != 0
     assert lib.hyb_profile_enable(ns._h, 0) == 0
+
+
+@pytest.mark.parametrize("n", [8, 12])
+def test_pair_passes_match_single_passes(gpu, n):
+    """Two pivots per tensor-core pass (mixed form default) against one pass per pivot: the
+    factors differ only by the FP32 rounding of summing both products before subtracting
+    (well inside BF16x3 accuracy), both refine to 1e-12 and agree with the oracle; with
+    pairs, the lookahead schedule and the alternating walk give bit-identical factors."""
+    mat, b = _mesh(n, 8, seed=19)
+    order, pm, ns = _native_from(gpu, mat)
+    bn = reorder_rhs(mat.sizes, order, b)
+    osys = O.OracleSystem.from_csr(pm.sizes, pm.row_ptr, pm.cols, pm.vals)
+    osys.decompose()
+    xo = osys.solve(bn)
+
+    def factor(opts=None):
+        for k, v in (opts or {}).items():
+            ns.set_option(k, v)
+        ns.set_values(pm.vals)
+        ns.decompose(gpu.MIXED)
+        fs = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
+        x, info = ns.solve(bn)
+        assert info["converged"] and info["relative_residual"] <= 1e-12, info
+        assert rel_err(x, xo) < TOL_X_MIXED
+        return fs
+
+    paired = factor({gpu.OPTION_PAIR_PASSES: 1})
+    single = factor({gpu.OPTION_PAIR_PASSES: 0})
+    worst = max(rel_err(a, b) for a, b in zip(paired, single))
+    assert 0 < worst < 1e-3, worst  # the pair path ran, and only rounding separates them
+    ns.set_option(gpu.OPTION_PAIR_PASSES, 1)
+    for opts in ({gpu.OPTION_LOOKAHEAD: 0}, {gpu.OPTION_LOOKAHEAD: 1, gpu.OPTION_ALTERNATE_WALK: 0}):
+        again = factor(opts)
+        assert all(np.array_equal(x, y) for x, y in zip(paired, again)), opts
 
 
 @pytest.mark.parametrize("n", [5, 12])

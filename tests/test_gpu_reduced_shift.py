@@ -166,18 +166,24 @@ def test_growth_check_leaves_well_conditioned_factors_alone(gpu):
     assert np.array_equal(x0, x1)
 
 
-@pytest.mark.parametrize("lu_once", [1, 0])
+# 64-row pivot paths: (HYB_OPTION_ROW_PIVOTS, HYB_OPTION_PIVOT_LU_ONCE)
+PIVOT_PATHS = {"inverse": (2, -1), "blocked": (1, -1), "fused": (0, 0), "once": (0, 1)}
+
+
+@pytest.mark.parametrize("path", sorted(PIVOT_PATHS))
 @pytest.mark.parametrize(("n", "p", "reduced"), [(8, 8, True), (16, 4, True), (6, "rand", False)])
-def test_growth_fallback_refactors_in_fp64(gpu, n, p, reduced, lu_once):
-    """A limit of 1 flags most pivots, so every path runs: the fused 64-row FP64 redo, the
-    FP64 LU and row solves of pivots of at most 32 rows, and pivots over 64 rows (orders
-    9 and 10) counted as kept in FP32. The mixed solve still reaches the tolerance."""
+def test_growth_fallback_refactors_in_fp64(gpu, n, p, reduced, path):
+    """A limit of 1 flags most pivots, so every path runs: the FP64 redo of each 64-row
+    pivot kernel (inverse and products, blocked, fused, once + strips), the FP64 LU and row
+    solves of pivots of at most 32 rows, and pivots over 64 rows (orders 9 and 10) counted
+    as kept in FP32. The mixed solve still reaches the tolerance."""
     from hybsol.b200 import meshgen
 
     pp = meshgen.random_orders(n, 2, 10, seed=8) if p == "rand" else p
     alpha = meshgen.reduced_shift(n, p) if reduced else 1.0
     ns, pm, bn = _system(gpu, n, pp, shift=alpha)
-    ns.set_option(gpu.OPTION_PIVOT_LU_ONCE, lu_once)  # both 64-row paths: LU once + strips, or fused
+    ns.set_option(gpu.OPTION_ROW_PIVOTS, PIVOT_PATHS[path][0])
+    ns.set_option(gpu.OPTION_PIVOT_LU_ONCE, PIVOT_PATHS[path][1])
     ns.set_option(gpu.OPTION_GROWTH_LIMIT, 1)
     d = ns.decompose(gpu.MIXED)
     assert d["growth_fp64"] > 0, d
