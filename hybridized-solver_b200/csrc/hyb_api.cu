@@ -171,7 +171,7 @@ struct hyb_system
     float growth_limit = 1024.0f;         // HYB_OPTION_GROWTH_LIMIT (mixed form)
     bool block_scaling = true;            // HYB_OPTION_BLOCK_SCALING (mixed form)
     bool alternate_walk = true;           // HYB_OPTION_ALTERNATE_WALK
-    bool pair_passes = false;             // HYB_OPTION_PAIR_PASSES (mixed form)
+    bool pair_passes = true;              // HYB_OPTION_PAIR_PASSES (mixed form)
     int row_pivots = -1;                  // HYB_OPTION_ROW_PIVOTS: -1 per precision (mixed 2, FP64 0)
     // generic-size Schur updates: HYB_OPTION_UPDATE_KERNEL (-1: tuned per size bucket), and
     // the tuned choice per precision and bucket (-1: not tuned yet)

@@ -24,6 +24,7 @@ namespace hyb
 constexpr int kPivThreads = 256;
 constexpr int kLdD = 65; // row stride of the diagonal block in shared memory
 constexpr int kLdQ = 80; // column stride of the transposed factors (four 16-row quarters, 20 apart)
+constexpr int kLdI = 68; // row stride of the inverses and product operands (16-byte rows)
 
 // Dynamic shared memory of k_piv64 (PivLayout below, plus reduction slots); the FP32
 // kernel's FP64 fallback reuses it for a 64 x 65 FP64 block, which fits.
@@ -61,6 +62,32 @@ template <typename T> __device__ __forceinline__ void load16(T *dst, const T *sr
         dst[0] = v.x;
         dst[1] = v.y;
     }
+}
+
+// Copies a 64x64 block from global memory into shared memory (row stride kLdD), every
+// thread's 16-byte loads issued before any is stored, and returns the thread's largest
+// |entry|; ends with a barrier.
+template <typename T> __device__ __forceinline__ T load_block64(const T *g, T *d)
+{
+    constexpr int n = Vec16<T>::n, per = 64 * 64 / n / kPivThreads; // vectors per thread
+    T v[per][n];
+#pragma unroll
+    for (int q = 0; q < per; ++q)
+        load16(v[q], g + (threadIdx.x + q * kPivThreads) * n);
+    T amax = T(0);
+#pragma unroll
+    for (int q = 0; q < per; ++q)
+    {
+        const int i = (threadIdx.x + q * kPivThreads) * n;
+#pragma unroll
+        for (int e = 0; e < n; ++e)
+        {
+            d[((i + e) >> 6) * kLdD + ((i + e) & 63)] = v[q][e];
+            amax = fmax(amax, fabs(v[q][e]));
+        }
+    }
+    __syncthreads();
+    return amax;
 }
 
 // Shared memory of one CTA (T elements):
@@ -343,9 +370,9 @@ template <typename T> __device__ void tri_inv64_blocked(const T *d, T *li, T *ui
     {
         const int r = e >> 6, c = e & 63;
         if (c > r)
-            li[r * kLdD + c] = T(0);
+            li[r * kLdI + c] = T(0);
         if (c < r)
-            ui[r * kLdD + c] = T(0);
+            ui[r * kLdI + c] = T(0);
     }
     // diagonal blocks: thread t < 64 takes column t & 7 of block t >> 3 of L^{-1};
     // threads 64 .. 127 the same of U^{-1}
@@ -366,7 +393,7 @@ template <typename T> __device__ void tri_inv64_blocked(const T *d, T *li, T *ui
             }
 #pragma unroll
             for (int r = 0; r < 8; ++r)
-                li[(o + r) * kLdD + o + jj] = y[r];
+                li[(o + r) * kLdI + o + jj] = y[r];
         }
         else
         {
@@ -381,35 +408,34 @@ template <typename T> __device__ void tri_inv64_blocked(const T *d, T *li, T *ui
             }
 #pragma unroll
             for (int r = 0; r < 8; ++r)
-                ui[(o + r) * kLdD + o + jj] = y[r];
+                ui[(o + r) * kLdI + o + jj] = y[r];
         }
     }
     __syncthreads();
 #pragma unroll 1
     for (int s = 1; s < 8; ++s)
     {
-        const int nb = 8 - s;          // blocks at distance s
-        const int outs = nb * 64;      // values per triangle
-        // partial sums: L side for block (i, j) = (j + s, j), U side for (i, i + s)
+        const int nb = 8 - s;     // blocks at distance s
+        const int outs = nb * 64; // values per triangle
+        // partial sums: L side for block (i, j) = (j + s, j), U side for (i, i + s); each
+        // an eight-term product per block of the sum, eight independent accumulators
         for (int e = tid; e < 2 * outs; e += blockDim.x)
         {
             const bool up = e >= outs;
             const int f = up ? e - outs : e;
             const int blk = f >> 6, r = (f >> 3) & 7, c = f & 7;
-            T acc = T(0);
-            if (!up)
+            const int i = up ? blk : blk + s, j = up ? blk + s : blk; // block (i, j)
+            const int m0 = up ? 8 * i + 8 : 8 * j, m1 = up ? 8 * j + 8 : 8 * i;
+            const T *row = d + (8 * i + r) * kLdD;
+            const T *inv = (up ? ui : li) + 8 * j + c;
+            T acc[8] = {};
+            for (int m = m0; m < m1; m += 8)
             {
-                const int j = blk, i = j + s; // sum_{k=j}^{i-1} L_ik Li_kj
-                for (int m = 8 * j; m < 8 * i; ++m)
-                    acc += d[(8 * i + r) * kLdD + m] * li[m * kLdD + 8 * j + c];
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    acc[q] += row[m + q] * inv[(m + q) * kLdI];
             }
-            else
-            {
-                const int i = blk, j = i + s; // sum_{k=i+1}^{j} U_ik Ui_kj
-                for (int m = 8 * i + 8; m < 8 * j + 8; ++m)
-                    acc += d[(8 * i + r) * kLdD + m] * ui[m * kLdD + 8 * j + c];
-            }
-            tmp[e] = acc;
+            tmp[e] = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
         }
         __syncthreads();
         for (int e = tid; e < 2 * outs; e += blockDim.x)
@@ -417,24 +443,14 @@ template <typename T> __device__ void tri_inv64_blocked(const T *d, T *li, T *ui
             const bool up = e >= outs;
             const int f = up ? e - outs : e;
             const int blk = f >> 6, r = (f >> 3) & 7, c = f & 7;
+            const int i = up ? blk : blk + s, j = up ? blk + s : blk;
             const T *t = tmp + (up ? outs : 0) + blk * 64;
+            const T *dgi = (up ? ui : li) + (8 * i + r) * kLdI + 8 * i; // row r of the diagonal block's inverse
             T acc = T(0);
-            if (!up)
-            {
-                const int j = blk, i = j + s; // Li_ij = -Li_ii t
 #pragma unroll
-                for (int m = 0; m < 8; ++m)
-                    acc -= li[(8 * i + r) * kLdD + 8 * i + m] * t[m * 8 + c];
-                li[(8 * i + r) * kLdD + 8 * j + c] = acc;
-            }
-            else
-            {
-                const int i = blk, j = i + s; // Ui_ij = -Ui_ii t
-#pragma unroll
-                for (int m = 0; m < 8; ++m)
-                    acc -= ui[(8 * i + r) * kLdD + 8 * i + m] * t[m * 8 + c];
-                ui[(8 * i + r) * kLdD + 8 * j + c] = acc;
-            }
+            for (int m = 0; m < 8; ++m)
+                acc -= dgi[m] * t[m * 8 + c];
+            (up ? ui : li)[(8 * i + r) * kLdI + 8 * j + c] = acc;
         }
         __syncthreads();
     }
@@ -442,7 +458,7 @@ template <typename T> __device__ void tri_inv64_blocked(const T *d, T *li, T *ui
 
 // the FP32 working set (LU, two triangular inverses, partial sums); the FP64 fallback's LU
 // (64 x 65 doubles) fits in it, its inverse goes straight to the FP64 slot in global memory
-constexpr int kInvSmem = (3 * 64 * kLdD + 2 * 7 * 64) * 4;
+constexpr int kInvSmem = (64 * kLdD + 2 * 64 * kLdI + 2 * 7 * 64) * 4;
 static_assert(64 * 65 * 8 <= kInvSmem, "the FP64 fallback's LU fits the FP32 working set");
 
 // One CTA per pivot of the level: the blocked LU of the 64x64 diagonal block (stored back
@@ -457,20 +473,13 @@ __global__ void __launch_bounds__(kPivThreads, 1)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float *d = reinterpret_cast<float *>(smem_raw);
-    float *li = d + 64 * kLdD, *ui = li + 64 * kLdD, *tmp = ui + 64 * kLdD;
+    float *li = d + 64 * kLdD, *ui = li + 64 * kLdI, *tmp = ui + 64 * kLdI; // li 16-byte aligned
     const int tid = threadIdx.x;
     const int64_t p = p0 + blockIdx.x;
     const int64_t k = S.piv[p];
     float *gd = slab + S.blk_off[S.diag_pos[k]];
     float *xt = dinv + (int64_t)S.inv_idx[k] * 4096;
-    float amax = 0.f;
-    for (int i = tid; i < 64 * 64; i += kPivThreads)
-    {
-        const float v = gd[i];
-        d[(i >> 6) * kLdD + (i & 63)] = v;
-        amax = fmaxf(amax, fabsf(v));
-    }
-    __syncthreads();
+    float amax = load_block64(gd, d);
     const bool check = growth_limit > 0;
     if (check)
         amax = cta_max(amax);
@@ -554,13 +563,12 @@ __global__ void __launch_bounds__(kPivThreads, 1)
         float acc[4][4] = {};
         for (int m = max(R, C); m < 64; ++m)
         {
-            float a4[4], b4[4];
+            float a4[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q)
-            {
-                a4[q] = ui[(R + q) * kLdD + m];
-                b4[q] = li[m * kLdD + C + q];
-            }
+                a4[q] = ui[(R + q) * kLdI + m];
+            const float4 b = *reinterpret_cast<const float4 *>(li + m * kLdI + C);
+            const float b4[4] = {b.x, b.y, b.z, b.w};
 #pragma unroll
             for (int q = 0; q < 4; ++q)
 #pragma unroll
@@ -568,12 +576,11 @@ __global__ void __launch_bounds__(kPivThreads, 1)
                     acc[q][e] += a4[q] * b4[e];
         }
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-#pragma unroll
-            for (int e = 0; e < 4; ++e)
-                xt[(C + e) * 64 + R + q] = acc[q][e];
+        for (int e = 0; e < 4; ++e)
+            *reinterpret_cast<float4 *>(xt + (C + e) * 64 + R) = make_float4(acc[0][e], acc[1][e], acc[2][e], acc[3][e]);
     }
 }
+
 
 // The upper blocks of the level's pivots as products with the pivots' inverses: CTA u of
 // the level's upper blocks (trsm_pref) computes U(k, c) = X A(k, c), X = D_k^{-1} from
@@ -583,8 +590,8 @@ __global__ void __launch_bounds__(kPivThreads, 2)
     k_strips64_inv(DevSym S, float *__restrict__ slab, int64_t p0, int64_t p1, const float *__restrict__ dinv,
                    const double *__restrict__ inv64, const int *__restrict__ hg, unsigned char *__restrict__ ops)
 {
-    __shared__ __align__(16) float xs[64 * 65]; // X transposed: xs[c * 65 + r] = X[r][c]
-    __shared__ __align__(16) float as[64 * 65]; // A(k, c), then the product, row-major
+    __shared__ __align__(16) float xs[64 * kLdI]; // X transposed: xs[c * kLdI + r] = X[r][c]
+    __shared__ __align__(16) float as[64 * kLdI]; // A(k, c), then the product, row-major
     const int tid = threadIdx.x;
     const int64_t u = S.trsm_pref[p0] + blockIdx.x;
     const int64_t p = find_owner(S.trsm_pref, p0, p1, u);
@@ -592,10 +599,11 @@ __global__ void __launch_bounds__(kPivThreads, 2)
     const int64_t j = u - S.trsm_pref[p];
     float *gb = slab + S.blk_off[S.diag_pos[k] + 1 + j];
     const float *xt = dinv + (int64_t)S.inv_idx[k] * 4096;
-    for (int i = tid; i < 64 * 64; i += kPivThreads)
+    for (int i = tid; i < 64 * 16; i += kPivThreads)
     {
-        xs[(i >> 6) * 65 + (i & 63)] = xt[i];
-        as[(i >> 6) * 65 + (i & 63)] = gb[i];
+        const int r = i >> 4, c4 = (i & 15) * 4;
+        *reinterpret_cast<float4 *>(xs + r * kLdI + c4) = *reinterpret_cast<const float4 *>(xt + r * 64 + c4);
+        *reinterpret_cast<float4 *>(as + r * kLdI + c4) = *reinterpret_cast<const float4 *>(gb + r * 64 + c4);
     }
     __syncthreads();
     const int R = 4 * (tid >> 4), C = 4 * (tid & 15);
@@ -610,7 +618,7 @@ __global__ void __launch_bounds__(kPivThreads, 2)
             for (int q = 0; q < 4; ++q)
 #pragma unroll
                 for (int e = 0; e < 4; ++e)
-                    ad[q][e] += x64[(R + q) * 64 + m] * (double)as[m * 65 + C + e];
+                    ad[q][e] += x64[(R + q) * 64 + m] * (double)as[m * kLdI + C + e];
 #pragma unroll
         for (int q = 0; q < 4; ++q)
 #pragma unroll
@@ -619,43 +627,38 @@ __global__ void __launch_bounds__(kPivThreads, 2)
     }
     else
     {
-#pragma unroll 4
+#pragma unroll 8
         for (int m = 0; m < 64; ++m)
         {
-            float a4[4], b4[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-            {
-                a4[q] = xs[m * 65 + R + q];
-                b4[q] = as[m * 65 + C + q];
-            }
+            const float4 a4 = *reinterpret_cast<const float4 *>(xs + m * kLdI + R);
+            const float4 b4 = *reinterpret_cast<const float4 *>(as + m * kLdI + C);
+            const float av[4] = {a4.x, a4.y, a4.z, a4.w}, bv[4] = {b4.x, b4.y, b4.z, b4.w};
 #pragma unroll
             for (int q = 0; q < 4; ++q)
 #pragma unroll
                 for (int e = 0; e < 4; ++e)
-                    acc[q][e] += a4[q] * b4[e];
+                    acc[q][e] += av[q] * bv[e];
         }
     }
     __syncthreads(); // every thread is done reading A
 #pragma unroll
     for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int e = 0; e < 4; ++e)
-        {
-            gb[(R + q) * 64 + C + e] = acc[q][e];
-            as[(R + q) * 65 + C + e] = acc[q][e];
-        }
+    {
+        const float4 v = make_float4(acc[q][0], acc[q][1], acc[q][2], acc[q][3]);
+        *reinterpret_cast<float4 *>(gb + (R + q) * 64 + C) = v;
+        *reinterpret_cast<float4 *>(as + (R + q) * kLdI + C) = v;
+    }
     __syncthreads();
     // split: row n of the transposed tile is column n of U, K = its row index
     const int64_t n_lc = S.lcol_ptr[k + 1] - S.lcol_ptr[k];
     unsigned char *dst = ops + (S.split_pref[p] - S.split_pref[p0] + n_lc + j) * (int64_t)kSplitBytes;
     for (int ch = tid; ch < 512; ch += kPivThreads)
     {
-        const int nn = ch >> 3, q = ch & 7;
+        const int nn = ch & 63, q = ch >> 6; // a warp reads 32 consecutive columns: no conflicts
         float x[8];
 #pragma unroll
         for (int e = 0; e < 8; ++e)
-            x[e] = as[(q * 8 + e) * 65 + nn];
+            x[e] = as[(q * 8 + e) * kLdI + nn];
         uint4 hi, lo;
         split8(x, hi, lo);
         const uint32_t off = sw128_offset(nn, q * 8);
@@ -793,14 +796,7 @@ __global__ void __launch_bounds__(kPivThreads, 3)
     unsigned char *split =
         kSplit && gb != nullptr ? ops + (S.split_pref[p] - S.split_pref[p0] + n_lc + j) * (int64_t)kSplitBytes : nullptr;
     const bool check = std::is_same_v<T, float> && growth_limit > 0;
-    T amax = T(0);
-    for (int i = tid; i < 64 * 64; i += kPivThreads)
-    {
-        const T v = gd[i];
-        f.d[(i >> 6) * kLdD + (i & 63)] = v;
-        amax = fmax(amax, fabs(v));
-    }
-    __syncthreads();
+    T amax = load_block64(gd, f.d);
     if (check)
         amax = cta_max(amax);
     lu64_blocked(f.d, owner ? status : nullptr, (int)k);

@@ -224,13 +224,13 @@ typedef enum
      * 1 (default) m16n8k8, 2 m16n8k16. The same products, summed in different groups inside
      * an instruction (FP64 factors agree to rounding). */
     HYB_OPTION_FP64_MMA_SHAPE = 13,
-    /* Mixed form: 1 applies consecutive single pivots in pairs where the pattern allows
+    /* Mixed form: 1 (default) applies consecutive single pivots in pairs where the pattern allows
      * (the second pivot lies in the first one's lower column and upper row, and the first
      * one's other lower rows and upper columns are among the second one's): the first
      * pivot's update of the second one's row and column runs on the pivot chain, and one
      * tensor-core pass then applies both pivots to the second one's targets (K = 128), so
-     * each target is read and written once for two pivots. 0 (default): one pass per pivot
-     * (while the two pivots' chain is longer than the update it saves). The factors differ
+     * each target is read and written once for two pivots. 0: one pass per pivot. The
+     * factors differ
      * only by FP32 rounding (the two products are summed in the accumulator before they are
      * subtracted). */
     HYB_OPTION_PAIR_PASSES = 14,
