@@ -49,6 +49,9 @@ CPU_SAMPLE_MESH = 20  # reference CPU sample: 20x20 elements at the same p
 # measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum, one pass) on a 96x96
 # p=8 stage, whose targets exceed L2: 245.3 MB for ~9,000 target blocks.
 TC_DRAM_BYTES_PER_TARGET_BLOCK = 245.3e6 / 9000
+# the two-pivot pass (k_update64_tc2) at 96x96 p=8: priority + rest launches of one pair,
+# dram__bytes_read.sum + dram__bytes_write.sum (12.6 + 152.5 + 82.6 MB) over ~9,400 target blocks
+TC2_DRAM_BYTES_PER_TARGET_BLOCK = 247.7e6 / 9400
 
 
 def parse_args():
@@ -845,6 +848,7 @@ def run_ours(args):
             "k_update64_tc2 (tcgen05 split-BF16, two pivots per pass: K = 128, targets staged in registers, "
             "persistent)"
         )
+        rmix["traffic"] = TC2_DRAM_BYTES_PER_TARGET_BLOCK * mixed_prof.c_elems / mixed_prof.launches / 4096.0
     if rf64 is not None:
         rf64["traffic_note"] = (
             "null: the FP64 update's DRAM bytes were captured only at 32x32 (profiles/k_update64_f64_mesh32_p8.md), "
@@ -852,8 +856,10 @@ def run_ours(args):
         )
     if rmix is not None:
         rmix["traffic_note"] = (
-            "dram__bytes_read.sum + dram__bytes_write.sum of one stage (both launches) from a 1-pass ncu capture "
-            "at 96x96 p=8, 27.2 KB per 64x64 target block, scaled to this stage's target blocks"
+            "dram__bytes_read.sum + dram__bytes_write.sum of one pass (both launches) from a 1-pass ncu capture "
+            "at 96x96 p=8 (profiles/k_update64_tc2_mesh48_p8.md for the two-pivot pass: 26.4 KB per 64x64 target "
+            "block per pair; profiles/k_update64_tc_dram_mesh96_p8.md for one pivot per pass: 27.2 KB per target "
+            "block per stage), scaled to this pass's target blocks"
         )
     if rmix is not None:
         # three BF16 MMAs per FP32 product on the tensor cores, against the sustained peak

@@ -171,7 +171,7 @@ struct hyb_system
     float growth_limit = 1024.0f;         // HYB_OPTION_GROWTH_LIMIT (mixed form)
     bool block_scaling = true;            // HYB_OPTION_BLOCK_SCALING (mixed form)
     bool alternate_walk = true;           // HYB_OPTION_ALTERNATE_WALK
-    bool pair_passes = true;              // HYB_OPTION_PAIR_PASSES (mixed form)
+    int pair_passes = 1;                  // HYB_OPTION_PAIR_PASSES (mixed form; 2: inner update launched apart)
     int row_pivots = -1;                  // HYB_OPTION_ROW_PIVOTS: -1 per precision (mixed 2, FP64 0)
     // generic-size Schur updates: HYB_OPTION_UPDATE_KERNEL (-1: tuned per size bucket), and
     // the tuned choice per precision and bucket (-1: not tuned yet)
@@ -489,6 +489,12 @@ const unsigned char *zero_split(const hyb_system *h)
     return h->d_ops + (size_t)kOpsSlots * h->split_half;
 }
 
+// One FP32 64x64 block after it: a pair's U(c,d), for the updates of the second pivot's column.
+float *pair_ucd(hyb_system *h)
+{
+    return reinterpret_cast<float *>(h->d_ops + (size_t)kOpsSlots * h->split_half + hyb::kSplitBytes);
+}
+
 // BF16 split of a tensor-core level's operands, once its pivots are factored.
 template <typename T> int enqueue_split(hyb_system *h, T *slab, int64_t l, cudaStream_t st, uint64_t &launches)
 {
@@ -516,7 +522,20 @@ bool fused_pivots(const Symbolic::LevelShape &sh)
     return sh.max_piv > 32 && sh.max_piv <= 64 && sh.max_up <= 128;
 }
 
-template <typename T> int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cudaStream_t st, uint64_t &launches)
+// Whether level l's 64-row pivots take the inverse-and-products path (HYB_OPTION_ROW_PIVOTS 2,
+// by default in the mixed form).
+template <typename T> bool inverse_pivots(const hyb_system *h, int64_t l)
+{
+    const Symbolic::LevelShape &sh = h->S.shape[l];
+    const int mode64 = h->row_pivots < 0 ? (std::is_same_v<T, float> ? 2 : 0) : h->row_pivots;
+    return std::is_same_v<T, float> && fused_pivots(sh) && sh.piv64 && mode64 == 2 && tc_level<T>(h, l) && h->d_dinv;
+}
+
+// With pair_first (level l's pivot is the first of a pair on the inverse-and-products path),
+// the first pivot's update of the second one's row and column is applied by the products
+// kernel too; the caller then issues no separate update for it.
+template <typename T>
+int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cudaStream_t st, uint64_t &launches, bool pair_first = false)
 {
     const Symbolic &S = h->S;
     const DevSym &ds = h->ds;
@@ -533,7 +552,7 @@ template <typename T> int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cuda
     const int mode64 = h->row_pivots < 0 ? (std::is_same_v<T, float> ? 2 : 0) : h->row_pivots;
     if constexpr (std::is_same_v<T, float>)
     {
-        if (fused_pivots(sh) && sh.piv64 && mode64 == 2 && tc_level<T>(h, l) && h->d_dinv)
+        if (inverse_pivots<T>(h, l))
         {
             const int64_t n_split = S.split_pref[p1] - S.split_pref[p0];
             const int64_t n_trsm = S.trsm_pref[p1] - S.trsm_pref[p0];
@@ -548,14 +567,18 @@ template <typename T> int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cuda
                 HYB_LAUNCHED("k_split64", l);
             }
             HYB_CUDA(cudaEventRecord(h->ev_join3, h->stream3));
+            // a pair's first pivot: the second pivot's positions in its lower column and upper row
+            const int32_t i0 = pair_first ? sh.la_i0 : -1, j0 = pair_first ? sh.la_j0 : -1;
+            const int64_t n_col = pair_first ? S.lcol_ptr[S.piv[p0] + 1] - S.lcol_ptr[S.piv[p0]] - 1 : 0;
             hyb::k_piv64_inv<<<(unsigned)(p1 - p0), hyb::kPivThreads, hyb::kInvSmem, st>>>(
-                ds, slab, p0, h->d_status, glim, h->d_dinv, inv64, h->d_hg);
+                ds, slab, p0, h->d_status, glim, h->d_dinv, inv64, h->d_hg, j0, pair_ucd(h));
             ++launches;
             HYB_LAUNCHED("k_piv64_inv", l);
-            if (n_trsm > 0)
+            if (n_trsm + n_col > 0)
             {
-                hyb::k_strips64_inv<<<(unsigned)n_trsm, hyb::kPivThreads, 0, st>>>(
-                    ds, slab, p0, p1, h->d_dinv, inv64, glim > 0 ? h->d_hg : nullptr, level_ops(h, l));
+                hyb::k_strips64_inv<<<(unsigned)(n_trsm + n_col), hyb::kPivThreads, 0, st>>>(
+                    ds, slab, p0, p1, h->d_dinv, inv64, glim > 0 ? h->d_hg : nullptr, level_ops(h, l), i0, j0,
+                    pair_ucd(h));
                 ++launches;
                 HYB_LAUNCHED("k_strips64_inv", l);
             }
@@ -930,7 +953,7 @@ template <typename T> int enqueue_update(hyb_system *h, T *slab, int64_t l, cuda
 // tensor cores, a pair of the symbolic phase (Symbolic::PairShape), option on.
 template <typename T> bool pair_unit(const hyb_system *h, int64_t l)
 {
-    return std::is_same_v<T, float> && h->pair_passes && l + 1 < h->S.n_levels && h->S.pair_first[l] &&
+    return std::is_same_v<T, float> && h->pair_passes != 0 && l + 1 < h->S.n_levels && h->S.pair_first[l] &&
            tc_level<T>(h, l) && tc_level<T>(h, l + 1);
 }
 
@@ -940,11 +963,15 @@ template <typename T> bool pair_unit(const hyb_system *h, int64_t l)
 // then b's.
 template <typename T> int enqueue_unit_pivots(hyb_system *h, T *slab, int64_t l, cudaStream_t st, uint64_t &launches)
 {
-    int rc = enqueue_pivots<T>(h, slab, l, st, launches);
-    if (rc != HYB_SUCCESS || !pair_unit<T>(h, l))
+    const bool pair = pair_unit<T>(h, l);
+    const bool fold = pair && h->pair_passes == 1 && inverse_pivots<T>(h, l) && h->S.shape[l].la_i0 >= 0 &&
+                      h->S.shape[l].la_j0 >= 0;
+    int rc = enqueue_pivots<T>(h, slab, l, st, launches, fold);
+    if (rc != HYB_SUCCESS || !pair)
         return rc;
     const Symbolic::LevelShape &sh = h->S.shape[l];
-    if ((rc = enqueue_generic_update<T>(h, slab, l, st, 1, sh.la_prio_units, UPD_TILE32, launches)) != HYB_SUCCESS)
+    if (!fold && (rc = enqueue_generic_update<T>(h, slab, l, st, 1, sh.la_prio_units, UPD_TILE32, launches)) !=
+                     HYB_SUCCESS)
         return rc;
     return enqueue_pivots<T>(h, slab, l + 1, st, launches);
 }
@@ -2201,9 +2228,11 @@ HYB_API int hyb_system_set_option(hyb_system *h, int option, int64_t value)
         }
         return HYB_SUCCESS;
     case HYB_OPTION_PAIR_PASSES:
-        if (h->pair_passes != (value != 0))
+        if (value < 0 || value > 2)
+            return HYB_INVALID_ARGUMENT;
+        if (h->pair_passes != (int)value)
         {
-            h->pair_passes = value != 0;
+            h->pair_passes = (int)value;
             h->g_factor[1].reset();
         }
         return HYB_SUCCESS;
@@ -2440,7 +2469,7 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
         {
             h->split_half = (size_t)S.max_split_blocks * hyb::kSplitBytes;
             h->tgt_half = (size_t)std::max<int64_t>(1, S.max_tc_targets);
-            HYB_CUDA(cudaMalloc(&h->d_ops, kOpsSlots * h->split_half + hyb::kSplitBytes));
+            HYB_CUDA(cudaMalloc(&h->d_ops, kOpsSlots * h->split_half + 2 * hyb::kSplitBytes));
             HYB_CUDA(cudaMemset(h->d_ops + kOpsSlots * h->split_half, 0, hyb::kSplitBytes));
             HYB_CUDA(cudaMalloc(&h->d_tgt, kOpsSlots * h->tgt_half * sizeof(int64_t)));
             h->g_factor[1].reset();

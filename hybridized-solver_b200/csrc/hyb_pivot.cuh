@@ -456,6 +456,65 @@ template <typename T> __device__ void tri_inv64_blocked(const T *d, T *li, T *ui
     }
 }
 
+// acc = X B for this thread's 4x4 tile (rows R .., columns C ..) of a 64x64 product, with
+// X transposed (xs[m * kLdI + r] = X[r][m]) and B row-major (bs[m * kLdI + c]) in shared
+// memory. Every caller uses this one loop, so a block formed in two places is the same bits.
+__device__ __forceinline__ void prod64_tile(const float *xs, const float *bs, int R, int C, float (&acc)[4][4])
+{
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            acc[q][e] = 0.f;
+#pragma unroll 8
+    for (int m = 0; m < 64; ++m)
+    {
+        const float4 a4 = *reinterpret_cast<const float4 *>(xs + m * kLdI + R);
+        const float4 b4 = *reinterpret_cast<const float4 *>(bs + m * kLdI + C);
+        const float av[4] = {a4.x, a4.y, a4.z, a4.w}, bv[4] = {b4.x, b4.y, b4.z, b4.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                acc[q][e] += av[q] * bv[e];
+    }
+}
+
+// The same in FP64 with X row-major in global memory (x64[r * 64 + m], a high-growth
+// pivot's FP64 inverse) and B in FP32 shared memory, rounded to FP32.
+__device__ __forceinline__ void prod64_tile_fp64(const double *x64, const float *bs, int R, int C, float (&acc)[4][4])
+{
+    double ad[4][4] = {};
+#pragma unroll 1
+    for (int m = 0; m < 64; ++m)
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                ad[q][e] += x64[(R + q) * 64 + m] * (double)bs[m * kLdI + C + e];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            acc[q][e] = (float)ad[q][e];
+}
+
+// Copies a row-major 64x64 FP32 block from global memory into shared memory with row stride
+// kLdI (16-byte loads, all issued before any is stored).
+__device__ __forceinline__ void load_block64_ldi(const float *g, float *s)
+{
+    float4 v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        v[q] = *reinterpret_cast<const float4 *>(g + (threadIdx.x + q * kPivThreads) * 4);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+    {
+        const int i = (threadIdx.x + q * kPivThreads) * 4;
+        *reinterpret_cast<float4 *>(s + (i >> 6) * kLdI + (i & 63)) = v[q];
+    }
+}
+
 // the FP32 working set (LU, two triangular inverses, partial sums); the FP64 fallback's LU
 // (64 x 65 doubles) fits in it, its inverse goes straight to the FP64 slot in global memory
 constexpr int kInvSmem = (64 * kLdD + 2 * 64 * kLdI + 2 * 7 * 64) * 4;
@@ -467,9 +526,15 @@ static_assert(64 * 65 * 8 <= kInvSmem, "the FP64 fallback's LU fits the FP32 wor
 // check (growth_limit > 0): past the limit the pivot is factored and inverted in FP64 from
 // its original values (rolled loops in shared memory), the FP64 inverse goes to `inv64`
 // (slot p - p0) for the products, and hg[k] is set.
+//
+// First pivot c of a pair (j0 >= 0: the second pivot d's position in c's upper row): the CTA
+// also forms U(c,d) = X A(c,d) into `ucd` (row-major), with the loop k_strips64_inv uses
+// for the same block, so the column updates of the pair's second pivot can read it while
+// that block is being overwritten in place.
 __global__ void __launch_bounds__(kPivThreads, 1)
     k_piv64_inv(DevSym S, float *__restrict__ slab, int64_t p0, int *status, float growth_limit,
-                float *__restrict__ dinv, double *__restrict__ inv64, int *__restrict__ hg)
+                float *__restrict__ dinv, double *__restrict__ inv64, int *__restrict__ hg, int32_t j0,
+                float *__restrict__ ucd)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float *d = reinterpret_cast<float *>(smem_raw);
@@ -551,6 +616,20 @@ __global__ void __launch_bounds__(kPivThreads, 1)
                 hg[k] = 1;
                 atomicAdd(status + ST_GROWTH_FP64, 1);
             }
+            if (j0 >= 0)
+            {
+                // U(c,d) in FP64 with the FP64 inverse, A(c,d) past the FP64 LU
+                float *bsm = reinterpret_cast<float *>(smem_raw + 64 * 65 * 8);
+                load_block64_ldi(slab + S.blk_off[S.diag_pos[k] + 1 + j0], bsm);
+                __syncthreads();
+                const int R = 4 * (tid >> 4), C = 4 * (tid & 15);
+                float acc[4][4];
+                prod64_tile_fp64(b, bsm, R, C, acc);
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    *reinterpret_cast<float4 *>(ucd + (R + q) * 64 + C) =
+                        make_float4(acc[q][0], acc[q][1], acc[q][2], acc[q][3]);
+            }
             return;
         }
     }
@@ -578,68 +657,111 @@ __global__ void __launch_bounds__(kPivThreads, 1)
 #pragma unroll
         for (int e = 0; e < 4; ++e)
             *reinterpret_cast<float4 *>(xt + (C + e) * 64 + R) = make_float4(acc[0][e], acc[1][e], acc[2][e], acc[3][e]);
+        if (j0 >= 0)
+        {
+            // X (transposed, stride kLdI) over L^{-1}, A(c,d) over U^{-1}, then U(c,d)
+            __syncthreads(); // every thread is done reading li and ui
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                *reinterpret_cast<float4 *>(li + (C + e) * kLdI + R) =
+                    make_float4(acc[0][e], acc[1][e], acc[2][e], acc[3][e]);
+            load_block64_ldi(slab + S.blk_off[S.diag_pos[k] + 1 + j0], ui);
+            __syncthreads();
+            prod64_tile(li, ui, R, C, acc);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                *reinterpret_cast<float4 *>(ucd + (R + q) * 64 + C) =
+                    make_float4(acc[q][0], acc[q][1], acc[q][2], acc[q][3]);
+        }
     }
 }
 
+
+// T -= L U for a 64x64 target T (global, row-major), L row-major in global memory, U in
+// shared memory (row-major, stride kLdI); ls is shared scratch for L transposed. Ends with
+// a barrier before ls is written, so callers may pass a buffer they just read.
+__device__ __forceinline__ void sub_lu64(float *T, const float *L, const float *us, float *ls)
+{
+    const int tid = threadIdx.x;
+    float4 v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        v[q] = *reinterpret_cast<const float4 *>(L + (tid + q * kPivThreads) * 4);
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+    {
+        const int i = (tid + q * kPivThreads) * 4, r = i >> 6, c = i & 63;
+        ls[(c + 0) * kLdI + r] = v[q].x;
+        ls[(c + 1) * kLdI + r] = v[q].y;
+        ls[(c + 2) * kLdI + r] = v[q].z;
+        ls[(c + 3) * kLdI + r] = v[q].w;
+    }
+    __syncthreads();
+    const int R = 4 * (tid >> 4), C = 4 * (tid & 15);
+    float acc[4][4];
+    prod64_tile(ls, us, R, C, acc);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+    {
+        float4 *t = reinterpret_cast<float4 *>(T + (R + q) * 64 + C);
+        float4 o = *t;
+        o.x -= acc[q][0];
+        o.y -= acc[q][1];
+        o.z -= acc[q][2];
+        o.w -= acc[q][3];
+        *t = o;
+    }
+}
 
 // The upper blocks of the level's pivots as products with the pivots' inverses: CTA u of
 // the level's upper blocks (trsm_pref) computes U(k, c) = X A(k, c), X = D_k^{-1} from
 // `dinv` (or, for a pivot flagged in hg, the FP64 inverse in `inv64`, in FP64), stores it
 // and writes its BF16 split (transposed K-major) to `ops` at its split unit.
+//
+// First pivot k of a pair (i0 >= 0: the second pivot d at position i0 of k's lower column
+// and j0 of its upper row; the level has this one pivot): each upper-block CTA then also
+// applies k's update to d's row, T(d, c) -= L(d, k) U(k, c), and CTAs past the upper blocks
+// apply it to d's column, T(t, d) -= L(t, k) U(k, d) for the other rows t of k's lower
+// column, with U(k, d) from `ucd` (formed by k_piv64_inv with the same loop).
 __global__ void __launch_bounds__(kPivThreads, 2)
     k_strips64_inv(DevSym S, float *__restrict__ slab, int64_t p0, int64_t p1, const float *__restrict__ dinv,
-                   const double *__restrict__ inv64, const int *__restrict__ hg, unsigned char *__restrict__ ops)
+                   const double *__restrict__ inv64, const int *__restrict__ hg, unsigned char *__restrict__ ops,
+                   int32_t i0, int32_t j0, const float *__restrict__ ucd)
 {
     __shared__ __align__(16) float xs[64 * kLdI]; // X transposed: xs[c * kLdI + r] = X[r][c]
     __shared__ __align__(16) float as[64 * kLdI]; // A(k, c), then the product, row-major
     const int tid = threadIdx.x;
+    const int64_t n_trsm = S.trsm_pref[p1] - S.trsm_pref[p0];
+    if ((int64_t)blockIdx.x >= n_trsm)
+    {
+        // pair: a target in the second pivot's column
+        const int64_t k = S.piv[p0];
+        const int32_t ci = (int32_t)((int64_t)blockIdx.x - n_trsm);
+        const int32_t i = ci < i0 ? ci : ci + 1; // skip d's own row
+        const int32_t t = S.lcol_row[S.lcol_ptr[k] + i];
+        const int32_t dcol = S.cols[S.diag_pos[k] + 1 + j0];
+        float *T = slab + S.blk_off[find_col(S.cols, S.row_ptr[t], S.row_ptr[t + 1], dcol)];
+        const float *L = slab + S.blk_off[S.lcol_blk[S.lcol_ptr[k] + i]];
+        load_block64_ldi(ucd, as);
+        sub_lu64(T, L, as, xs);
+        return;
+    }
     const int64_t u = S.trsm_pref[p0] + blockIdx.x;
     const int64_t p = find_owner(S.trsm_pref, p0, p1, u);
     const int64_t k = S.piv[p];
     const int64_t j = u - S.trsm_pref[p];
     float *gb = slab + S.blk_off[S.diag_pos[k] + 1 + j];
     const float *xt = dinv + (int64_t)S.inv_idx[k] * 4096;
-    for (int i = tid; i < 64 * 16; i += kPivThreads)
-    {
-        const int r = i >> 4, c4 = (i & 15) * 4;
-        *reinterpret_cast<float4 *>(xs + r * kLdI + c4) = *reinterpret_cast<const float4 *>(xt + r * 64 + c4);
-        *reinterpret_cast<float4 *>(as + r * kLdI + c4) = *reinterpret_cast<const float4 *>(gb + r * 64 + c4);
-    }
+    load_block64_ldi(xt, xs);
+    load_block64_ldi(gb, as);
     __syncthreads();
     const int R = 4 * (tid >> 4), C = 4 * (tid & 15);
-    float acc[4][4] = {};
+    float acc[4][4];
     if (hg != nullptr && hg[k])
-    {
-        const double *x64 = inv64 + (p - p0) * 4096; // row-major X
-        double ad[4][4] = {};
-#pragma unroll 1
-        for (int m = 0; m < 64; ++m)
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-#pragma unroll
-                for (int e = 0; e < 4; ++e)
-                    ad[q][e] += x64[(R + q) * 64 + m] * (double)as[m * kLdI + C + e];
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-#pragma unroll
-            for (int e = 0; e < 4; ++e)
-                acc[q][e] = (float)ad[q][e];
-    }
+        prod64_tile_fp64(inv64 + (p - p0) * 4096, as, R, C, acc);
     else
-    {
-#pragma unroll 8
-        for (int m = 0; m < 64; ++m)
-        {
-            const float4 a4 = *reinterpret_cast<const float4 *>(xs + m * kLdI + R);
-            const float4 b4 = *reinterpret_cast<const float4 *>(as + m * kLdI + C);
-            const float av[4] = {a4.x, a4.y, a4.z, a4.w}, bv[4] = {b4.x, b4.y, b4.z, b4.w};
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-#pragma unroll
-                for (int e = 0; e < 4; ++e)
-                    acc[q][e] += av[q] * bv[e];
-        }
-    }
+        prod64_tile(xs, as, R, C, acc);
     __syncthreads(); // every thread is done reading A
 #pragma unroll
     for (int q = 0; q < 4; ++q)
@@ -664,6 +786,14 @@ __global__ void __launch_bounds__(kPivThreads, 2)
         const uint32_t off = sw128_offset(nn, q * 8);
         *reinterpret_cast<uint4 *>(dst + off) = hi;
         *reinterpret_cast<uint4 *>(dst + kSplitHalf + off) = lo;
+    }
+    if (i0 >= 0)
+    {
+        // pair: the target in the second pivot's row, T(d, c) -= L(d, k) U(k, c)
+        const int32_t drow = S.lcol_row[S.lcol_ptr[k] + i0];
+        const int32_t col = S.cols[S.diag_pos[k] + 1 + j];
+        float *T = slab + S.blk_off[find_col(S.cols, S.row_ptr[drow], S.row_ptr[drow + 1], col)];
+        sub_lu64(T, slab + S.blk_off[S.lcol_blk[S.lcol_ptr[k] + i0]], as, xs);
     }
 }
 

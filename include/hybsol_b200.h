@@ -229,8 +229,10 @@ typedef enum
      * one's other lower rows and upper columns are among the second one's): the first
      * pivot's update of the second one's row and column runs on the pivot chain, and one
      * tensor-core pass then applies both pivots to the second one's targets (K = 128), so
-     * each target is read and written once for two pivots. 0: one pass per pivot. The
-     * factors differ
+     * each target is read and written once for two pivots; on the inverse-and-products path
+     * (HYB_OPTION_ROW_PIVOTS 2) the first pivot's update of the second one's row and column
+     * is applied by the products launch. 2: the same with that update as its own launch.
+     * 0: one pass per pivot. The factors differ
      * only by FP32 rounding (the two products are summed in the accumulator before they are
      * subtracted). */
     HYB_OPTION_PAIR_PASSES = 14,
