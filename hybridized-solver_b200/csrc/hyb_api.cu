@@ -534,8 +534,11 @@ template <typename T> bool inverse_pivots(const hyb_system *h, int64_t l)
 // With pair_first (level l's pivot is the first of a pair on the inverse-and-products path),
 // the first pivot's update of the second one's row and column is applied by the products
 // kernel too; the caller then issues no separate update for it.
+// With second_done (level l's pivot is the second of such a pair), its LU and inverse were
+// formed by the first pivot's products launch: only its products (and splits) remain.
 template <typename T>
-int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cudaStream_t st, uint64_t &launches, bool pair_first = false)
+int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cudaStream_t st, uint64_t &launches, bool pair_first = false,
+                   bool second_done = false)
 {
     const Symbolic &S = h->S;
     const DevSym &ds = h->ds;
@@ -570,15 +573,21 @@ int enqueue_pivots(hyb_system *h, T *slab, int64_t l, cudaStream_t st, uint64_t 
             // a pair's first pivot: the second pivot's positions in its lower column and upper row
             const int32_t i0 = pair_first ? sh.la_i0 : -1, j0 = pair_first ? sh.la_j0 : -1;
             const int64_t n_col = pair_first ? S.lcol_ptr[S.piv[p0] + 1] - S.lcol_ptr[S.piv[p0]] - 1 : 0;
-            hyb::k_piv64_inv<<<(unsigned)(p1 - p0), hyb::kPivThreads, hyb::kInvSmem, st>>>(
-                ds, slab, p0, h->d_status, glim, h->d_dinv, inv64, h->d_hg, j0, pair_ucd(h));
-            ++launches;
-            HYB_LAUNCHED("k_piv64_inv", l);
+            // the second pivot's LU and inverse run in the first one's products launch
+            const int64_t pd = pair_first ? S.lvl_ptr[l + 1] : -1;
+            double *x64_d = h->d_piv64f + ((l + 1) & 1) * h->fused_half * 4096;
+            if (!second_done)
+            {
+                hyb::k_piv64_inv<<<(unsigned)(p1 - p0), hyb::kPivThreads, hyb::kInvSmem, st>>>(
+                    ds, slab, p0, h->d_status, glim, h->d_dinv, inv64, h->d_hg, j0, pair_ucd(h));
+                ++launches;
+                HYB_LAUNCHED("k_piv64_inv", l);
+            }
             if (n_trsm + n_col > 0)
             {
-                hyb::k_strips64_inv<<<(unsigned)(n_trsm + n_col), hyb::kPivThreads, 0, st>>>(
-                    ds, slab, p0, p1, h->d_dinv, inv64, glim > 0 ? h->d_hg : nullptr, level_ops(h, l), i0, j0,
-                    pair_ucd(h));
+                hyb::k_strips64_inv<<<(unsigned)(n_trsm + n_col), hyb::kPivThreads, pd >= 0 ? hyb::kInvSmem : 0,
+                                      st>>>(ds, slab, p0, p1, h->d_dinv, inv64, h->d_hg, level_ops(h, l), i0, j0,
+                                            pair_ucd(h), pd, x64_d, glim, h->d_status);
                 ++launches;
                 HYB_LAUNCHED("k_strips64_inv", l);
             }
@@ -964,8 +973,8 @@ template <typename T> bool pair_unit(const hyb_system *h, int64_t l)
 template <typename T> int enqueue_unit_pivots(hyb_system *h, T *slab, int64_t l, cudaStream_t st, uint64_t &launches)
 {
     const bool pair = pair_unit<T>(h, l);
-    const bool fold = pair && h->pair_passes == 1 && inverse_pivots<T>(h, l) && h->S.shape[l].la_i0 >= 0 &&
-                      h->S.shape[l].la_j0 >= 0;
+    const bool fold = pair && h->pair_passes == 1 && inverse_pivots<T>(h, l) && inverse_pivots<T>(h, l + 1) &&
+                      h->S.shape[l].la_i0 >= 0 && h->S.shape[l].la_j0 >= 0;
     int rc = enqueue_pivots<T>(h, slab, l, st, launches, fold);
     if (rc != HYB_SUCCESS || !pair)
         return rc;
@@ -973,7 +982,7 @@ template <typename T> int enqueue_unit_pivots(hyb_system *h, T *slab, int64_t l,
     if (!fold && (rc = enqueue_generic_update<T>(h, slab, l, st, 1, sh.la_prio_units, UPD_TILE32, launches)) !=
                      HYB_SUCCESS)
         return rc;
-    return enqueue_pivots<T>(h, slab, l + 1, st, launches);
+    return enqueue_pivots<T>(h, slab, l + 1, st, launches, false, fold);
 }
 
 // The two-pivot pass of the pair that starts at level l: mode 0 every target of b, 1 / 2 the
@@ -2360,6 +2369,7 @@ HYB_API int hyb_decompose(hyb_system *h, int precision, hyb_decompose_info *info
             allow_smem(hyb::k_piv64<float, false>, hyb::piv64_smem<float>()),
             allow_smem(hyb::k_piv64<float, true>, hyb::piv64_smem<float>()),
             allow_smem(hyb::k_piv64_inv, hyb::kInvSmem),
+            allow_smem(hyb::k_strips64_inv, hyb::kInvSmem),
             allow_smem(hyb::k_split64, 0),
             allow_smem(hyb::k_update<double>, 0),
             allow_smem(hyb::k_update<float>, 0),

@@ -531,16 +531,16 @@ static_assert(64 * 65 * 8 <= kInvSmem, "the FP64 fallback's LU fits the FP32 wor
 // also forms U(c,d) = X A(c,d) into `ucd` (row-major), with the loop k_strips64_inv uses
 // for the same block, so the column updates of the pair's second pivot can read it while
 // that block is being overwritten in place.
-__global__ void __launch_bounds__(kPivThreads, 1)
-    k_piv64_inv(DevSym S, float *__restrict__ slab, int64_t p0, int *status, float growth_limit,
-                float *__restrict__ dinv, double *__restrict__ inv64, int *__restrict__ hg, int32_t j0,
-                float *__restrict__ ucd)
+// The work of k_piv64_inv for pivot slot p, by the calling CTA (256 threads) in the
+// kInvSmem bytes at smem_raw, the FP64 inverse (if any) in `x64` (4096 doubles).
+__device__ __noinline__ void piv64_inv_body(const DevSym &S, float *__restrict__ slab, int64_t p, int *status,
+                                            float growth_limit, float *__restrict__ dinv, double *__restrict__ x64,
+                                            int *__restrict__ hg, int32_t j0, float *__restrict__ ucd,
+                                            unsigned char *smem_raw)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     float *d = reinterpret_cast<float *>(smem_raw);
     float *li = d + 64 * kLdD, *ui = li + 64 * kLdI, *tmp = ui + 64 * kLdI; // li 16-byte aligned
     const int tid = threadIdx.x;
-    const int64_t p = p0 + blockIdx.x;
     const int64_t k = S.piv[p];
     float *gd = slab + S.blk_off[S.diag_pos[k]];
     float *xt = dinv + (int64_t)S.inv_idx[k] * 4096;
@@ -564,7 +564,7 @@ __global__ void __launch_bounds__(kPivThreads, 1)
             // FP64: a = LU (64 x 65, shared memory), b = the inverse, row-major in the
             // pivot's FP64 slot (each thread works on its own column)
             double *a = reinterpret_cast<double *>(smem_raw);
-            double *b = inv64 + (p - p0) * 4096;
+            double *b = x64;
             __syncthreads();
             for (int i = tid; i < 64 * 64; i += kPivThreads)
                 a[(i >> 6) * 65 + (i & 63)] = (double)gd[i];
@@ -676,6 +676,16 @@ __global__ void __launch_bounds__(kPivThreads, 1)
     }
 }
 
+__global__ void __launch_bounds__(kPivThreads, 1)
+    k_piv64_inv(DevSym S, float *__restrict__ slab, int64_t p0, int *status, float growth_limit,
+                float *__restrict__ dinv, double *__restrict__ inv64, int *__restrict__ hg, int32_t j0,
+                float *__restrict__ ucd)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int64_t p = p0 + blockIdx.x;
+    piv64_inv_body(S, slab, p, status, growth_limit, dinv, inv64 + (p - p0) * 4096, hg, j0, ucd, smem_raw);
+}
+
 
 // T -= L U for a 64x64 target T (global, row-major), L row-major in global memory, U in
 // shared memory (row-major, stride kLdI); ls is shared scratch for L transposed. Ends with
@@ -724,10 +734,17 @@ __device__ __forceinline__ void sub_lu64(float *T, const float *L, const float *
 // applies k's update to d's row, T(d, c) -= L(d, k) U(k, c), and CTAs past the upper blocks
 // apply it to d's column, T(t, d) -= L(t, k) U(k, d) for the other rows t of k's lower
 // column, with U(k, d) from `ucd` (formed by k_piv64_inv with the same loop).
+//
+// With pd >= 0 (the pair's second pivot, slot pd), the CTA of the upper block in d's column
+// -- which forms d's diagonal block T(d, d) -- goes on to factor and invert it
+// (piv64_inv_body, in the launch's dynamic shared memory, FP64 inverse in x64_d), while the
+// launch's other CTAs finish: d's pivot work then needs only its products launch.
+// growth_limit > 0: hg flags pivots whose products run in FP64 (and d's check may set it).
 __global__ void __launch_bounds__(kPivThreads, 2)
-    k_strips64_inv(DevSym S, float *__restrict__ slab, int64_t p0, int64_t p1, const float *__restrict__ dinv,
-                   const double *__restrict__ inv64, const int *__restrict__ hg, unsigned char *__restrict__ ops,
-                   int32_t i0, int32_t j0, const float *__restrict__ ucd)
+    k_strips64_inv(DevSym S, float *__restrict__ slab, int64_t p0, int64_t p1, float *__restrict__ dinv,
+                   const double *__restrict__ inv64, int *__restrict__ hg, unsigned char *__restrict__ ops,
+                   int32_t i0, int32_t j0, const float *__restrict__ ucd, int64_t pd, double *__restrict__ x64_d,
+                   float growth_limit, int *status)
 {
     __shared__ __align__(16) float xs[64 * kLdI]; // X transposed: xs[c * kLdI + r] = X[r][c]
     __shared__ __align__(16) float as[64 * kLdI]; // A(k, c), then the product, row-major
@@ -758,7 +775,7 @@ __global__ void __launch_bounds__(kPivThreads, 2)
     __syncthreads();
     const int R = 4 * (tid >> 4), C = 4 * (tid & 15);
     float acc[4][4];
-    if (hg != nullptr && hg[k])
+    if (growth_limit > 0 && hg[k])
         prod64_tile_fp64(inv64 + (p - p0) * 4096, as, R, C, acc);
     else
         prod64_tile(xs, as, R, C, acc);
@@ -794,6 +811,13 @@ __global__ void __launch_bounds__(kPivThreads, 2)
         const int32_t col = S.cols[S.diag_pos[k] + 1 + j];
         float *T = slab + S.blk_off[find_col(S.cols, S.row_ptr[drow], S.row_ptr[drow + 1], col)];
         sub_lu64(T, slab + S.blk_off[S.lcol_blk[S.lcol_ptr[k] + i0]], as, xs);
+        if (pd >= 0 && j == j0)
+        {
+            // this CTA formed T(d, d): the second pivot's LU and inverse follow here
+            extern __shared__ __align__(16) unsigned char smem_dyn[];
+            __syncthreads(); // T(d, d) written by every thread of the CTA
+            piv64_inv_body(S, slab, pd, status, growth_limit, dinv, x64_d, hg, -1, nullptr, smem_dyn);
+        }
     }
 }
 
