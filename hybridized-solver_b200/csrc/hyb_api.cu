@@ -173,6 +173,7 @@ struct hyb_system
     bool alternate_walk = true;           // HYB_OPTION_ALTERNATE_WALK
     int pair_passes = 1;                  // HYB_OPTION_PAIR_PASSES (mixed form; 2: inner update launched apart)
     int row_pivots = -1;                  // HYB_OPTION_ROW_PIVOTS: -1 per precision (mixed 2, FP64 0)
+    int update_sm_reserve = 4;            // HYB_OPTION_UPDATE_SM_RESERVE
     // generic-size Schur updates: HYB_OPTION_UPDATE_KERNEL (-1: tuned per size bucket), and
     // the tuned choice per precision and bucket (-1: not tuned yet)
     int update_kernel = -1;
@@ -1000,7 +1001,9 @@ template <typename T> int enqueue_pair_update(hyb_system *h, T *slab, int64_t l,
         const int4 pr = make_int4(ps.i0, ps.i1, ps.j0, ps.j1);
         // alternate passes walk their targets backwards (the priority launch keeps its order)
         const int reverse = h->alternate_walk && mode != 1 && ((l >> 1) & 1) ? 1 : 0;
-        const unsigned grid = (unsigned)std::min<int64_t>(tiles, (int64_t)sm_count());
+        // the main launch may leave SMs free for the next unit's pivot work
+        const int64_t sms = mode == 1 ? sm_count() : std::max(1, sm_count() - h->update_sm_reserve);
+        const unsigned grid = (unsigned)std::min<int64_t>(tiles, sms);
         hyb::k_update64_tc2<<<grid, hyb::kTc2Threads, hyb::kTc2Smem, st>>>(
             h->ds, slab, level_ops(h, l), level_ops(h, l + 1), level_tgt(h, l + 1), zero_split(h), S.lvl_ptr[l],
             S.lvl_ptr[l + 1], mode, pr, tiles, h->d_status, reverse);
@@ -2085,6 +2088,7 @@ HYB_API int hyb_system_copy(const hyb_system *src, hyb_system **out)
     h->alternate_walk = src->alternate_walk;
     h->pair_passes = src->pair_passes;
     h->row_pivots = src->row_pivots;
+    h->update_sm_reserve = src->update_sm_reserve;
     h->update_kernel = src->update_kernel;
     h->lu_once = src->lu_once;
     h->fp64_shape = src->fp64_shape;
@@ -2223,6 +2227,15 @@ HYB_API int hyb_system_set_option(hyb_system *h, int option, int64_t value)
         {
             h->alternate_walk = value != 0;
             h->g_factor[0].reset();
+            h->g_factor[1].reset();
+        }
+        return HYB_SUCCESS;
+    case HYB_OPTION_UPDATE_SM_RESERVE:
+        if (value < 0 || value > 64)
+            return HYB_INVALID_ARGUMENT;
+        if (h->update_sm_reserve != (int)value)
+        {
+            h->update_sm_reserve = (int)value;
             h->g_factor[1].reset();
         }
         return HYB_SUCCESS;

@@ -41,7 +41,8 @@ OPTION_UPDATE_KERNEL = 11  # -1 tuned, 0 32x32 SIMT, 1 64x64 SIMT, 2 DMMA
 OPTION_PIVOT_LU_ONCE = 12
 OPTION_FP64_MMA_SHAPE = 13
 OPTION_PAIR_PASSES = 14  # mixed form: two consecutive pivots per tensor-core pass
-OPTION_ROW_PIVOTS = 15  # 64-row pivots: LU by rows, row solves by columns (64-thread CTAs)
+OPTION_ROW_PIVOTS = 15  # 64-row pivots: -1 per precision, 0 256-thread kernels, 1 blocked, 2 inverse + products
+OPTION_UPDATE_SM_RESERVE = 16  # mixed form: SMs the two-pivot update leaves free for the pivot work
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _i64p = ctypes.POINTER(ctypes.c_int64)

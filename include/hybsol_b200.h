@@ -245,7 +245,13 @@ typedef enum
      * upper blocks are taken as products with the inverse, so the pivot's critical path
      * holds no substitution (FP32 factors that differ from 0 and 1 by rounding); -1
      * (default): 2 for the mixed form, 0 for the FP64 form. */
-    HYB_OPTION_ROW_PIVOTS = 15
+    HYB_OPTION_ROW_PIVOTS = 15,
+    /* Mixed form, two-pivot passes: SMs the main update launch leaves free for the next
+     * unit's pivot work, which runs beside it (default 4, at most 64). The pivot chain is
+     * latency-bound; beside an update CTA it runs about twice as slowly as on a free SM.
+     * Measured at 128x128 p=8 on one B200: factorization 1,561 ms with 0, 1,350 ms with 4,
+     * 1,364 ms with 8, 1,383 ms with 16. The factors do not depend on it. */
+    HYB_OPTION_UPDATE_SM_RESERVE = 16
 } hyb_option;
 
 /* Sets a schedule option of the handle (takes effect at the next decomposition). */
