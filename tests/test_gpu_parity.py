@@ -285,6 +285,25 @@ def test_row_pivots_match_256_thread_kernels(gpu, prec, pairs):
     assert all(np.array_equal(x, y) for x, y in zip(blocks, blocks2))
 
 
+def test_update_sm_reserve_is_schedule_only(gpu):
+    """Leaving SMs free for the pivot chain changes which CTA updates a target, not the
+    target's arithmetic: the mixed factors are bit-identical for 0, 4 and 16 free SMs."""
+    mat, b = _mesh(12, 8, seed=29)
+    order, pm, ns = _native_from(gpu, mat)
+    ref = None
+    for reserve in (0, 4, 16):
+        ns.set_option(gpu.OPTION_UPDATE_SM_RESERVE, reserve)
+        ns.set_values(pm.vals)
+        ns.decompose(gpu.MIXED)
+        blocks = [ns.get_block(i, c, (int(pm.sizes[i]), int(pm.sizes[c]))) for i in range(pm.n_blocks) for c in ns.row_cols(i)]
+        if ref is None:
+            ref = blocks
+        else:
+            assert all(np.array_equal(x, y) for x, y in zip(ref, blocks)), reserve
+    with pytest.raises(gpu.HybError):
+        ns.set_option(gpu.OPTION_UPDATE_SM_RESERVE, 65)
+
+
 @pytest.mark.parametrize("pairs", [0, 1])
 def test_inverse_pivots_match_substitution(gpu, pairs):
     """Mixed form: each 64-row pivot factored once and its upper blocks taken as products
