@@ -1985,6 +1985,7 @@ HYB_API int hyb_analyze(uint64_t n, const uint64_t *block_sizes, const uint64_t 
         out->nops = (uint64_t)(S.lcol_ptr[S.n] + S.n);
         out->slab_bytes_fp64 = (uint64_t)S.slab_elems() * sizeof(double);
         out->factor_flops = S.factor_flops;
+        out->pair_levels = (uint64_t)S.n_pairs;
         if (filled_row_ptr)
             for (int64_t i = 0; i <= S.n; ++i)
                 filled_row_ptr[i] = (uint64_t)S.row_ptr[i];

@@ -101,6 +101,7 @@ class Analysis(ctypes.Structure):
         ("nops", ctypes.c_uint64),
         ("slab_bytes_fp64", ctypes.c_uint64),
         ("factor_flops", ctypes.c_double),
+        ("pair_levels", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:

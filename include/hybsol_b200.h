@@ -121,6 +121,8 @@ typedef struct
     uint64_t nops;            /* operations() entries: lower blocks + block rows */
     uint64_t slab_bytes_fp64; /* device bytes of the FP64 factor slab (blocks padded to 256 B) */
     double factor_flops;      /* exact algorithmic flops of the factorization */
+    uint64_t pair_levels;     /* pairs of consecutive single-pivot, uniform-64 levels the mixed form can
+                                 apply in one two-pivot pass (HYB_OPTION_PAIR_PASSES) */
 } hyb_analysis;
 
 /* Runs the symbolic phase on the host alone (no GPU needed): the fill the reference's

@@ -35,6 +35,22 @@ def test_orderings_and_fill_match_reference(native, name):
     assert a["filled_blocks"] == len(g["filled_cols"])
 
 
+@pytest.mark.parametrize(("n", "p", "pairs"), [(8, 8, 31), (12, 8, 71), (24, 8, 287), (16, 4, 0), (6, "rand", 0)])
+def test_two_pivot_pairs(native, n, p, pairs):
+    """Consecutive single-pivot levels of 64-blocks pair up for the mixed form's two-pivot
+    update passes: on an n x n p=8 mesh the n*n element levels form n*n/2 - 1 pairs (the
+    last element has no lower or upper blocks to share); blocks of other sizes never pair."""
+    from hybsol.b200 import meshgen
+
+    pp = meshgen.random_orders(n, 2, 10, seed=3) if p == "rand" else p
+    mat, _ = meshgen.mesh_system(n, pp, seed=0)
+    order = native.compute_ordering(mat.row_ptr, mat.cols, "first")
+    pm = mat.permuted(order)
+    a = native.analyze(pm.sizes, pm.row_ptr, pm.cols)
+    assert a["pair_levels"] == pairs
+    assert 2 * a["pair_levels"] <= a["n_levels"]
+
+
 def test_mesh16_work_counts(native):
     """Exact algorithmic counts of the 16x16 p=4 system (10,558 blocks after fill, 0.531 GFLOP)."""
     g = golden("mesh16_p4.npz")
