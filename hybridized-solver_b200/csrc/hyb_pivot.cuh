@@ -1,19 +1,22 @@
 // hyb_pivot.cuh - pivot work of levels whose pivots and upper blocks are all 64x64: the LU
-// of each diagonal block and the solves of its row's upper blocks, and (mixed form) the BF16
-// splits of the pivot's lower-column and upper-row blocks for the tensor-core update.
+// of each diagonal block and its row's upper blocks U(k, c) = D_k^{-1} A(k, c), plus (mixed
+// form) the BF16 splits of the pivot's upper-row blocks for the tensor-core update.
 //
-// The work of one pivot sits on the elimination's critical path (the next pivot waits for
-// it), so it is organised for latency with 64 threads per CTA:
-//  - LU: thread i holds row i of the block in registers; at step k the thread of row k
-//    publishes it through shared memory (one barrier of two warps per step), and every
-//    thread below eliminates its own row -- no shuffles, no per-element shared traffic.
-//  - row solve: thread j holds column j of one upper block in registers and substitutes
-//    with the factors read as shared-memory broadcasts (every thread reads the same
-//    address), so a step of the substitution is one FMA chain in registers.
-//  - the solved block's split is written from the registers that hold it.
-// Every element receives the same operations in the same order as in k_lu_trsm64 (unit-L
-// Doolittle, multipliers times the pivot's reciprocal; forward substitution, then backward
-// dividing by the diagonal), so the factors are the same bits.
+// The work of one pivot lies on the elimination's critical path (the next pivot waits for
+// it), so it is organised for latency, in CTAs of 256 threads:
+//  - lu64_blocked: the 64x64 LU in eight panels of eight columns; one warp factors a panel
+//    with shuffles (no CTA barrier per pivot step), then the CTA solves the panel's row
+//    block and applies the rank-8 trailing update;
+//  - solve64_blocked: a row solve in 8x8 blocks, four threads per column, a block's values
+//    shuffled from the thread that owns it;
+//  - k_piv64 (HYB_OPTION_ROW_PIVOTS 1): one CTA per upper block, each factoring the block
+//    itself and solving its upper block; every element receives the operations of the
+//    unblocked kernels in the same order, so the factors are the same bits;
+//  - k_piv64_inv + k_strips64_inv (mixed form default): one CTA per pivot factors the block
+//    once and forms its inverse, and the upper blocks become independent products with it
+//    (plus, for the first pivot of a two-pivot pass, that pivot's update of the second one's
+//    row and column, and the second one's LU and inverse in the CTA that forms its diagonal
+//    block).
 #pragma once
 
 #include "hyb_umma.cuh"
@@ -21,7 +24,7 @@
 namespace hyb
 {
 
-constexpr int kPivThreads = 256;
+constexpr int kPivThreads = 256; // threads of every pivot kernel's CTA
 constexpr int kLdD = 65; // row stride of the diagonal block in shared memory
 constexpr int kLdQ = 80; // column stride of the transposed factors (four 16-row quarters, 20 apart)
 constexpr int kLdI = 68; // row stride of the inverses and product operands (16-byte rows)
