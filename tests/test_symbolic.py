@@ -51,6 +51,55 @@ def test_two_pivot_pairs(native, n, p, pairs):
     assert 2 * a["pair_levels"] <= a["n_levels"]
 
 
+def _banded_pattern(n, seed):
+    """Random unsymmetric banded pattern of 64x64 blocks (half bandwidth 3), diagonal set."""
+    rng = np.random.default_rng(seed)
+    rows = []
+    for i in range(n):
+        cs = {i} | {j for j in range(max(0, i - 3), min(n, i + 4)) if j != i and rng.random() < 0.55}
+        rows.append(sorted(cs))
+    row_ptr = np.cumsum([0] + [len(r) for r in rows]).astype(np.uint64)
+    cols = np.array([c for r in rows for c in r], dtype=np.uint64)
+    return np.full(n, 64, dtype=np.uint64), row_ptr, cols
+
+
+def _restated_pairs(n, frp, fcols):
+    """The pairing rule, restated on the filled pattern: levels l, l+1 (one pivot each, a
+    then b, greedily from the first level) pair when b has lower and upper blocks, b lies in
+    a's lower column and upper row, and a's other lower rows / upper columns are b's too."""
+    filled = [set(fcols[frp[i] : frp[i + 1]].tolist()) for i in range(n)]
+    lower = [{t for t in range(k + 1, n) if k in filled[t]} for k in range(n)]
+    upper = [{c for c in filled[k] if c > k} for k in range(n)]
+    level = [0] * n
+    for k in range(n):
+        deps = [j for j in range(k) if j in filled[k] or k in filled[j]]
+        level[k] = 1 + max(level[j] for j in deps) if deps else 0
+    piv = [[k for k in range(n) if level[k] == lv] for lv in range(max(level) + 1)]
+    pairs, lv = 0, 0
+    while lv + 1 < len(piv):
+        if len(piv[lv]) == 1 and len(piv[lv + 1]) == 1:
+            a, b = piv[lv][0], piv[lv + 1][0]
+            ra, ca, rb, cb = lower[a], upper[a], lower[b], upper[b]
+            if rb and cb and b in ra and b in ca and ra - {b} <= rb and ca - {b} <= cb:
+                pairs += 1
+                lv += 2
+                continue
+        lv += 1
+    return pairs
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_pairs_match_restated_rule(native, seed):
+    """The symbolic phase's pairs of levels (two-pivot passes) on random banded patterns
+    agree with the pairing rule restated on the filled pattern."""
+    n = 24 + seed
+    sizes, row_ptr, cols = _banded_pattern(n, seed)
+    a = native.analyze(sizes, row_ptr, cols, pattern=True)
+    frp = a["filled_row_ptr"].astype(np.int64)
+    fc = a["filled_cols"].astype(np.int64)
+    assert a["pair_levels"] == _restated_pairs(n, frp, fc)
+
+
 def test_mesh16_work_counts(native):
     """Exact algorithmic counts of the 16x16 p=4 system (10,558 blocks after fill, 0.531 GFLOP)."""
     g = golden("mesh16_p4.npz")
